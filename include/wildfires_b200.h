@@ -1,0 +1,148 @@
+/*
+ * wildfires_b200.h -- C-ABI of the B200 coupled atmosphere-wildfire solver.
+ *
+ * The solver advances the state of the reference model (dsanmartinreyes'
+ * wildfires, src/cu) by RK time steps on one NVIDIA B200 with hand-written
+ * sm_100a kernels: one fused right-hand-side pass per RK stage, an FP64
+ * FFT(x,y) + tridiagonal(z) pressure Poisson solve, and a fused projection /
+ * boundary / clamp pass.  All entry points return a wf_status (never exit or
+ * assert); a human-readable message for the last failure on the calling host
+ * thread is available from wf_last_error().
+ *
+ * Data conventions are the reference's: a packed state vector holds
+ * [u | v | w | T | Y], u..T as Nx*Ny*Nz FP64 values in IDX(i,j,k) =
+ * k + Nz*(j + Ny*i) (z fastest; reference include/cu/utils.cuh:18-20), then Y as
+ * Nx*Ny*Nz_Y_max values in k + Nz_Y_max*(j + Ny*i).  Pressure p is Nx*Ny*Nz
+ * FP64 in the same layout.  The planes i = Nx-1 and j = Ny-1 duplicate planes
+ * 0 (period Nx-1, Ny-1).
+ *
+ * The reference-compatible C++ entry points (solve_PDE, Phi, RK4,
+ * solve_pressure, solve_pressure_iterative) are declared in wf_dropin.h.
+ */
+#ifndef WILDFIRES_B200_H
+#define WILDFIRES_B200_H
+
+#include <stddef.h>
+
+#include "wf_parameters.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum wf_status {
+    WF_OK = 0,
+    WF_ERR_ARG = 1,          /* invalid argument or unsupported configuration */
+    WF_ERR_CUDA = 2,         /* CUDA runtime error (message in wf_last_error) */
+    WF_ERR_IO = 3,           /* file missing, unreadable or of the wrong size */
+    WF_ERR_PARSE = 4,        /* parameter file could not be parsed */
+    WF_ERR_OOM = 5,          /* device or host allocation failed */
+    WF_ERR_NAN = 6,          /* a NaN was found in the state (diagnostics) */
+    WF_ERR_NO_DEVICE = 7     /* no CUDA device of compute capability 10.0 */
+} wf_status;
+
+typedef enum wf_precision {
+    WF_FP64 = 0,             /* every field and operator in FP64 */
+    WF_FP32_STENCIL = 1      /* u,v,w,T,Y stored and advanced in FP32; pressure,
+                                divergence and diagnostics in FP64 */
+} wf_precision;
+
+typedef struct wf_ctx wf_ctx;
+
+/* Global diagnostics of the current state, reduced on the GPU in FP64. */
+typedef struct wf_diag {
+    double mass;             /* sum rho dV over interior cells, rho = T_inf rho_inf / T */
+    double energy;           /* sum rho c_p T dV */
+    double fuel;             /* sum Y dV over stored fuel cells (k < Nz_Y(i,j)) */
+    double fuel_consumed;    /* initial fuel minus fuel (since the last upload) */
+    double max_abs_u, max_abs_v, max_abs_w;
+    double cfl;              /* dt (max|u|/dx + max|v|/dy + max|w|/dz), functions.cu:180 */
+    double T_min, T_max;     /* over all cells */
+    double Y_min, Y_max;     /* over stored fuel cells */
+    long long nan_count;     /* NaN values found in u, v, w, T, Y */
+} wf_diag;
+
+/* ---- parameters --------------------------------------------------------- */
+
+/* Parse a `key = value` parameter file with the reference's rules
+ * (src/cu/parameters.cu:39-415: defaults, prefix match, later lines override,
+ * unknown keys ignored) and fill the derived arrays (grid, time, wavenumbers,
+ * terrain, immersed-boundary tables; parameters.cu:416-523, ibm.cu:3-95).
+ * Unlike the reference it creates no output directory and opens no log file.
+ * Release with wf_free_parameters. */
+wf_status wf_read_parameters(const char *path, Parameters *out);
+
+/* Release the host arrays allocated by wf_read_parameters / wf_set_topography. */
+void wf_free_parameters(Parameters *p);
+
+/* Replace the terrain by an explicit Nx*Ny height field (j fastest) and
+ * recompute cut_nodes, Nz_Y, Nz_Y_max, z_ibm (ibm.cu:57-95).  Changes the
+ * packed-state size when Nz_Y_max changes. */
+wf_status wf_set_topography(Parameters *p, const double *topo);
+
+/* Number of FP64 values in a packed state vector: 4*Nx*Ny*Nz + Nx*Ny*Nz_Y_max. */
+size_t wf_state_size(const Parameters *p);
+
+/* Read an initial state from `<dir>u.bin, v.bin, w.bin, T.bin, Y.bin, p.bin`
+ * (input.cu:3-58) into a packed host state y (wf_state_size values) and p
+ * (Nx*Ny*Nz values). */
+wf_status wf_load_fields(const Parameters *p, const char *dir, double *y, double *pr);
+
+/* Write a packed host state and p as `<dir>u.bin.<n>` ... `p.bin.<n>` in the
+ * reference's raw FP64 format (output.cu:3-44). */
+wf_status wf_save_fields(const Parameters *p, const char *dir, int n, const double *y, const double *pr);
+
+/* ---- solver context ----------------------------------------------------- */
+
+/* Create a solver on the current CUDA device for the given record (copied;
+ * the record's host arrays are read once).  Allocates all device memory the
+ * time loop needs; nothing is allocated afterwards. */
+wf_status wf_create(const Parameters *p, int precision, wf_ctx **out);
+wf_status wf_destroy(wf_ctx *ctx);
+
+/* Upload a packed FP64 host state and p (the time level becomes 0). */
+wf_status wf_upload_state(wf_ctx *ctx, const double *y, const double *pr);
+/* Download the current packed state and p as FP64. */
+wf_status wf_download_state(wf_ctx *ctx, double *y, double *pr);
+
+/* Advance nsteps time steps (RK stages, pressure solve, projection, boundary
+ * rules, clamps, temperature source).  Enqueued on the context's stream; the
+ * first call records the step into a CUDA graph that later calls replay. */
+wf_status wf_step(wf_ctx *ctx, int nsteps);
+wf_status wf_synchronize(wf_ctx *ctx);
+
+/* Current time level n and time t[n]. */
+wf_status wf_time(const wf_ctx *ctx, int *n, double *t);
+
+/* FP64 diagnostics of the current state. */
+wf_status wf_diagnostics(wf_ctx *ctx, wf_diag *out);
+
+/* Device pointers of the current state (precision-dependent element type:
+ * double for WF_FP64, float for WF_FP32_STENCIL) and of p (double).  Valid
+ * until the next wf_step. */
+wf_status wf_device_state(wf_ctx *ctx, void **y, double **pr);
+/* The CUDA stream (cudaStream_t) the context enqueues on. */
+void *wf_stream(wf_ctx *ctx);
+
+/* ---- operator-level entry points (used by the parity tests) ------------- */
+
+/* One right-hand-side evaluation R_new = Phi(R_old) on host buffers (packed
+ * state layout) -- RHS, SGS terms and boundary rules (pde.cu:910-917). */
+wf_status wf_phi(wf_ctx *ctx, const double *R_old, double *R_new);
+
+/* One pressure solve on host buffers: p is read (top plane, and the previous
+ * iterate for variable density) and overwritten (pressure.cu:506-606).
+ * Returns the number of solves in *iters (may be NULL). */
+wf_status wf_pressure(wf_ctx *ctx, const double *y_np1, const double *y_n, double *pr, int *iters);
+
+/* Number of kernel launches one wf_step(ctx, 1) enqueues. */
+int wf_launches_per_step(const wf_ctx *ctx);
+
+const char *wf_status_string(wf_status s);
+const char *wf_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

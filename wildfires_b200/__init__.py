@@ -1,0 +1,184 @@
+"""B200 coupled atmosphere-wildfire solver: Python host API over the C-ABI.
+
+The time step of the reference model (dsanmartinreyes' wildfires, src/cu) runs
+as hand-written sm_100a CUDA kernels in libwildfires_b200.so; this module only
+moves host buffers in and out.  Typical use::
+
+    from wildfires_b200 import read_parameters, Solver
+    P = read_parameters("parameters.txt")
+    with Solver(P, precision="fp32") as s:
+        s.upload(y0, p0)          # packed [u|v|w|T|Y] FP64 host state, pressure
+        s.step(100)
+        y, p = s.download()
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._abi import WF_FP32_STENCIL, WF_FP64, WfDiag, WfError, check, lib
+from ._params import Parameters
+
+__all__ = ["Params", "Solver", "read_parameters", "WfError", "Parameters"]
+
+_dp = C.POINTER(C.c_double)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+class Params:
+    """A parsed parameter record whose host arrays are owned by the library."""
+
+    def __init__(self, rec):
+        self.rec = rec
+        self._owned = True
+
+    @property
+    def shape(self):
+        r = self.rec
+        return r.Nx, r.Ny, r.Nz
+
+    @property
+    def state_size(self):
+        return int(lib().wf_state_size(C.byref(self.rec)))
+
+    def array(self, name, n):
+        p = getattr(self.rec, name)
+        return np.ctypeslib.as_array(p, shape=(n,)).copy()
+
+    def z(self):
+        return self.array("z", self.rec.Nz)
+
+    def nz_y(self):
+        r = self.rec
+        return np.ctypeslib.as_array(r.Nz_Y, shape=(r.Nx * r.Ny,)).copy().reshape(r.Nx, r.Ny)
+
+    def cut_nodes(self):
+        r = self.rec
+        return np.ctypeslib.as_array(r.cut_nodes, shape=(r.Nx * r.Ny,)).copy().reshape(r.Nx, r.Ny)
+
+    def set_topography(self, topo):
+        t = np.ascontiguousarray(topo, dtype=np.float64).reshape(-1)
+        r = self.rec
+        assert t.size == r.Nx * r.Ny
+        check(lib().wf_set_topography(C.byref(r), _ptr(t)), "wf_set_topography")
+
+    def free(self):
+        if self._owned:
+            lib().wf_free_parameters(C.byref(self.rec))
+            self._owned = False
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def read_parameters(path):
+    """Parse a reference-format parameter file (no output directory is created)."""
+    rec = Parameters()
+    check(lib().wf_read_parameters(str(path).encode(), C.byref(rec)), "wf_read_parameters")
+    return Params(rec)
+
+
+def load_fields(params, directory):
+    """Read <dir>u.bin ... p.bin into a packed state and p (reference input format)."""
+    r = params.rec
+    y = np.empty(params.state_size)
+    p = np.empty(r.Nx * r.Ny * r.Nz)
+    d = str(directory)
+    if not d.endswith("/"):
+        d += "/"
+    check(lib().wf_load_fields(C.byref(r), d.encode(), _ptr(y), _ptr(p)), "wf_load_fields")
+    return y, p
+
+
+class Solver:
+    """A solver context on the current CUDA device."""
+
+    def __init__(self, params, precision="fp64"):
+        self.params = params
+        prec = {"fp64": WF_FP64, "fp32": WF_FP32_STENCIL}[precision]
+        self.precision = precision
+        h = C.c_void_p()
+        check(lib().wf_create(C.byref(params.rec), prec, C.byref(h)), "wf_create")
+        self._h = h
+        r = params.rec
+        self.N = r.Nx * r.Ny * r.Nz
+        self.S = params.state_size
+
+    def close(self):
+        if self._h:
+            lib().wf_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, y, p):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        assert y.size == self.S and p.size == self.N
+        check(lib().wf_upload_state(self._h, _ptr(y), _ptr(p)), "wf_upload_state")
+
+    def download(self):
+        y = np.empty(self.S)
+        p = np.empty(self.N)
+        check(lib().wf_download_state(self._h, _ptr(y), _ptr(p)), "wf_download_state")
+        return y, p
+
+    def step(self, n=1):
+        check(lib().wf_step(self._h, int(n)), "wf_step")
+
+    def synchronize(self):
+        check(lib().wf_synchronize(self._h), "wf_synchronize")
+
+    def time(self):
+        n = C.c_int()
+        t = C.c_double()
+        check(lib().wf_time(self._h, C.byref(n), C.byref(t)), "wf_time")
+        return n.value, t.value
+
+    def diagnostics(self, allow_nan=False):
+        d = WfDiag()
+        s = lib().wf_diagnostics(self._h, C.byref(d))
+        if not (allow_nan and s == 6):
+            check(s, "wf_diagnostics")
+        return {f: getattr(d, f) for f, _ in WfDiag._fields_}
+
+    def phi(self, R_old):
+        R_old = np.ascontiguousarray(R_old, dtype=np.float64)
+        out = np.empty(self.S)
+        check(lib().wf_phi(self._h, _ptr(R_old), _ptr(out)), "wf_phi")
+        return out
+
+    def pressure(self, y_np1, y_n, p):
+        a = np.ascontiguousarray(y_np1, dtype=np.float64)
+        b = np.ascontiguousarray(y_n, dtype=np.float64)
+        pp = np.array(p, dtype=np.float64, copy=True)
+        it = C.c_int()
+        check(lib().wf_pressure(self._h, _ptr(a), _ptr(b), _ptr(pp), C.byref(it)), "wf_pressure")
+        return pp, it.value
+
+    def device_state(self):
+        y = C.c_void_p()
+        p = _dp()
+        check(lib().wf_device_state(self._h, C.byref(y), C.byref(p)), "wf_device_state")
+        return y.value, C.cast(p, C.c_void_p).value
+
+    def stream(self):
+        return lib().wf_stream(self._h)
+
+    def launches_per_step(self):
+        return lib().wf_launches_per_step(self._h)

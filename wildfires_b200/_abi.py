@@ -1,0 +1,95 @@
+"""ctypes binding of libwildfires_b200.so (the C-ABI in include/wildfires_b200.h).
+
+The library is built in-tree by wildfires_b200/build.py.  Loading fails
+loudly when it is missing: there is no CPU implementation behind this API.
+"""
+import ctypes as C
+import os
+
+from ._params import Parameters
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwildfires_b200.so")
+
+WF_OK, WF_ERR_ARG, WF_ERR_CUDA, WF_ERR_IO, WF_ERR_PARSE, WF_ERR_OOM, WF_ERR_NAN, WF_ERR_NO_DEVICE = range(8)
+WF_FP64, WF_FP32_STENCIL = 0, 1
+
+#: every symbol include/wildfires_b200.h declares
+EXPORTS = [
+    "wf_read_parameters", "wf_free_parameters", "wf_set_topography", "wf_state_size",
+    "wf_load_fields", "wf_save_fields", "wf_create", "wf_destroy", "wf_upload_state",
+    "wf_download_state", "wf_step", "wf_synchronize", "wf_time", "wf_diagnostics",
+    "wf_device_state", "wf_stream", "wf_phi", "wf_pressure", "wf_launches_per_step",
+    "wf_status_string", "wf_last_error",
+]
+
+
+class WfDiag(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "mass", "energy", "fuel", "fuel_consumed", "max_abs_u", "max_abs_v", "max_abs_w",
+        "cfl", "T_min", "T_max", "Y_min", "Y_max")] + [("nan_count", C.c_longlong)]
+
+
+class WfError(RuntimeError):
+    def __init__(self, status, where, msg):
+        super().__init__("%s: status %d (%s): %s" % (where, status, _status_name(status), msg))
+        self.status = status
+
+
+_names = {WF_OK: "ok", WF_ERR_ARG: "invalid argument", WF_ERR_CUDA: "CUDA error", WF_ERR_IO: "I/O error",
+          WF_ERR_PARSE: "parse error", WF_ERR_OOM: "out of memory", WF_ERR_NAN: "NaN in state",
+          WF_ERR_NO_DEVICE: "no sm_100 device"}
+
+
+def _status_name(s):
+    return _names.get(s, "unknown")
+
+
+_lib = None
+
+
+def lib():
+    """Load the library once; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libwildfires_b200.so is not built (run python wildfires_b200/build.py)")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER(Parameters)
+    dp = C.POINTER(C.c_double)
+    vp = C.c_void_p
+    sig = {
+        "wf_read_parameters": (C.c_int, [C.c_char_p, P]),
+        "wf_free_parameters": (None, [P]),
+        "wf_set_topography": (C.c_int, [P, dp]),
+        "wf_state_size": (C.c_size_t, [P]),
+        "wf_load_fields": (C.c_int, [P, C.c_char_p, dp, dp]),
+        "wf_save_fields": (C.c_int, [P, C.c_char_p, C.c_int, dp, dp]),
+        "wf_create": (C.c_int, [P, C.c_int, C.POINTER(vp)]),
+        "wf_destroy": (C.c_int, [vp]),
+        "wf_upload_state": (C.c_int, [vp, dp, dp]),
+        "wf_download_state": (C.c_int, [vp, dp, dp]),
+        "wf_step": (C.c_int, [vp, C.c_int]),
+        "wf_synchronize": (C.c_int, [vp]),
+        "wf_time": (C.c_int, [vp, C.POINTER(C.c_int), dp]),
+        "wf_diagnostics": (C.c_int, [vp, C.POINTER(WfDiag)]),
+        "wf_device_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(dp)]),
+        "wf_stream": (vp, [vp]),
+        "wf_phi": (C.c_int, [vp, dp, dp]),
+        "wf_pressure": (C.c_int, [vp, dp, dp, dp, C.POINTER(C.c_int)]),
+        "wf_launches_per_step": (C.c_int, [vp]),
+        "wf_status_string": (C.c_char_p, [C.c_int]),
+        "wf_last_error": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status, where):
+    if status != WF_OK:
+        raise WfError(status, where, lib().wf_last_error().decode(errors="replace"))

@@ -1,0 +1,799 @@
+// solver.cu -- solver context of the C-ABI: device buffers, precomputed
+// tables, the per-step launch sequence and its CUDA-graph replay.
+//
+// One step (reference src/cu/solver.cu:178-265) is
+//   RK stages       launch_stage x {1,2,4}  (stage.cu)
+//   pressure solve  launch_poisson_impl      (poisson.cu), repeated for the
+//                   variable-density fixed point (pressure.cu:551-606)
+//   end of step     launch_project           (project.cu)
+// with the state in two ping-pong buffers; nothing is allocated after wf_create.
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "wf_internal.h"
+
+namespace wf {
+size_t diag_scratch_bytes();
+
+static thread_local char g_err[1024];
+
+void set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+// ---- FFT plans: factorisation and tables (setup only) ---------------------
+bool stockham_factors(int m, int *fac, int &nfac)
+{
+    nfac = 0;
+    int r = m;
+    while (r % 4 == 0) { fac[nfac++] = 4; r /= 4; }
+    while (r % 2 == 0) { fac[nfac++] = 2; r /= 2; }
+    for (int p = 3; p <= 17 && r > 1; p += 2)
+        while (r % p == 0) { fac[nfac++] = p; r /= p; }
+    return r == 1 && nfac <= 20;
+}
+
+const long double kPiL = 3.141592653589793238462643383279502884L;
+
+struct HostFft {
+    FftDesc d;
+    std::vector<double2> tw, chirp, filt;
+};
+
+HostFft plan_fft(int n)
+{
+    HostFft h;
+    memset(&h.d, 0, sizeof(h.d));
+    h.d.n = n;
+    int fac[20], nf = 0;
+    if (n == 1) {
+        h.d.m = 1;
+        h.d.nfac = 0;
+    } else if (stockham_factors(n, fac, nf)) {
+        h.d.m = n;
+        h.d.nfac = nf;
+        memcpy(h.d.fac, fac, sizeof(int) * nf);
+    } else {
+        int m = 1;
+        while (m < 2 * n - 1) m <<= 1;
+        h.d.m = m;
+        h.d.bluestein = 1;
+        stockham_factors(m, fac, nf);
+        h.d.nfac = nf;
+        memcpy(h.d.fac, fac, sizeof(int) * nf);
+    }
+    const int m = h.d.m;
+    h.tw.resize(m);
+    for (int j = 0; j < m; j++) {
+        const long double a = -2.0L * kPiL * (long double)j / (long double)m;
+        h.tw[j] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    if (h.d.bluestein) {
+        std::vector<long double> cr(n), ci(n);
+        h.chirp.resize(n);
+        for (int j = 0; j < n; j++) {
+            const long long jj = ((long long)j * j) % (2LL * n);
+            const long double a = -kPiL * (long double)jj / (long double)n;
+            cr[j] = cosl(a);
+            ci[j] = sinl(a);
+            h.chirp[j] = make_double2((double)cr[j], (double)ci[j]);
+        }
+        // b_j = conj(chirp_j) on 0..n-1 and mirrored at m-j; filt = DFT_m(b),
+        // evaluated directly in long double (setup only)
+        std::vector<long double> br(m, 0.0L), bi(m, 0.0L), twr(m), twi(m);
+        for (int j = 0; j < n; j++) {
+            br[j] = cr[j];
+            bi[j] = -ci[j];
+            if (j > 0) {
+                br[m - j] = cr[j];
+                bi[m - j] = -ci[j];
+            }
+        }
+        for (int j = 0; j < m; j++) {
+            const long double a = -2.0L * kPiL * (long double)j / (long double)m;
+            twr[j] = cosl(a);
+            twi[j] = sinl(a);
+        }
+        h.filt.resize(m);
+        for (int q = 0; q < m; q++) {
+            long double sr = 0, si = 0;
+            for (int j = 0; j < m; j++) {
+                if (br[j] == 0.0L && bi[j] == 0.0L) continue;
+                const int e = (int)(((long long)j * q) % m);
+                sr += br[j] * twr[e] - bi[j] * twi[e];
+                si += br[j] * twi[e] + bi[j] * twr[e];
+            }
+            h.filt[q] = make_double2((double)sr, (double)si);
+        }
+    }
+    return h;
+}
+
+}  // namespace
+}  // namespace wf
+
+using namespace wf;
+
+struct wf_ctx {
+    Parameters P;
+    std::vector<double> hx, hy, hz, ht, hkx, hky, htopo, hzibm;
+    std::vector<int> hnzy, hcut;
+    int prec = 0;          // WF_FP64 / WF_FP32_STENCIL
+    int method = 2;        // 0 Euler, 1 RK2, 2 RK4
+    int nstages = 4;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int Nx, Ny, Nz, NzY, N, NY;
+    size_t S;              // packed state size (elements)
+    size_t esz;            // element size of the stencil state
+    std::vector<DevBuf> bufs;
+    void *ybuf[2] = {nullptr, nullptr};
+    int cur = 0;
+    void *Xa = nullptr, *Xb = nullptr, *acc = nullptr, *scr = nullptr, *utau = nullptr, *bc = nullptr;
+    void *Tsrc = nullptr;
+    double *p = nullptr, *p_prev = nullptr, *red = nullptr, *d_diag = nullptr;
+    double2 *G = nullptr;
+    double *d_z = nullptr, *d_zc = nullptr, *d_topo = nullptr, *d_kx2 = nullptr, *d_ky2 = nullptr, *d_zt = nullptr;
+    double *d_x = nullptr, *d_y = nullptr;
+    int *d_nzy = nullptr, *d_cut = nullptr;
+    FftDesc fx, fy;
+    Phys ph;
+    Geom geom;
+    int h1;
+    int n = 0;             // current time level
+    double fuel0 = 0.0;    // fuel integral at upload
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int launches = 0;
+    int last_iters = 0;
+};
+
+namespace wfs {
+
+wf_status dev_alloc(wf_ctx *c, void **out, size_t bytes)
+{
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+    if (e != cudaSuccess) {
+        set_error("device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+        cudaGetLastError();
+        return WF_ERR_OOM;
+    }
+    c->bufs.push_back(DevBuf{p, bytes});
+    *out = p;
+    return WF_OK;
+}
+
+template <class T> wf_status upload(wf_ctx *c, T **dst, const T *src, size_t n)
+{
+    wf_status s = dev_alloc(c, (void **)dst, n * sizeof(T));
+    if (s) return s;
+    WF_TRY_CUDA(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+    return WF_OK;
+}
+
+wf_status upload_fft(wf_ctx *c, const HostFft &h, FftDesc &d)
+{
+    d = h.d;
+    double2 *tw = nullptr, *ch = nullptr, *fl = nullptr;
+    wf_status s = upload(c, &tw, h.tw.data(), h.tw.size());
+    if (s) return s;
+    d.tw = tw;
+    if (h.d.bluestein) {
+        if ((s = upload(c, &ch, h.chirp.data(), h.chirp.size()))) return s;
+        if ((s = upload(c, &fl, h.filt.data(), h.filt.size()))) return s;
+        d.chirp = ch;
+        d.filt = fl;
+    }
+    return WF_OK;
+}
+
+// z-stencil weight table (see ZCoef); values of the reference's formulas.
+std::vector<double> zcoef_table(const Parameters &P, const double *z)
+{
+    const int Nz = P.Nz;
+    std::vector<double> t((size_t)ZCOUNT * Nz, 0.0);
+    auto at = [&](int e, int k) -> double & { return t[(size_t)e * Nz + k]; };
+    for (int k = 0; k < Nz; k++) {
+        if (k <= Nz - 3) {
+            const double a = z[k + 1] - z[k], b = z[k + 2] - z[k + 1];
+            at(ZF0, k) = -(2 * a + b) / (a * (a + b));
+            at(ZF1, k) = (a + b) / (a * b);
+            at(ZF2, k) = -a / (b * (a + b));
+        }
+        if (k >= 2) {
+            const double a1 = z[k] - z[k - 1], a2 = z[k - 1] - z[k - 2];
+            at(ZB0, k) = a1 / (a2 * (a2 + a1));
+            at(ZB1, k) = -(a2 + a1) / (a2 * a1);
+            at(ZB2, k) = (a2 + 2 * a1) / (a1 * (a2 + a1));
+        }
+        if (k > 0 && k < Nz - 1) {
+            const double a1 = z[k] - z[k - 1], a = z[k + 1] - z[k];
+            at(ZC, k) = 1.0 / (a1 + a);
+            at(ZCM, k) = 2 / (a1 * (a1 + a));
+            at(ZC0, k) = -2 / (a1 * a);
+            at(ZCP, k) = 2 / (a * (a1 + a));
+        }
+        const double dzk = (k < Nz - 1) ? z[k + 1] - z[k] : z[k] - z[k - 1];
+        at(ZDZ, k) = dzk;
+        at(ZDELTA2, k) = pow(P.C_s * pow(P.dx * P.dy * dzk, 1.0 / 3.0), 2.0);
+    }
+    {
+        const double a = z[1] - z[0], b = z[2] - z[1], cc = z[3] - z[2];
+        at(ZFF0, 0) = (6 * a + 4 * b + 2 * cc) / (a * (a + b) * (a + b + cc));
+        at(ZFF1, 0) = -(4 * a + 4 * b + 2 * cc) / (a * b * (b + cc));
+        at(ZFF2, 0) = (4 * a + 2 * b + 2 * cc) / (b * cc * (a + b));
+        at(ZFF3, 0) = -(4 * a + 2 * b) / (cc * (b + cc) * (a + b + cc));
+    }
+    {
+        const int k = Nz - 1;
+        const double a1 = z[k] - z[k - 1], a2 = z[k - 1] - z[k - 2], a3 = z[k - 2] - z[k - 3];
+        at(ZBB0, k) = -(2 * a2 + 4 * a1) / (a3 * (a3 + a2) * (a3 + a2 + a1));
+        at(ZBB1, k) = (2 * a3 + 2 * a2 + 4 * a1) / (a3 * a2 * (a2 + a1));
+        at(ZBB2, k) = -(2 * a3 + 4 * a2 + 4 * a1) / (a2 * a1 * (a3 + a2));
+        at(ZBB3, k) = (2 * a3 + 4 * a2 + 6 * a1) / (a1 * (a2 + a1) * (a3 + a2 + a1));
+    }
+    return t;
+}
+
+// Tridiagonal constants (pressure.cu:356-390; layout read by k_p_tridiag).
+std::vector<double> tridiag_table(const Parameters &P, const double *z)
+{
+    const int Nz = P.Nz, nk = Nz - 1;
+    std::vector<double> t((size_t)3 * nk + 5, 0.0);
+    for (int k = 0; k + 1 < nk; k++) {
+        const double dk = z[k + 1] - z[k], dkp1 = z[k + 2] - z[k + 1];
+        t[k] = 2 / (dk * (dk + dkp1));                       // a[k]
+    }
+    for (int k = 1; k + 1 < nk; k++) {
+        const double dkm1 = z[k] - z[k - 1], dk = z[k + 1] - z[k];
+        t[nk + k] = 2 / (dk * (dkm1 + dk));                  // c[k]
+    }
+    for (int k = 1; k < nk; k++) {
+        const double dkm1 = z[k] - z[k - 1], dk = z[k + 1] - z[k];
+        t[2 * nk + k] = 2 / (dkm1 * dk);                     // b[k] = -(kk + D[k])
+    }
+    const double dz0 = z[1] - z[0], dz1 = z[2] - z[1];
+    const double dzNm2 = z[Nz - 2] - z[Nz - 3], dzNm1 = z[Nz - 1] - z[Nz - 2];
+    t[3 * nk + 0] = -1.0 / dz0;                              // b[0]
+    t[3 * nk + 1] = (dz0 + dz1) / (dz0 * dz1);               // c[0] + 0.5 dz0 kk + 1/dz1
+    t[3 * nk + 2] = 1 / dz1;
+    t[3 * nk + 3] = 0.5 * dz0;
+    t[3 * nk + 4] = 2 / (dzNm1 * (dzNm2 + dzNm1));           // coupling of the top row
+    return t;
+}
+
+Phys make_phys(const Parameters &P)
+{
+    Phys ph;
+    memset(&ph, 0, sizeof(ph));
+    ph.dx = P.dx; ph.dy = P.dy; ph.dt = P.dt;
+    ph.mu = P.mu; ph.kT = P.k; ph.Y_f = P.Y_f; ph.H_C = P.H_C; ph.A = P.A; ph.T_act = P.T_act;
+    ph.T_pc = P.T_pc; ph.h_c = P.h_c; ph.alpha_s = P.alpha_s; ph.sigma_s = P.sigma_s;
+    ph.T_inf = P.T_inf; ph.c_p = P.c_p; ph.rho_inf = P.rho_inf; ph.C_d = P.C_d; ph.g = P.g;
+    ph.delta = P.delta; ph.Pr = P.Pr;
+    ph.T_min = P.T_min; ph.T_max = P.T_max; ph.Y_min = P.Y_min; ph.Y_max = P.Y_max;
+    ph.u_dead = P.u_dead_nodes; ph.v_dead = P.v_dead_nodes; ph.w_dead = P.w_dead_nodes;
+    ph.T_dead = P.T_dead_nodes; ph.Y_dead = P.Y_dead_nodes;
+    ph.temperature_convection = P.temperature_convection;
+    ph.sutherland_viscosity = P.sutherland_viscosity;
+    ph.sutherland_conductivity = P.sutherland_conductivity;
+    ph.variable_density = P.variable_density;
+    ph.velocity_correction_fd = P.velocity_correction_fd;
+    return ph;
+}
+
+template <class R> StageArgs<R> stage_args(wf_ctx *c, const void *X, const void *yn, void *Xout, int stage)
+{
+    StageArgs<R> a;
+    a.g = c->geom;
+    a.ph = c->ph;
+    a.X = (const R *)X;
+    a.yn = (const R *)yn;
+    a.acc = (R *)c->acc;
+    a.Xout = (R *)Xout;
+    a.scr = (R *)c->scr;
+    a.utau = (R *)c->utau;
+    a.bc = (R *)c->bc;
+    a.method = c->method;
+    a.stage = stage;
+    a.a_prev = 0.0;
+    const double dt = c->P.dt;
+    if (c->method == 0) a.a_next = dt;
+    else if (c->method == 1) a.a_next = (stage == 1) ? dt : 0.5 * dt;
+    else a.a_next = (stage == 1 || stage == 2) ? dt * 0.5 : (stage == 3) ? dt : dt / 6;
+    return a;
+}
+
+template <class R> PoissonArgs<R> poisson_args(wf_ctx *c, const void *y1, const void *yn)
+{
+    PoissonArgs<R> a;
+    a.g = c->geom;
+    a.ph = c->ph;
+    a.y1 = (const R *)y1;
+    a.yn = (const R *)yn;
+    a.p = c->p;
+    a.G = c->G;
+    a.kx2 = c->d_kx2;
+    a.ky2 = c->d_ky2;
+    a.fx = c->fx;
+    a.fy = c->fy;
+    a.h1 = c->h1;
+    return a;
+}
+
+// source mode of the step that produces time level n1 (solver.cu:217-223)
+int source_mode(const wf_ctx *c, int n1, double *scale)
+{
+    const double t1 = c->P.t_min + n1 * c->P.dt;
+    *scale = 1.0;
+    if (!(t1 <= c->P.t_source_end)) return 0;
+    if (c->P.t_source_start <= 0) return 1;
+    if (strcmp(c->P.T_source_shape, "gaussian") != 0 && strcmp(c->P.T_source_shape, "parallelepiped") != 0) return 0;
+    if (t1 <= c->P.t_source_start) *scale = t1 / c->P.t_source_start;
+    return 2;
+}
+
+template <class R> wf_status enqueue_stages(wf_ctx *c, void *yn, void *y1)
+{
+    cudaStream_t s = c->stream;
+    if (c->nstages == 1) {
+        WF_TRY_CUDA(launch_stage<R>(stage_args<R>(c, yn, yn, y1, 1), s));
+        return WF_OK;
+    }
+    if (c->nstages == 2) {
+        WF_TRY_CUDA(launch_stage<R>(stage_args<R>(c, yn, yn, c->Xa, 1), s));
+        WF_TRY_CUDA(launch_stage<R>(stage_args<R>(c, c->Xa, yn, y1, 2), s));
+        return WF_OK;
+    }
+    WF_TRY_CUDA(launch_stage<R>(stage_args<R>(c, yn, yn, c->Xa, 1), s));
+    WF_TRY_CUDA(launch_stage<R>(stage_args<R>(c, c->Xa, yn, c->Xb, 2), s));
+    WF_TRY_CUDA(launch_stage<R>(stage_args<R>(c, c->Xb, yn, c->Xa, 3), s));
+    WF_TRY_CUDA(launch_stage<R>(stage_args<R>(c, c->Xa, yn, y1, 4), s));
+    return WF_OK;
+}
+
+// Pressure solve(s) for y1 given yn.  For variable density the fixed point
+// stops on the max-norm change; that decision is taken on the host.
+template <class R> wf_status enqueue_pressure(wf_ctx *c, const void *y1, const void *yn, bool fixed_only, int *iters)
+{
+    cudaStream_t s = c->stream;
+    const PoissonArgs<R> a = poisson_args<R>(c, y1, yn);
+    if (c->P.variable_density == 0) {
+        WF_TRY_CUDA(launch_poisson_impl<R>(a, c->d_zt, s));
+        if (iters) *iters = 1;
+        return WF_OK;
+    }
+    const int maxit = c->P.pressure_solver_iter;
+    const bool use_tol = !fixed_only && c->P.pressure_solver_tol >= 0;
+    int m = 0;
+    for (m = 0; m < maxit; m++) {
+        if (use_tol) WF_TRY_CUDA(cudaMemcpyAsync(c->p_prev, c->p, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, s));
+        WF_TRY_CUDA(launch_poisson_impl<R>(a, c->d_zt, s));
+        if (use_tol) {
+            WF_TRY_CUDA(launch_maxdiff(c->p, c->p_prev, c->N, c->red, s));
+            double h = 0;
+            WF_TRY_CUDA(cudaMemcpyAsync(&h, c->red, sizeof(double), cudaMemcpyDeviceToHost, s));
+            WF_TRY_CUDA(cudaStreamSynchronize(s));
+            if (h <= c->P.pressure_solver_tol) { m++; break; }
+        }
+    }
+    if (iters) *iters = m;
+    return WF_OK;
+}
+
+template <class R> wf_status enqueue_step(wf_ctx *c, int cur, int n1, bool fixed_only)
+{
+    void *yn = c->ybuf[cur], *y1 = c->ybuf[1 - cur];
+    wf_status st = enqueue_stages<R>(c, yn, y1);
+    if (st) return st;
+    if ((st = enqueue_pressure<R>(c, y1, yn, fixed_only, &c->last_iters))) return st;
+    ProjectArgs<R> pa;
+    memset(&pa, 0, sizeof(pa));
+    pa.g = c->geom;
+    pa.ph = c->ph;
+    pa.y = (R *)y1;
+    pa.yn = (const R *)yn;
+    pa.p = c->p;
+    double scale;
+    pa.source_mode = source_mode(c, n1, &scale);
+    pa.src_scale = scale;
+    pa.Tsrc = (const R *)c->Tsrc;
+    if (pa.source_mode == 1 && !c->Tsrc) pa.source_mode = 0;
+    pa.t_n1 = c->P.t_min + n1 * c->P.dt;
+    pa.xg = c->d_x;
+    pa.yg = c->d_y;
+    memcpy(pa.TS, &c->P.TS_x_start, sizeof(pa.TS));
+    pa.TS_gauss = strcmp(c->P.T_source_shape, "gaussian") == 0;
+    pa.T_source = c->P.T_source;
+    WF_TRY_CUDA(launch_project<R>(pa, c->stream));
+    return WF_OK;
+}
+
+wf_status enqueue_step_any(wf_ctx *c, int cur, int n1, bool fixed_only)
+{
+    return c->prec == WF_FP64 ? enqueue_step<double>(c, cur, n1, fixed_only)
+                              : enqueue_step<float>(c, cur, n1, fixed_only);
+}
+
+// A step can be replayed from a graph when its launch sequence does not depend
+// on the time level or on host decisions.
+bool step_is_static(const wf_ctx *c, int n1)
+{
+    double sc;
+    if (source_mode(c, n1, &sc) != 0) return false;
+    if (c->P.variable_density != 0 && c->P.pressure_solver_tol >= 0) return false;
+    return true;
+}
+
+template <class R> __global__ void k_to_prec(R *dst, const double *src, size_t n)
+{
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+        dst[t] = (R)src[t];
+}
+template <class R> __global__ void k_from_prec(double *dst, const R *src, size_t n)
+{
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+        dst[t] = (double)src[t];
+}
+
+// host FP64 packed vector -> device buffer of the stencil precision
+wf_status put_state(wf_ctx *c, void *dst, const double *src)
+{
+    if (c->prec == WF_FP64) {
+        WF_TRY_CUDA(cudaMemcpyAsync(dst, src, c->S * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        return WF_OK;
+    }
+    // stage through the (double-sized) spectral buffer
+    double *tmp = reinterpret_cast<double *>(c->G);
+    size_t done = 0;
+    const size_t chunk = c->bufs.empty() ? 0 : c->G ? (size_t)(c->Nz) * (c->Nx - 1) * c->h1 * 2 : 0;
+    while (done < c->S) {
+        const size_t nn = (c->S - done < chunk) ? c->S - done : chunk;
+        WF_TRY_CUDA(cudaMemcpyAsync(tmp, src + done, nn * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        k_to_prec<float><<<592, 256, 0, c->stream>>>((float *)dst + done, tmp, nn);
+        WF_TRY_CUDA(cudaGetLastError());
+        done += nn;
+    }
+    return WF_OK;
+}
+
+wf_status get_state(wf_ctx *c, double *dst, const void *src)
+{
+    if (c->prec == WF_FP64) {
+        WF_TRY_CUDA(cudaMemcpyAsync(dst, src, c->S * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+        return WF_OK;
+    }
+    double *tmp = reinterpret_cast<double *>(c->G);
+    const size_t chunk = (size_t)(c->Nz) * (c->Nx - 1) * c->h1 * 2;
+    size_t done = 0;
+    while (done < c->S) {
+        const size_t nn = (c->S - done < chunk) ? c->S - done : chunk;
+        k_from_prec<float><<<592, 256, 0, c->stream>>>(tmp, (const float *)src + done, nn);
+        WF_TRY_CUDA(cudaGetLastError());
+        WF_TRY_CUDA(cudaMemcpyAsync(dst + done, tmp, nn * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+        done += nn;
+    }
+    return WF_OK;
+}
+
+void drop_graphs(wf_ctx *c)
+{
+    for (int q = 0; q < 2; q++)
+        if (c->graph[q]) {
+            cudaGraphExecDestroy(c->graph[q]);
+            c->graph[q] = nullptr;
+        }
+}
+
+}  // namespace wfs
+
+using namespace wfs;
+
+// ===========================================================================
+extern "C" {
+
+const char *wf_last_error(void) { return g_err; }
+
+const char *wf_status_string(wf_status s)
+{
+    switch (s) {
+    case WF_OK: return "ok";
+    case WF_ERR_ARG: return "invalid argument";
+    case WF_ERR_CUDA: return "CUDA error";
+    case WF_ERR_IO: return "I/O error";
+    case WF_ERR_PARSE: return "parse error";
+    case WF_ERR_OOM: return "out of memory";
+    case WF_ERR_NAN: return "NaN in state";
+    case WF_ERR_NO_DEVICE: return "no sm_100 device";
+    }
+    return "unknown status";
+}
+
+wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
+{
+    if (!P || !out) { set_error("wf_create: null argument"); return WF_ERR_ARG; }
+    *out = nullptr;
+    if (precision != WF_FP64 && precision != WF_FP32_STENCIL) { set_error("wf_create: unknown precision %d", precision); return WF_ERR_ARG; }
+    const int Nx = P->Nx, Ny = P->Ny, Nz = P->Nz;
+    if (Nx < 4 || Ny < 4 || Nz < 5) { set_error("wf_create: grid %dx%dx%d too small (need Nx,Ny >= 4, Nz >= 5)", Nx, Ny, Nz); return WF_ERR_ARG; }
+    if (Nx - 1 > kMaxFftLength || Ny - 1 > kMaxFftLength) { set_error("wf_create: Nx-1 and Ny-1 must be <= %d", kMaxFftLength); return WF_ERR_ARG; }
+    if (Nz - 1 > kMaxZUnknowns) { set_error("wf_create: Nz-1 must be <= %d", kMaxZUnknowns); return WF_ERR_ARG; }
+    if ((long long)Nx * Ny * Nz * 5 > 2000000000LL) { set_error("wf_create: grid too large for 32-bit cell indices"); return WF_ERR_ARG; }
+    if (!P->z || !P->Nz_Y || !P->cut_nodes || !P->kx || !P->ky || !P->topography || !P->x || !P->y) {
+        set_error("wf_create: derived arrays missing (use wf_read_parameters)");
+        return WF_ERR_ARG;
+    }
+    for (int q = 0; q < Nx * Ny; q++)
+        if (P->cut_nodes[q] < 0 || P->cut_nodes[q] > Nz - 4) {
+            set_error("wf_create: terrain cut node %d in column %d is above Nz-4 = %d", P->cut_nodes[q], q, Nz - 4);
+            return WF_ERR_ARG;
+        }
+    int dev = 0, cc_major = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&cc_major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("wf_create: no CUDA device");
+        return WF_ERR_NO_DEVICE;
+    }
+    if (cc_major != 10) { set_error("wf_create: device %d is sm_%d0, this build targets sm_100a", dev, cc_major); return WF_ERR_NO_DEVICE; }
+
+    wf_ctx *c = new wf_ctx();
+    c->P = *P;
+    c->device = dev;
+    c->prec = precision;
+    c->Nx = Nx; c->Ny = Ny; c->Nz = Nz; c->NzY = P->Nz_Y_max;
+    c->N = Nx * Ny * Nz;
+    c->NY = Nx * Ny * c->NzY;
+    c->S = (size_t)4 * c->N + c->NY;
+    c->esz = precision == WF_FP64 ? 8 : 4;
+    if (strncmp(P->method, "Euler", 5) == 0) { c->method = 0; c->nstages = 1; }
+    else if (strncmp(P->method, "RK2", 3) == 0) { c->method = 1; c->nstages = 2; }
+    else if (strncmp(P->method, "RK4", 3) == 0) { c->method = 2; c->nstages = 4; }
+    else { delete c; set_error("wf_create: time integration method '%s' not found", P->method); return WF_ERR_ARG; }
+    // host copies of the arrays the record points to
+    c->hx.assign(P->x, P->x + Nx);
+    c->hy.assign(P->y, P->y + Ny);
+    c->hz.assign(P->z, P->z + Nz);
+    c->hkx.assign(P->kx, P->kx + Nx - 1);
+    c->hky.assign(P->ky, P->ky + Ny - 1);
+    c->htopo.assign(P->topography, P->topography + (size_t)Nx * Ny);
+    c->hnzy.assign(P->Nz_Y, P->Nz_Y + (size_t)Nx * Ny);
+    c->hcut.assign(P->cut_nodes, P->cut_nodes + (size_t)Nx * Ny);
+    c->P.x = c->hx.data(); c->P.y = c->hy.data(); c->P.z = c->hz.data();
+    c->P.kx = c->hkx.data(); c->P.ky = c->hky.data(); c->P.topography = c->htopo.data();
+    c->P.Nz_Y = c->hnzy.data(); c->P.cut_nodes = c->hcut.data();
+    c->P.t = nullptr; c->P.r = nullptr; c->P.s = nullptr; c->P.z_ibm = nullptr;
+    c->P.log_files.parameters = nullptr; c->P.log_files.log = nullptr;
+    c->h1 = (Ny - 1) / 2 + 1;
+
+    wf_status st = WF_OK;
+    auto fail = [&](wf_status s) { wf_destroy(c); return s; };
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error("wf_create: stream creation failed");
+        delete c;
+        return WF_ERR_CUDA;
+    }
+    const size_t sb = c->S * c->esz;
+    if ((st = dev_alloc(c, &c->ybuf[0], sb)) || (st = dev_alloc(c, &c->ybuf[1], sb))) return fail(st);
+    if (c->nstages > 1) {
+        if ((st = dev_alloc(c, &c->Xa, sb)) || (st = dev_alloc(c, &c->acc, sb))) return fail(st);
+        if (c->nstages > 2 && (st = dev_alloc(c, &c->Xb, sb))) return fail(st);
+    }
+    if ((st = dev_alloc(c, &c->scr, (size_t)kScratchFields * c->N * c->esz))) return fail(st);
+    if ((st = dev_alloc(c, &c->utau, (size_t)Nx * Ny * c->esz))) return fail(st);
+    if ((st = dev_alloc(c, &c->bc, (size_t)Nx * Ny * kBcSlots * c->esz))) return fail(st);
+    if ((st = dev_alloc(c, (void **)&c->p, sizeof(double) * c->N))) return fail(st);
+    if ((st = dev_alloc(c, (void **)&c->p_prev, sizeof(double) * c->N))) return fail(st);
+    if ((st = dev_alloc(c, (void **)&c->G, sizeof(double2) * (size_t)Nz * (Nx - 1) * c->h1))) return fail(st);
+    if ((st = dev_alloc(c, (void **)&c->red, 64))) return fail(st);
+    if ((st = dev_alloc(c, (void **)&c->d_diag, diag_scratch_bytes()))) return fail(st);
+    // tables
+    std::vector<double> zc = zcoef_table(c->P, c->hz.data()), zt = tridiag_table(c->P, c->hz.data());
+    std::vector<double> kx2(Nx - 1), ky2(Ny - 1);
+    for (int i = 0; i < Nx - 1; i++) kx2[i] = c->hkx[i] * c->hkx[i];
+    for (int j = 0; j < Ny - 1; j++) ky2[j] = c->hky[j] * c->hky[j];
+    if ((st = upload(c, &c->d_z, c->hz.data(), Nz)) || (st = upload(c, &c->d_zc, zc.data(), zc.size())) ||
+        (st = upload(c, &c->d_zt, zt.data(), zt.size())) || (st = upload(c, &c->d_kx2, kx2.data(), kx2.size())) ||
+        (st = upload(c, &c->d_ky2, ky2.data(), ky2.size())) || (st = upload(c, &c->d_topo, c->htopo.data(), c->htopo.size())) ||
+        (st = upload(c, &c->d_nzy, c->hnzy.data(), c->hnzy.size())) || (st = upload(c, &c->d_cut, c->hcut.data(), c->hcut.size())) ||
+        (st = upload(c, &c->d_x, c->hx.data(), Nx)) || (st = upload(c, &c->d_y, c->hy.data(), Ny)))
+        return fail(st);
+    const HostFft hfx = plan_fft(Nx - 1), hfy = plan_fft(Ny - 1);
+    if ((st = upload_fft(c, hfx, c->fx)) || (st = upload_fft(c, hfy, c->fy))) return fail(st);
+    if (P->t_source_end > P->t_min && P->t_source_start <= 0)
+        if ((st = dev_alloc(c, &c->Tsrc, (size_t)c->N * c->esz))) return fail(st);
+    c->geom.Nx = Nx; c->geom.Ny = Ny; c->geom.Nz = Nz; c->geom.NzY = c->NzY;
+    c->geom.N = c->N; c->geom.NY = c->NY;
+    c->geom.z = c->d_z; c->geom.zc = c->d_zc; c->geom.topo = c->d_topo;
+    c->geom.nzy = c->d_nzy; c->geom.cut = c->d_cut;
+    c->ph = make_phys(c->P);
+    cudaError_t e = (precision == WF_FP64) ? poisson_set_attributes<double>() : poisson_set_attributes<float>();
+    if (e != cudaSuccess) { set_error("wf_create: %s", cudaGetErrorString(e)); return fail(WF_ERR_CUDA); }
+    WF_TRY_CUDA(cudaMemsetAsync(c->p, 0, sizeof(double) * c->N, c->stream));
+    WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+    c->launches = c->nstages * 3 + 5 + 1;
+    *out = c;
+    return WF_OK;
+}
+
+wf_status wf_destroy(wf_ctx *c)
+{
+    if (!c) return WF_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+    for (auto &b : c->bufs) cudaFree(b.p);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return WF_OK;
+}
+
+wf_status wf_upload_state(wf_ctx *c, const double *y, const double *pr)
+{
+    if (!c || !y || !pr) { set_error("wf_upload_state: null argument"); return WF_ERR_ARG; }
+    c->cur = 0;
+    c->n = 0;
+    wf_status st = put_state(c, c->ybuf[0], y);
+    if (st) return st;
+    WF_TRY_CUDA(cudaMemcpyAsync(c->p, pr, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
+    if (c->Tsrc) {
+        // the held source is the initial temperature field (solver.cu:169)
+        WF_TRY_CUDA(cudaMemcpyAsync(c->Tsrc, (char *)c->ybuf[0] + (size_t)3 * c->N * c->esz, (size_t)c->N * c->esz,
+                                    cudaMemcpyDeviceToDevice, c->stream));
+    }
+    WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+    wf_diag d;
+    st = wf_diagnostics(c, &d);
+    c->fuel0 = d.fuel;
+    return st == WF_ERR_NAN ? WF_OK : st;
+}
+
+wf_status wf_download_state(wf_ctx *c, double *y, double *pr)
+{
+    if (!c || !y || !pr) { set_error("wf_download_state: null argument"); return WF_ERR_ARG; }
+    wf_status st = get_state(c, y, c->ybuf[c->cur]);
+    if (st) return st;
+    WF_TRY_CUDA(cudaMemcpyAsync(pr, c->p, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
+    WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+    return WF_OK;
+}
+
+wf_status wf_step(wf_ctx *c, int nsteps)
+{
+    if (!c || nsteps < 0) { set_error("wf_step: invalid argument"); return WF_ERR_ARG; }
+    for (int q = 0; q < nsteps; q++) {
+        const int n1 = c->n + 1;
+        if (step_is_static(c, n1)) {
+            cudaGraphExec_t &ge = c->graph[c->cur];
+            if (!ge) {
+                cudaGraph_t gph;
+                WF_TRY_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+                wf_status st = enqueue_step_any(c, c->cur, n1, true);
+                cudaError_t e = cudaStreamEndCapture(c->stream, &gph);
+                if (st) return st;
+                if (e != cudaSuccess) { set_error("wf_step: capture failed: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
+                e = cudaGraphInstantiate(&ge, gph, 0);
+                cudaGraphDestroy(gph);
+                if (e != cudaSuccess) { set_error("wf_step: instantiate failed: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
+            }
+            WF_TRY_CUDA(cudaGraphLaunch(ge, c->stream));
+        } else {
+            wf_status st = enqueue_step_any(c, c->cur, n1, false);
+            if (st) return st;
+        }
+        c->cur = 1 - c->cur;
+        c->n = n1;
+    }
+    return WF_OK;
+}
+
+wf_status wf_synchronize(wf_ctx *c)
+{
+    if (!c) return WF_ERR_ARG;
+    WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+    return WF_OK;
+}
+
+wf_status wf_time(const wf_ctx *c, int *n, double *t)
+{
+    if (!c) return WF_ERR_ARG;
+    if (n) *n = c->n;
+    if (t) *t = c->P.t_min + c->n * c->P.dt;
+    return WF_OK;
+}
+
+wf_status wf_diagnostics(wf_ctx *c, wf_diag *out)
+{
+    if (!c || !out) return WF_ERR_ARG;
+    cudaError_t e = (c->prec == WF_FP64)
+                        ? launch_diag<double>(c->geom, c->ph, (const double *)c->ybuf[c->cur], nullptr, c->d_diag, c->stream)
+                        : launch_diag<float>(c->geom, c->ph, (const float *)c->ybuf[c->cur], nullptr, c->d_diag, c->stream);
+    if (e != cudaSuccess) { set_error("wf_diagnostics: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
+    double h[13];
+    WF_TRY_CUDA(cudaMemcpyAsync(h, c->d_diag, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+    out->mass = h[0];
+    out->energy = h[1];
+    out->fuel = h[2];
+    out->fuel_consumed = c->fuel0 - h[2];
+    out->max_abs_u = h[4];
+    out->max_abs_v = h[5];
+    out->max_abs_w = h[6];
+    out->T_min = -h[7];
+    out->T_max = h[8];
+    out->Y_min = -h[9];
+    out->Y_max = h[10];
+    out->nan_count = (long long)h[12];
+    out->cfl = c->P.dt * (h[4] / c->P.dx + h[5] / c->P.dy + h[6] / c->P.dz);
+    return out->nan_count ? WF_ERR_NAN : WF_OK;
+}
+
+wf_status wf_device_state(wf_ctx *c, void **y, double **pr)
+{
+    if (!c) return WF_ERR_ARG;
+    if (y) *y = c->ybuf[c->cur];
+    if (pr) *pr = c->p;
+    return WF_OK;
+}
+
+void *wf_stream(wf_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int wf_launches_per_step(const wf_ctx *c) { return c ? c->launches : 0; }
+
+wf_status wf_phi(wf_ctx *c, const double *R_old, double *R_new)
+{
+    if (!c || !R_old || !R_new) { set_error("wf_phi: null argument"); return WF_ERR_ARG; }
+    void *in = c->ybuf[1 - c->cur], *outb = c->Xa ? c->Xa : c->ybuf[c->cur];
+    wf_status st = put_state(c, in, R_old);
+    if (st) return st;
+    const int saved = c->method;
+    c->method = 3;
+    cudaError_t e;
+    if (c->prec == WF_FP64) e = launch_stage<double>(stage_args<double>(c, in, in, outb, 1), c->stream);
+    else e = launch_stage<float>(stage_args<float>(c, in, in, outb, 1), c->stream);
+    c->method = saved;
+    if (e != cudaSuccess) { set_error("wf_phi: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
+    // fuel entries above each column's fuel top are never written: zero them
+    st = get_state(c, R_new, outb);
+    if (st) return st;
+    for (int col = 0; col < c->Nx * c->Ny; col++)
+        for (int k = c->hnzy[col]; k < c->NzY; k++) R_new[(size_t)4 * c->N + (size_t)col * c->NzY + k] = 0.0;
+    drop_graphs(c);
+    return WF_OK;
+}
+
+wf_status wf_pressure(wf_ctx *c, const double *y_np1, const double *y_n, double *pr, int *iters)
+{
+    if (!c || !y_np1 || !y_n || !pr) { set_error("wf_pressure: null argument"); return WF_ERR_ARG; }
+    void *b1 = c->ybuf[1 - c->cur], *bn = c->Xa ? c->Xa : c->ybuf[c->cur];
+    wf_status st = put_state(c, b1, y_np1);
+    if (st) return st;
+    if ((st = put_state(c, bn, y_n))) return st;
+    WF_TRY_CUDA(cudaMemcpyAsync(c->p, pr, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
+    int it = 0;
+    st = (c->prec == WF_FP64) ? enqueue_pressure<double>(c, b1, bn, false, &it) : enqueue_pressure<float>(c, b1, bn, false, &it);
+    if (st) return st;
+    WF_TRY_CUDA(cudaMemcpyAsync(pr, c->p, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
+    WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+    if (iters) *iters = it;
+    drop_graphs(c);
+    return WF_OK;
+}
+
+}  // extern "C"

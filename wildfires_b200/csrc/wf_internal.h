@@ -1,0 +1,147 @@
+// wf_internal.h -- definitions shared by the host code and the CUDA kernels of
+// the B200 solver.  Not part of the public interface.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/wildfires_b200.h"
+
+namespace wf {
+
+// Records a formatted message for wf_last_error() on this host thread.
+void set_error(const char *fmt, ...);
+
+#define WF_TRY_CUDA(call)                                                                  \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            ::wf::set_error("%s:%d: %s failed: %s", __FILE__, __LINE__, #call,             \
+                            cudaGetErrorString(e_));                                       \
+            return WF_ERR_CUDA;                                                            \
+        }                                                                                  \
+    } while (0)
+
+// Per-k z-stencil weights on the non-uniform grid, one row of Nz doubles per
+// entry.  They are the reference's finite-difference formulas with the
+// division folded into a weight (src/cu/pde.cu:363-576, turbulence.cu:344-427).
+enum ZCoef {
+    ZF0, ZF1, ZF2,          // forward 1st derivative at k: weights of k, k+1, k+2  (k <= Nz-3)
+    ZB0, ZB1, ZB2,          // backward 1st derivative at k: weights of k-2, k-1, k (k >= 2)
+    ZC,                     // 1 / (dz_{k-1} + dz_k)                                (0 < k < Nz-1)
+    ZCM, ZC0, ZCP,          // central 2nd derivative: weights of k-1, k, k+1       (0 < k < Nz-1)
+    ZFF0, ZFF1, ZFF2, ZFF3, // forward 2nd derivative at k = 0: weights of 0..3
+    ZBB0, ZBB1, ZBB2, ZBB3, // backward 2nd derivative at k = Nz-1: weights of Nz-4..Nz-1
+    ZDZ,                    // dz_k = z[k+1]-z[k] (k < Nz-1), z[k]-z[k-1] at the top
+    ZDELTA2,                // (C_s (dx dy dz_k)^(1/3))^2, the Smagorinsky length squared
+    ZCOUNT
+};
+
+// Scalars of the model used on the device (reference Parameters members).
+struct Phys {
+    double dx, dy, dt;
+    double mu, kT, Y_f, H_C, A, T_act, T_pc, h_c, alpha_s, sigma_s;
+    double T_inf, c_p, rho_inf, C_d, g, delta, Pr;
+    double T_min, T_max, Y_min, Y_max;
+    double u_dead, v_dead, w_dead, T_dead, Y_dead;
+    int temperature_convection, sutherland_viscosity, sutherland_conductivity;
+    int variable_density, velocity_correction_fd;
+};
+
+// Grid geometry and immersed-boundary tables (device pointers).
+struct Geom {
+    int Nx, Ny, Nz, NzY;        // NzY = Nz_Y_max
+    int N;                      // Nx*Ny*Nz
+    int NY;                     // Nx*Ny*NzY
+    const double *z;            // [Nz]
+    const double *zc;           // [ZCOUNT][Nz]
+    const double *topo;         // [Nx*Ny] terrain height (z_ibm = max(z_k - topo, 0))
+    const int *nzy;             // [Nx*Ny] fuel-storage height per column
+    const int *cut;             // [Nx*Ny] cut node per column
+};
+
+// Number of turbulence-input fields kept between the two stage passes:
+// raw mu_sgs, S11, S12, S13, S22, S23, S33 and the divergence source divU.
+constexpr int kScratchFields = 8;
+// Per-column values the boundary pass needs from the stage pass:
+// T,Y at cut+1, cut+2 (4) and u,v,w,T at Nz-2, Nz-3 (8).
+constexpr int kBcSlots = 12;
+
+template <class R>
+struct StageArgs {
+    Geom g;
+    Phys ph;
+    const R *X;      // stage input state (packed)
+    const R *yn;     // state at the start of the step (packed)
+    R *acc;          // RK accumulator of k-values (packed)
+    R *Xout;         // next stage input, or y_{n+1} after the last stage
+    R *scr;          // [kScratchFields][N]
+    R *utau;         // [Nx*Ny] wall friction velocity from the k = 0 plane
+    R *bc;           // [Nx*Ny][kBcSlots]
+    double a_next;   // c_{s+1} dt of the next stage input, or dt/6 after the last stage
+    double a_prev;   // Euler/RK2 weights (see stage.cu)
+    int method;      // 0 Euler, 1 RK2, 2 RK4, 3 = store k_s itself (operator tests)
+    int stage;       // 1-based stage index
+};
+
+// Launch helpers implemented in the .cu files.
+template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t s);
+
+template <class R>
+struct ProjectArgs {
+    Geom g;
+    Phys ph;
+    R *y;                  // y_{n+1} (packed), updated in place
+    const R *yn;           // y_n (packed), density for variable density
+    const double *p;       // pressure [N]
+    const R *Tsrc;         // initial temperature field or nullptr
+    int source_mode;       // 0 none, 1 hold initial field, 2 ramped shape
+    double t_n1;           // time of the new level (ramped source)
+    double src_scale;      // ramp factor t/t_source_start (ramped source)
+    const double *xg, *yg; // coordinates (ramped source)
+    double TS[12];         // source box/gaussian parameters (ramped source)
+    int TS_gauss;
+    double T_source;
+};
+template <class R> cudaError_t launch_project(const ProjectArgs<R> &a, cudaStream_t s);
+
+// ---- pressure -------------------------------------------------------------
+// FFT descriptor for one transform length, tables in device memory.
+struct FftDesc {
+    int n;                  // transform length
+    int m;                  // inner (Stockham) length: n, or the Bluestein length
+    int bluestein;
+    int nfac;
+    int fac[20];            // radices of m, applied in order
+    const double2 *tw;      // exp(-2 pi i j / m), j < m
+    const double2 *chirp;   // Bluestein: exp(-i pi j^2 / n), j < n
+    const double2 *filt;    // Bluestein: FFT_m of the conjugate chirp filter
+};
+
+template <class R>
+struct PoissonArgs {
+    Geom g;
+    Phys ph;
+    const R *y1;            // y_{n+1} (packed) -- velocity, T, Y
+    const R *yn;            // y_n (packed) -- density for variable density
+    double *p;              // pressure [N], read (top plane, previous iterate) and written
+    double2 *G;             // spectral buffer [(Nz-1)+1][Nx-1][h1], s fastest
+    const double *kx2;      // [Nx-1] kx^2
+    const double *ky2;      // [Ny-1] ky^2
+    FftDesc fx, fy;         // x: length Nx-1, y: length Ny-1
+    int h1;                 // (Ny-1)/2 + 1
+};
+// zt: tridiagonal constants per k (layout documented at k_p_tridiag).
+template <class R> cudaError_t launch_poisson_impl(const PoissonArgs<R> &a, const double *zt, cudaStream_t s);
+template <class R> cudaError_t poisson_set_attributes();
+int poisson_pairs_per_block(int m);
+int poisson_lines_per_block(int m);
+constexpr int kMaxFftLength = 2048;     // longest supported x or y transform
+constexpr int kMaxZUnknowns = 256;      // longest supported tridiagonal system (Nz-1)
+
+// Grid-wide FP64 reductions for the diagnostics and the pressure fixed point.
+template <class R>
+cudaError_t launch_diag(const Geom &g, const Phys &ph, const R *y, const R *y0fuel_ref, double *out, cudaStream_t s);
+cudaError_t launch_maxdiff(const double *a, const double *b, int n, double *out, cudaStream_t s);
+
+}  // namespace wf
