@@ -1,0 +1,418 @@
+"""Throughput of the coupled atmosphere-wildfire time step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config hills8|hill|flat] [--precision fp32|fp64]
+
+Metric: Mcell-steps/s = (Nx*Ny*Nz stored nodes) x steps / time.  A step is one
+full RK4 time step (4 RHS stages, FP64 pressure Poisson solve, projection,
+boundary rules, clamps) over the whole grid.  Default workload: the
+mixed-precision configuration, 512 x 512 x 128 with 8 seeded hills, FP32
+stencil + FP64 pressure (`hills8`); the plain FP64 path on the same grid is
+timed beside it.  Data are seeded synthetic fields (no dataset exists for this
+model).  The state (670 MB FP32, 1.3 GB FP64) is larger than the 126 MB L2,
+so no explicit L2 flush is needed between timed steps.
+
+Under torchrun (N > 1) every rank advances its own replica of the workload
+(the single-domain step does not shard) and the reported value
+is the aggregate over ranks, timed as the max over ranks.
+
+--impl reference times the reference's own CPU implementation (its src/cu
+sources compiled for the host by oracle/Makefile, OpenMP over its virtual
+threads) on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="hills8", choices=["hills8", "hill", "flat"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    return ap.parse_args()
+
+
+def build_case(name, **kw):
+    from wildfires_b200 import configs, read_parameters
+    case = configs.CASES[name](**kw)
+    d = tempfile.mkdtemp(prefix="wf_bench_")
+    path = os.path.join(d, "parameters.txt")
+    with open(path, "w") as f:
+        f.write(configs.param_text(case.params))
+    P = read_parameters(path)
+    topo = case.topography(P)
+    if topo is not None:
+        P.set_topography(topo)
+    y0, p0 = case.fields(P)
+    return case, P, y0, p0
+
+
+def workload_name(name, P, prec):
+    r = P.rec
+    form = "FP32 stencil + FP64 Poisson" if prec == "fp32" else "plain FP64"
+    desc = {"hills8": "8 seeded gaussian hills", "hill": "single gaussian hill", "flat": "flat terrain"}[name]
+    return "%s %dx%dx%d, %s, %s, RK4 dt=%g s" % (name, r.Nx, r.Ny, r.Nz, desc, form, r.dt)
+
+
+# ---- clocks sampled during the timed region ----------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.out.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---- algorithmic bytes (roofline model) -------------------------------------
+def kernel_bytes(name, P, prec):
+    """Compulsory DRAM bytes per launch of each kernel kind."""
+    r = P.rec
+    N = r.Nx * r.Ny * r.Nz
+    NY = r.Nx * r.Ny * r.Nz_Y_max
+    s = 4 if prec == "fp32" else 8
+    S = 4 * N + NY
+    h1 = (r.Ny - 1) // 2 + 1
+    G = (r.Nz) * (r.Nx - 1) * h1 * 16          # spectral slab incl. the top-plane slice
+    return {
+        # read X (state) + write 8 SGS-input fields
+        "turb_inputs": s * S + 8 * s * N,
+        # read X, SGS inputs, y_n, acc; write acc, X_next (stage 2/3 form)
+        "stage_rhs": s * S + 8 * s * N + 4 * s * S,
+        "stage_bc": 0,
+        # read u, v, w (+ top plane of p); write half spectrum
+        "p_rhs_ffty": 3 * s * N + G,
+        "p_fftx_fwd": 2 * G,
+        "p_tridiag": 2 * G,
+        "p_fftx_inv": 2 * G,
+        # read half spectrum, write p
+        "p_iffty_out": G + 8 * N,
+        # read p, u, v, w, T, Y; write u, v, w
+        "project": 8 * N + s * S + 3 * s * N,
+    }.get(name, 0)
+
+
+def step_model_bytes(P, prec):
+    """Algorithmic bytes per cell-step of the whole step (SURVEY model)."""
+    r = P.rec
+    s = 4 if prec == "fp32" else 8
+    fY = r.Nz_Y_max / r.Nz
+    return 17 * s * (4 + fY) + 3 * s + 152 + (8 + 6 * s)
+
+
+def peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_table():
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ---- CPU reference ------------------------------------------------------------
+def cpu_reference_sample(case_name, target_s=20.0, steps=None):
+    """Time the reference's own solver on the host cores on a bounded sample of
+    the workload (same spacing and physics, fewer cells)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner
+    from wildfires_b200 import configs
+    if not ref_runner.available("host"):
+        return None
+    cores = os.cpu_count()
+    # calibrate on a small grid, then size the sample for ~target_s seconds
+    cal = configs.CASES[case_name](**_sample_kw(case_name, 64, 2))
+    r = ref_runner.run(cal, "time", parallel=True)
+    rate = 64 * 64 * _nz(case_name) * 2 / r["seconds"]          # cell-steps per second
+    nsteps = steps or 2
+    n = 64
+    while (2 * n) ** 2 * _nz(case_name) * nsteps / rate <= target_s and 2 * n <= _full_n(case_name):
+        n *= 2
+    case = configs.CASES[case_name](**_sample_kw(case_name, n, nsteps))
+    r = ref_runner.run(case, "time", parallel=True)
+    cells = n * n * _nz(case_name)
+    return {"value": cells * nsteps / r["seconds"] / 1e6, "unit": METRIC, "cores": cores, "kind": "reference",
+            "sample": "%s workload at %dx%dx%d (same spacing), %d steps, %.1f s" % (case_name, n, n, _nz(case_name), nsteps, r["seconds"]),
+            "seconds": r["seconds"], "steps": nsteps}
+
+
+def _nz(name):
+    return {"hills8": 128, "hill": 128, "flat": 64}[name]
+
+
+def _full_n(name):
+    return {"hills8": 512, "hill": 256, "flat": 128}[name]
+
+
+def _sample_kw(name, n, nsteps):
+    full = _full_n(name)
+    L = {"hills8": 800.0, "hill": 400.0, "flat": 200.0}[name] * (n - 1) / (full - 1)
+    kw = dict(Nx=n, Ny=n, Nt=nsteps)
+    if name in ("hills8", "hill"):
+        kw["L"] = L
+    return kw
+
+
+# ---- GPU arm --------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from wildfires_b200 import Solver
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    case, P, y0, p0 = build_case(args.config)
+    r = P.rec
+    cells = r.Nx * r.Ny * r.Nz
+    K, W = args.steps, args.warmup
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_steps(solver, K, clocks=None):
+        stream = torch.cuda.ExternalStream(solver.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        solver.synchronize()
+        if clocks:
+            clocks.start()
+        e0.record(stream)
+        solver.step(K)
+        e1.record(stream)
+        solver.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        info = clocks.stop() if clocks else None
+        return e0.elapsed_time(e1), info
+
+    res = {}
+    sol = Solver(P, args.precision)
+    sol.upload(y0, p0)
+    sol.step(W)
+    sol.synchronize()
+    clocks = ClockSampler(dev)
+    ms, clk = timed_steps(sol, K, clocks)
+    ms = max_over_ranks(ms)
+    ms_step = ms / K
+    value = cells * K * world / (ms * 1e-3) / 1e6
+    launches = sol.launches_per_step() * K
+
+    # per-kernel device times (eager launches with events on the solver stream)
+    prof = sol.profile(2)
+    total = sum(t for t, n in prof.values())
+    dom = max(prof, key=lambda k: prof[k][0])
+    t_dom, n_dom = prof[dom]
+    avg_ms = t_dom / max(n_dom, 1)
+    peak, peak_kind = peak_hbm()
+    bytes_dom = kernel_bytes(dom, P, args.precision)
+    achieved = bytes_dom / (avg_ms * 1e-3) / 1e9
+    traf = traffic_table().get("%s/%s/%s" % (args.config, args.precision, dom))
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traf, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": bytes_dom, "avg_launch_ms": round(avg_ms, 4),
+                "share_of_step": round(t_dom / total, 4)}
+    model = step_model_bytes(P, args.precision)
+    step_roof = {"bytes_per_cell_step": round(model, 1),
+                 "achieved_GBps": round(model * cells / (ms_step * 1e-3) / 1e9, 1)}
+    step_roof["frac"] = round(step_roof["achieved_GBps"] / peak, 4)
+    kernels = {k: {"ms_per_launch": round(t / max(n, 1), 4), "launches": n, "share": round(t / total, 4)}
+               for k, (t, n) in prof.items()}
+    y_fp32, _ = sol.download()
+    steps_done = sol.time()[0]
+
+    # end to end through the C-ABI with host buffers: H2D state, one step, D2H state
+    pin_y = torch.empty(sol.S, dtype=torch.float64, pin_memory=True).numpy()
+    pin_p = torch.empty(sol.N, dtype=torch.float64, pin_memory=True).numpy()
+    pin_y[:] = y0
+    pin_p[:] = p0
+    from wildfires_b200 import _abi
+    import ctypes as C
+    L = _abi.lib()
+    dp = C.POINTER(C.c_double)
+    py, pp = pin_y.ctypes.data_as(dp), pin_p.ctypes.data_as(dp)
+    ke = max(3, min(K, 10))
+    for _ in range(2):
+        _abi.check(L.wf_upload_state(sol._h, py, pp), "upload")
+        _abi.check(L.wf_step(sol._h, 1), "step")
+        _abi.check(L.wf_download_state(sol._h, py, pp), "download")
+    pin_y[:] = y0
+    pin_p[:] = p0
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        _abi.check(L.wf_upload_state(sol._h, py, pp), "upload")
+        _abi.check(L.wf_step(sol._h, 1), "step")
+        _abi.check(L.wf_download_state(sol._h, py, pp), "download")
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    h2d = sol.S * 8 + sol.N * 8
+    e2e = {"value": round(cells * ke * world / e2e_s / 1e6, 2), "unit": METRIC,
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
+           "note": "per step: upload of the FP64 packed state and p from pinned host memory, one step, download"}
+    sol.close()
+
+    # plain FP64 path on the same workload
+    fp64 = None
+    if not args.no_fp64 and args.precision == "fp32":
+        s64 = Solver(P, "fp64")
+        s64.upload(y0, p0)
+        s64.step(W)
+        s64.synchronize()
+        ms64, _ = timed_steps(s64, K)
+        ms64 = max_over_ranks(ms64)
+        # bring the FP64 run to the same time level as the FP32 state
+        n64 = s64.time()[0]
+        if n64 < steps_done:
+            s64.step(steps_done - n64)
+        y64, _ = s64.download()
+        s64.close()
+        N = cells
+        err = {}
+        for q, nm in enumerate("uvwT"):
+            a, b = y_fp32[q * N:(q + 1) * N], y64[q * N:(q + 1) * N]
+            err[nm] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+        nzy = P.nz_y()
+        kk = np.arange(r.Nz_Y_max)[None, None, :]
+        m = (kk < nzy[:, :, None]).reshape(-1)
+        a, b = y_fp32[4 * N:][m], y64[4 * N:][m]
+        err["Y"] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+        v64 = cells * K * world / (ms64 * 1e-3) / 1e6
+        fp64 = {"value": round(v64, 2), "ms_per_step": round(ms64 / K, 4),
+                "speedup_fp32_over_fp64": round(value / v64, 3),
+                "fp32_rel_l2_vs_fp64_after_%d_steps" % steps_done: err}
+
+    out = None
+    if rank == 0:
+        cpu = None if args.no_cpu else cpu_reference_sample(args.config)
+        if cpu is None and not args.no_cpu:
+            cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": "reference host build not available on this machine"}
+        out = {
+            "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64" if args.precision == "fp32" else "f64",
+            "data": "synthetic (seeded fields; no dataset exists for this model)",
+            "config": {"workload": workload_name(args.config, P, args.precision),
+                       "grid": [r.Nx, r.Ny, r.Nz], "cells": cells, "dt": r.dt,
+                       "l2": "inputs larger than L2 (state %.0f MB), no flush" % (sol.S * (4 if args.precision == "fp32" else 8) / 1e6),
+                       "parallelism": "replicas x%d" % world},
+            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roof,
+            "kernels": kernels, "cpu_baseline": cpu, "clocks": clk, "fp64": fp64,
+        }
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner
+    if not ref_runner.available("host"):
+        print(json.dumps({"impl": "reference", "unavailable": "reference host build (oracle/_ref/ref_host) not present"}))
+        return None
+    # each step of this arm is a bounded sample of the workload; K steps in one run
+    cpu = cpu_reference_sample(args.config, target_s=max(5.0, 120.0 / max(args.steps, 1)), steps=args.steps)
+    out = {"impl": "reference", "metric": METRIC, "value": round(cpu["value"], 4), "unit": METRIC,
+           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(cpu["seconds"] / cpu["steps"] * 1e3, 2), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded fields)",
+           "config": {"workload": "%s (reference CPU path, bounded sample)" % args.config},
+           "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+           "e2e": {"value": round(cpu["value"], 4), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

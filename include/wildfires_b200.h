@@ -138,6 +138,16 @@ wf_status wf_pressure(wf_ctx *ctx, const double *y_np1, const double *y_n, doubl
 /* Number of kernel launches one wf_step(ctx, 1) enqueues. */
 int wf_launches_per_step(const wf_ctx *ctx);
 
+/* Kinds of kernels in a step, for wf_profile_phases. */
+#define WF_NPHASES 9
+/* Advance nsteps steps with the kernels launched one by one (no graph) and a
+ * CUDA event recorded after each kernel on the context's stream.  For every
+ * kernel kind q < WF_NPHASES, ms[q] receives the summed device time and
+ * launches[q] the number of launches.  Returns WF_OK or an error status. */
+wf_status wf_profile_phases(wf_ctx *ctx, int nsteps, double *ms, int *launches);
+/* Name of kernel kind q ("stage_rhs", "p_fftx_fwd", ...), or NULL. */
+const char *wf_phase_name(int q);
+
 const char *wf_status_string(wf_status s);
 const char *wf_last_error(void);
 

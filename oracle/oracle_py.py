@@ -90,7 +90,7 @@ def steps(P, y0, p0, nsteps, first=1):
     p = np.array(p0, dtype=np.float64, copy=True)
     r = P.rec
     N = r.Nx * r.Ny * r.Nz
-    Ts = np.ascontiguousarray(y[3 * N:4 * N])
+    Ts = y[3 * N:4 * N].copy()    # the held source is the initial temperature field
     for n in range(first, first + nsteps):
         rc = lib().wfo_step(_rec(P), _p(y), _p(p), n, _p(Ts))
         if rc != 0:

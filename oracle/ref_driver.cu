@@ -13,6 +13,10 @@
  * its set-up sequence (main.cu:27-76) but reads initial conditions from
  * `input_path` only and writes results into OUTDIR.
  *
+ * An optional topography.bin (Nx*Ny FP64, j fastest) in the working directory
+ * replaces the terrain before the immersed-boundary tables are rebuilt with
+ * the reference's ibm_parameters (ibm.cu:57-95).
+ *
  * usage: ref_driver MODE PARAMS_FILE OUTDIR [parallel]
  *   MODE phi      -- one right-hand-side evaluation Phi(y0)          -> OUTDIR/R.bin
  *        rk4      -- one RK4 stage combination y1 = RK4(y0)         -> OUTDIR/y1.bin
@@ -83,6 +87,22 @@ int main(int argc, char **argv)
     mkdir("data", 0777);
     mkdir("data/output", 0777);
     Parameters P = read_parameters_file(argv[2]);
+    {
+        /* optional terrain override: topography.bin (Nx*Ny FP64) in the working
+         * directory replaces the parsed terrain, then the reference's own
+         * immersed-boundary precompute runs again (ibm.cu:57-95) */
+        FILE *tf = fopen("topography.bin", "rb");
+        if (tf) {
+            const size_t nt = (size_t)P.Nx * P.Ny;
+            const size_t got = fread(P.topography, sizeof(double), nt, tf);
+            fclose(tf);
+            if (got != nt) {
+                fprintf(stderr, "ref_driver: topography.bin has %zu values, expected %zu\n", got, nt);
+                return 2;
+            }
+            ibm_parameters(&P);
+        }
+    }
     P.threads_per_block = THREADS;
     P.number_of_blocks = BLOCKS;
     if (P.input_path[0] == '\0') {

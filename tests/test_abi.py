@@ -1,0 +1,82 @@
+"""Host-side checks of the C-ABI library that need no GPU: symbols, parser
+rules, field-file round trip, error statuses."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, gpu_available
+
+
+def test_library_exports_every_declared_symbol():
+    from wildfires_b200 import _abi
+    L = _abi.lib()
+    header = open(os.path.join(ROOT, "include", "wildfires_b200.h")).read()
+    header = re.sub(r"/\*.*?\*/", "", header, flags=re.S)
+    declared = set(re.findall(r"\b(wf_[a-z_]+)\s*\([^()]*\)\s*;", header))
+    assert declared == set(_abi.EXPORTS), declared ^ set(_abi.EXPORTS)
+    for name in declared:
+        assert hasattr(L, name), name
+
+
+def test_parser_defaults_and_override(params_from_text):
+    P = params_from_text("Nx = 8\nNy = 9\nNz = 10\nNt = 4\nx_max = 7\ny_max = 8\nz_max = 9\nt_max = 1\n"
+                         "C_s = 0.1\nC_s = 0.3\nunknown_key = 5\nT_min = 290\nmethod = RK2\n")
+    r = P.rec
+    assert (r.Nx, r.Ny, r.Nz, r.Nt) == (8, 9, 10, 4)
+    assert r.C_s == 0.3                   # later lines override earlier ones
+    assert r.T_min == 290.0
+    assert r.mu == 1.802e-5 and r.T_act == 18040.8533 and r.variable_density == 1   # defaults
+    assert r.method == b"RK2"
+    assert r.dx == 1.0 and r.dt == 0.25
+    assert r.NT == 4                      # missing save interval -> Nt
+    assert r.field_indexes.T == 3 * 8 * 9 * 10
+
+
+def test_parser_missing_file_is_an_error(tmp_path):
+    from wildfires_b200 import WfError, read_parameters
+    with pytest.raises(WfError) as e:
+        read_parameters(tmp_path / "nope.txt")
+    assert e.value.status == 3
+
+
+def test_wavenumbers_and_hill_tables(params_from_text):
+    P = params_from_text("Nx = 12\nNy = 10\nNz = 8\nNt = 1\nx_max = 22\ny_max = 18\nz_max = 7\nt_max = 1\n"
+                         "topo_shape = hill\nhill_center_x = 11\nhill_center_y = 9\nhill_length = 4\n"
+                         "hill_width = 4\nhill_height = 3\nY_h = 0.5\n")
+    r = P.rec
+    kx = np.ctypeslib.as_array(r.kx, shape=(11,))
+    expect = 2 * np.pi * np.fft.fftfreq(11, 1.0 / 11) / 22.0
+    np.testing.assert_allclose(kx, expect, rtol=0, atol=1e-15)
+    cut = P.cut_nodes()
+    assert cut.max() == 2 and cut.min() == 0      # peak 3 exp(-1/8) = 2.65 m
+    assert r.Nz_Y_max == 4
+
+
+def test_field_files_round_trip(tmp_path, params_from_text):
+    from wildfires_b200 import _abi, load_fields
+    P = params_from_text("Nx = 5\nNy = 6\nNz = 7\nNt = 1\nx_max = 4\ny_max = 5\nz_max = 6\nt_max = 1\nY_h = 1.5\n")
+    S, N = P.state_size, 5 * 6 * 7
+    y = np.arange(S, dtype=np.float64)
+    p = -np.arange(N, dtype=np.float64)
+    d = str(tmp_path) + "/"
+    dp = C.POINTER(C.c_double)
+    _abi.check(_abi.lib().wf_save_fields(C.byref(P.rec), d.encode(), 3, y.ctypes.data_as(dp), p.ctypes.data_as(dp)), "save")
+    for nm in "uvwTYp":
+        os.rename(os.path.join(d, nm + ".bin.3"), os.path.join(d, nm + ".bin"))
+    y2, p2 = load_fields(P, d)
+    assert np.array_equal(y, y2) and np.array_equal(p, p2)
+    os.truncate(os.path.join(d, "T.bin"), 8 * 10)
+    with pytest.raises(Exception):
+        load_fields(P, d)
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the error path without a device")
+def test_create_without_device_reports_no_device(params_from_text):
+    from wildfires_b200 import Solver, WfError
+    P = params_from_text("Nx = 8\nNy = 8\nNz = 8\nNt = 1\nx_max = 7\ny_max = 7\nz_max = 7\nt_max = 1\n")
+    with pytest.raises(WfError) as e:
+        Solver(P)
+    assert e.value.status in (2, 7)

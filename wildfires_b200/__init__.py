@@ -182,3 +182,11 @@ class Solver:
 
     def launches_per_step(self):
         return lib().wf_launches_per_step(self._h)
+
+    def profile(self, nsteps=1):
+        """Per-kernel-kind device time over nsteps eager steps: {name: (total_ms, launches)}."""
+        from ._abi import WF_NPHASES
+        ms = (C.c_double * WF_NPHASES)()
+        n = (C.c_int * WF_NPHASES)()
+        check(lib().wf_profile_phases(self._h, int(nsteps), ms, n), "wf_profile_phases")
+        return {lib().wf_phase_name(q).decode(): (ms[q], n[q]) for q in range(WF_NPHASES)}

@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(HERE, "libwildfires_b200.so")
 
 WF_OK, WF_ERR_ARG, WF_ERR_CUDA, WF_ERR_IO, WF_ERR_PARSE, WF_ERR_OOM, WF_ERR_NAN, WF_ERR_NO_DEVICE = range(8)
 WF_FP64, WF_FP32_STENCIL = 0, 1
+WF_NPHASES = 9
 
 #: every symbol include/wildfires_b200.h declares
 EXPORTS = [
@@ -20,7 +21,7 @@ EXPORTS = [
     "wf_load_fields", "wf_save_fields", "wf_create", "wf_destroy", "wf_upload_state",
     "wf_download_state", "wf_step", "wf_synchronize", "wf_time", "wf_diagnostics",
     "wf_device_state", "wf_stream", "wf_phi", "wf_pressure", "wf_launches_per_step",
-    "wf_status_string", "wf_last_error",
+    "wf_status_string", "wf_last_error", "wf_profile_phases", "wf_phase_name",
 ]
 
 
@@ -80,6 +81,8 @@ def lib():
         "wf_pressure": (C.c_int, [vp, dp, dp, dp, C.POINTER(C.c_int)]),
         "wf_launches_per_step": (C.c_int, [vp]),
         "wf_status_string": (C.c_char_p, [C.c_int]),
+        "wf_profile_phases": (C.c_int, [vp, C.c_int, dp, C.POINTER(C.c_int)]),
+        "wf_phase_name": (C.c_char_p, [C.c_int]),
         "wf_last_error": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():

@@ -180,10 +180,11 @@ def hill(Nx=256, Ny=256, Nz=128, Nt=500, dt=0.003, seed=0, jitter=0.0, L=400.0, 
 
 # ---- eight seeded hills (mixed-precision workload) ------------------------------
 def hills8(Nx=512, Ny=512, Nz=128, Nt=1000, dt=0.003, seed=1234, L=800.0, H=60.0, jitter=0.0, **kw):
-    s = L / 800.0
+    # hill heights and widths are physical sizes: a smaller box (a bounded
+    # sample of the workload) keeps the same terrain statistics
     params = base_params(Nx, Ny, Nz, Nt, L, L, H, Nt * dt, **kw)
     rng0 = np.random.default_rng(seed)
-    hills = [(rng0.uniform(0, L), rng0.uniform(0, L), rng0.uniform(2, 15) * H / 60.0, rng0.uniform(20, 80) * s)
+    hills = [(rng0.uniform(0, L), rng0.uniform(0, L), rng0.uniform(2, 15), rng0.uniform(20, 80))
              for _ in range(8)]
     theta = rng0.uniform(0, 2 * math.pi)
     spots = rng0.uniform(0, 1, size=(3, 2))
@@ -209,8 +210,11 @@ def hills8(Nx=512, Ny=512, Nz=128, Nt=1000, dt=0.003, seed=1234, L=800.0, H=60.0
         u = speed * math.cos(theta)
         v = speed * math.sin(theta)
         w = np.zeros_like(u)
-        # hot spots in the upwind third along the wind direction
-        T = np.full_like(u, T_AMB)
+        # hot spots in the upwind third along the wind direction; overlapping
+        # spots take the hotter value (a sum would exceed the +500 K of one spot
+        # and drive fuel cells past the RK4 stability limit of the reaction,
+        # dt * Y_f * K(T) < 2.8, i.e. about 950 K at dt = 0.003 s)
+        heat = np.zeros_like(u)
         ux, uy = math.cos(theta), math.sin(theta)
         for (a, b) in spots:
             along = (a / 3.0 - 0.5) * L       # upwind third of the box
@@ -219,7 +223,8 @@ def hills8(Nx=512, Ny=512, Nz=128, Nt=1000, dt=0.003, seed=1234, L=800.0, H=60.0
             cy = L / 2 + along * uy + across * ux
             dx = (X - cx + L / 2) % L - L / 2
             dy = (Yg - cy + L / 2) % L - L / 2
-            T += np.where(hgt < 1.0, 500.0 * np.exp(-(dx ** 2 + dy ** 2) / (2 * 3.0 ** 2)), 0.0)
+            heat = np.maximum(heat, np.where(hgt < 1.0, 500.0 * np.exp(-(dx ** 2 + dy ** 2) / (2 * 3.0 ** 2)), 0.0))
+        T = T_AMB + heat
         frng = np.random.default_rng(fuel_seed)
         Ycol = frng.uniform(0.6, 1.0, size=(P.rec.Nx, P.rec.Ny))
         Y = np.broadcast_to(Ycol[:, :, None], u.shape).copy()
@@ -250,6 +255,7 @@ def write_case(case, directory, P=None, input_subdir="in/"):
     topo = case.topography(P)
     if topo is not None:
         P.set_topography(topo)
+        np.ascontiguousarray(topo, dtype=np.float64).tofile(os.path.join(directory, "topography.bin"))
     y0, p0 = case.fields(P)
     r = P.rec
     N = r.Nx * r.Ny * r.Nz

@@ -437,7 +437,8 @@ template cudaError_t poisson_set_attributes<float>();
 
 // zt: tridiagonal constants (see k_p_tridiag); passed through the G pointer's
 // companion allocation by the caller.
-template <class R> cudaError_t launch_poisson_impl(const PoissonArgs<R> &a, const double *zt, cudaStream_t s)
+template <class R>
+cudaError_t launch_poisson_impl(const PoissonArgs<R> &a, const double *zt, cudaStream_t s, cudaEvent_t *ev)
 {
     const int n0 = a.g.Nx - 1, nk = a.g.Nz - 1, h1 = a.h1;
     const int KP = poisson_pairs_per_block(a.fy.m);
@@ -445,19 +446,24 @@ template <class R> cudaError_t launch_poisson_impl(const PoissonArgs<R> &a, cons
     const int np1 = (nk + 1 + 1) / 2;
     dim3 g1(n0, (np1 + KP - 1) / KP);
     k_p_rhs_ffty<R><<<g1, 256, (size_t)2 * KP * a.fy.m * sizeof(double2), s>>>(a, KP);
+    if (ev) cudaEventRecord(ev[0], s);
     dim3 g2(nk + 1, (h1 + SC - 1) / SC);
     k_p_fftx<false><<<g2, 256, (size_t)2 * SC * a.fx.m * sizeof(double2), s>>>(a.G, a.fx, n0, h1, SC);
+    if (ev) cudaEventRecord(ev[1], s);
     dim3 g3(n0, (h1 + 127) / 128);
     k_p_tridiag<<<g3, 128, 0, s>>>(a.G, a.kx2, a.ky2, zt, n0, h1, nk);
+    if (ev) cudaEventRecord(ev[2], s);
     dim3 g4(nk, (h1 + SC - 1) / SC);
     k_p_fftx<true><<<g4, 256, (size_t)2 * SC * a.fx.m * sizeof(double2), s>>>(a.G, a.fx, n0, h1, SC);
+    if (ev) cudaEventRecord(ev[3], s);
     const int np5 = (nk + 1) / 2;
     dim3 g5(n0, (np5 + KP - 1) / KP);
     k_p_iffty_out<R><<<g5, 256, (size_t)2 * KP * a.fy.m * sizeof(double2), s>>>(a, KP);
+    if (ev) cudaEventRecord(ev[4], s);
     return cudaGetLastError();
 }
-template cudaError_t launch_poisson_impl<double>(const PoissonArgs<double> &, const double *, cudaStream_t);
-template cudaError_t launch_poisson_impl<float>(const PoissonArgs<float> &, const double *, cudaStream_t);
+template cudaError_t launch_poisson_impl<double>(const PoissonArgs<double> &, const double *, cudaStream_t, cudaEvent_t *);
+template cudaError_t launch_poisson_impl<float>(const PoissonArgs<float> &, const double *, cudaStream_t, cudaEvent_t *);
 
 // ---- max |a - b| reduction (pressure fixed point) ------------------------
 namespace {

@@ -503,6 +503,43 @@ void drop_graphs(wf_ctx *c)
         }
 }
 
+const char *kPhaseNames[WF_NPHASES] = {"turb_inputs", "stage_rhs", "stage_bc", "p_rhs_ffty", "p_fftx_fwd",
+                                       "p_tridiag", "p_fftx_inv", "p_iffty_out", "project"};
+
+template <class R> wf_status profile_step(wf_ctx *c, cudaEvent_t *ev, int &ne)
+{
+    cudaStream_t s = c->stream;
+    void *yn = c->ybuf[c->cur], *y1 = c->ybuf[1 - c->cur];
+    const void *ins[4], *outs[4];
+    if (c->nstages == 1) { ins[0] = yn; outs[0] = y1; }
+    else if (c->nstages == 2) { ins[0] = yn; outs[0] = c->Xa; ins[1] = c->Xa; outs[1] = y1; }
+    else {
+        ins[0] = yn; outs[0] = c->Xa; ins[1] = c->Xa; outs[1] = c->Xb;
+        ins[2] = c->Xb; outs[2] = c->Xa; ins[3] = c->Xa; outs[3] = y1;
+    }
+    WF_TRY_CUDA(cudaEventRecord(ev[ne++], s));
+    for (int st = 0; st < c->nstages; st++) {
+        WF_TRY_CUDA(launch_stage<R>(stage_args<R>(c, ins[st], yn, (void *)outs[st], st + 1), s, ev + ne));
+        ne += 3;
+    }
+    const PoissonArgs<R> a = poisson_args<R>(c, y1, yn);
+    const int nsolve = (c->P.variable_density == 0) ? 1 : c->P.pressure_solver_iter;
+    for (int q = 0; q < nsolve; q++) {
+        WF_TRY_CUDA(launch_poisson_impl<R>(a, c->d_zt, s, ev + ne));
+        ne += 5;
+    }
+    ProjectArgs<R> pa;
+    memset(&pa, 0, sizeof(pa));
+    pa.g = c->geom;
+    pa.ph = c->ph;
+    pa.y = (R *)y1;
+    pa.yn = (const R *)yn;
+    pa.p = c->p;
+    WF_TRY_CUDA(launch_project<R>(pa, s));
+    WF_TRY_CUDA(cudaEventRecord(ev[ne++], s));
+    return WF_OK;
+}
+
 }  // namespace wfs
 
 using namespace wfs;
@@ -755,6 +792,40 @@ wf_status wf_device_state(wf_ctx *c, void **y, double **pr)
 void *wf_stream(wf_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
 int wf_launches_per_step(const wf_ctx *c) { return c ? c->launches : 0; }
+
+const char *wf_phase_name(int q) { return (q >= 0 && q < WF_NPHASES) ? kPhaseNames[q] : nullptr; }
+
+wf_status wf_profile_phases(wf_ctx *c, int nsteps, double *ms, int *launches)
+{
+    if (!c || !ms || !launches || nsteps < 1) { set_error("wf_profile_phases: invalid argument"); return WF_ERR_ARG; }
+    for (int q = 0; q < WF_NPHASES; q++) { ms[q] = 0.0; launches[q] = 0; }
+    const int maxev = 2 + 3 * 4 + 5 * (c->P.pressure_solver_iter > 1 ? c->P.pressure_solver_iter : 1);
+    std::vector<cudaEvent_t> ev(maxev);
+    for (auto &e : ev) WF_TRY_CUDA(cudaEventCreate(&e));
+    wf_status st = WF_OK;
+    for (int it = 0; it < nsteps && st == WF_OK; it++) {
+        int ne = 0;
+        st = (c->prec == WF_FP64) ? profile_step<double>(c, ev.data(), ne) : profile_step<float>(c, ev.data(), ne);
+        if (st) break;
+        if (cudaEventSynchronize(ev[ne - 1]) != cudaSuccess) { set_error("wf_profile_phases: sync failed"); st = WF_ERR_CUDA; break; }
+        // kinds in launch order: stages (3 each), solves (5 each), projection
+        int e = 0;
+        auto add = [&](int kind) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[e], ev[e + 1]);
+            ms[kind] += t;
+            launches[kind] += 1;
+            e++;
+        };
+        for (int sidx = 0; sidx < c->nstages; sidx++) { add(0); add(1); add(2); }
+        while (e < ne - 2) { add(3); add(4); add(5); add(6); add(7); }
+        add(8);
+        c->cur = 1 - c->cur;
+        c->n += 1;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    return st;
+}
 
 wf_status wf_phi(wf_ctx *c, const double *R_old, double *R_new)
 {

@@ -526,17 +526,20 @@ __global__ void __launch_bounds__(128) k_stage_bc(const StageArgs<R> a)
 
 }  // namespace
 
-template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t s)
+template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t s, cudaEvent_t *ev)
 {
     const int nb = (a.g.N + 255) / 256;
     k_turb_inputs<R><<<nb, 256, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[0], s);
     k_stage_rhs<R><<<nb, 256, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[1], s);
     const int ncol = a.g.Nx * a.g.Ny;
     k_stage_bc<R><<<(ncol + 127) / 128, 128, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[2], s);
     return cudaGetLastError();
 }
 
-template cudaError_t launch_stage<double>(const StageArgs<double> &, cudaStream_t);
-template cudaError_t launch_stage<float>(const StageArgs<float> &, cudaStream_t);
+template cudaError_t launch_stage<double>(const StageArgs<double> &, cudaStream_t, cudaEvent_t *);
+template cudaError_t launch_stage<float>(const StageArgs<float> &, cudaStream_t, cudaEvent_t *);
 
 }  // namespace wf

@@ -85,7 +85,8 @@ struct StageArgs {
 };
 
 // Launch helpers implemented in the .cu files.
-template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t s);
+// ev (optional): one event recorded after each of the 3 kernels, for profiling.
+template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t s, cudaEvent_t *ev = nullptr);
 
 template <class R>
 struct ProjectArgs {
@@ -132,7 +133,9 @@ struct PoissonArgs {
     int h1;                 // (Ny-1)/2 + 1
 };
 // zt: tridiagonal constants per k (layout documented at k_p_tridiag).
-template <class R> cudaError_t launch_poisson_impl(const PoissonArgs<R> &a, const double *zt, cudaStream_t s);
+// ev (optional): one event recorded after each of the 5 kernels, for profiling.
+template <class R>
+cudaError_t launch_poisson_impl(const PoissonArgs<R> &a, const double *zt, cudaStream_t s, cudaEvent_t *ev = nullptr);
 template <class R> cudaError_t poisson_set_attributes();
 int poisson_pairs_per_block(int m);
 int poisson_lines_per_block(int m);
