@@ -144,3 +144,18 @@ def test_full_size_flat_one_step_matches_oracle():
             y, p = s.download()
         _assert_fields(P, y, yo, 1e-11, "full-size flat step")
         assert np.max(np.abs(p - po)) <= 1e-10 * max(np.max(np.abs(po)), 1e-30)
+
+
+@pytest.mark.parametrize("nx,ny", [(512, 9), (9, 512), (96, 160), (192, 256), (128, 65), (33, 17)])
+def test_pressure_fft_lengths_match_oracle(nx, ny, params_from_text):
+    """Transform lengths Nx-1, Ny-1 of every workload (511, 95, 159, 191, 255,
+    127, 64, 32, 16) through the pressure solve, against the oracle."""
+    from wildfires_b200 import configs
+    case = configs.flat(Nx=nx, Ny=ny, Nz=8, Nt=1, jitter=0.3, seed=nx + ny)
+    P = params_from_text(configs.param_text(case.params))
+    y0, p0 = case.fields(P)
+    po, _ = O.pressure(P, y0, y0, p0)
+    with _solver(P) as s:
+        p, _ = s.pressure(y0, y0, p0)
+    scale = np.max(np.abs(po))
+    assert np.max(np.abs(p - po)) <= 1e-11 * scale

@@ -34,121 +34,163 @@ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_doub
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 
-constexpr int kMaxRadix = 17;
-
-// One radix-R DFT (forward) of v[0..R) in registers/local memory.
-__device__ __forceinline__ void dft_radix(double2 *v, int R, const double2 *__restrict__ tw, int m)
+// Forward radix-4 DFT of (a0, a1, a2, a3) in natural output order.
+__device__ __forceinline__ void bfly4(double2 &a0, double2 &a1, double2 &a2, double2 &a3)
 {
-    if (R == 2) {
-        const double2 a = v[0], b = v[1];
-        v[0] = cadd(a, b);
-        v[1] = csub(a, b);
-    } else if (R == 4) {
-        const double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
-        const double2 a2 = cadd(v[1], v[3]), d = csub(v[1], v[3]);
-        const double2 a3 = make_double2(d.y, -d.x);  // -i * d
-        v[0] = cadd(a0, a2);
-        v[2] = csub(a0, a2);
-        v[1] = cadd(a1, a3);
-        v[3] = csub(a1, a3);
-    } else if (R == 3) {
-        const double h = 0.86602540378443864676;  // sqrt(3)/2
-        const double2 s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
-        const double2 t = make_double2(v[0].x - 0.5 * s.x, v[0].y - 0.5 * s.y);
-        const double2 mm = make_double2(h * d.y, -h * d.x);
-        v[0] = cadd(v[0], s);
-        v[1] = cadd(t, mm);
-        v[2] = csub(t, mm);
-    } else {
-        double2 o[kMaxRadix];
-        const int step = m / R;
-        for (int q = 0; q < R; q++) {
-            double2 acc = v[0];
-            for (int r = 1; r < R; r++) acc = cadd(acc, cmul(v[r], __ldg(tw + ((r * q) % R) * step)));
-            o[q] = acc;
+    const double2 s0 = cadd(a0, a2), d0 = csub(a0, a2);
+    const double2 s1 = cadd(a1, a3), d1 = csub(a1, a3);
+    const double2 md1 = make_double2(d1.y, -d1.x);   // -i * d1
+    a0 = cadd(s0, s1);
+    a2 = csub(s0, s1);
+    a1 = cadd(d0, md1);
+    a3 = csub(d0, md1);
+}
+
+// Forward Stockham FFT of length M = 2^L (radix-4 stages, one radix-2 stage
+// when L is odd) on nl lines held in place in shared memory (data[l*M + j]).
+// Blocks have 256 threads; lines go in groups of 1024/M so that every thread
+// owns B4 radix-4 (or B2 radix-2) butterflies per stage, kept in registers
+// between the loads and the stores of the stage.  All index arithmetic is
+// shifts and masks.  tw[j] = exp(-2 pi i j / M).
+template <int L>
+__device__ void fft_pow2(double2 *data, int nl, const double2 *__restrict__ tw)
+{
+    constexpr int M = 1 << L;
+    constexpr int Q = M / 4;
+    constexpr int GL = (M >= 1024) ? 1 : 1024 / M;
+    constexpr int B4 = (M > 1024) ? M / 1024 : 1;
+    constexpr int B2 = (GL * M / 2 + 255) / 256;
+    for (int l0 = 0; l0 < nl; l0 += GL) {
+        const int ng = min(GL, nl - l0);
+        double2 *base = data + (size_t)l0 * M;
+#pragma unroll
+        for (int st = 0; st < L / 2; st++) {
+            const int lns = 2 * st;
+            double2 v[B4][4];
+            int jb[B4];
+            double2 *xl[B4];
+#pragma unroll
+            for (int b = 0; b < B4; b++) {
+                const int t = threadIdx.x + b * 256;
+                jb[b] = -1;
+                if (t < ng * Q) {
+                    jb[b] = t & (Q - 1);
+                    xl[b] = base + (size_t)(t / Q) * M;
+#pragma unroll
+                    for (int r = 0; r < 4; r++) v[b][r] = xl[b][jb[b] + r * Q];
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int b = 0; b < B4; b++) {
+                if (jb[b] < 0) continue;
+                const int j = jb[b], k = j & ((1 << lns) - 1);
+                if (st > 0) {
+                    const int tsh = L - 2 - lns;
+                    v[b][1] = cmul(v[b][1], __ldg(tw + ((1 * k) << tsh)));
+                    v[b][2] = cmul(v[b][2], __ldg(tw + ((2 * k) << tsh)));
+                    v[b][3] = cmul(v[b][3], __ldg(tw + ((3 * k) << tsh)));
+                }
+                bfly4(v[b][0], v[b][1], v[b][2], v[b][3]);
+                const int o = ((j >> lns) << (lns + 2)) + k;
+#pragma unroll
+                for (int r = 0; r < 4; r++) xl[b][o + (r << lns)] = v[b][r];
+            }
+            __syncthreads();
         }
-        for (int q = 0; q < R; q++) v[q] = o[q];
+        if (L & 1) {
+            // final radix-2 stage: Ns = M/2, twiddle exp(-2 pi i j / M)
+            double2 v[B2][2];
+            int jb[B2];
+            double2 *xl[B2];
+#pragma unroll
+            for (int b = 0; b < B2; b++) {
+                const int t = threadIdx.x + b * 256;
+                jb[b] = -1;
+                if (t < ng * (M / 2)) {
+                    jb[b] = t & (M / 2 - 1);
+                    xl[b] = base + (size_t)(t / (M / 2)) * M;
+                    v[b][0] = xl[b][jb[b]];
+                    v[b][1] = xl[b][jb[b] + M / 2];
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int b = 0; b < B2; b++) {
+                if (jb[b] < 0) continue;
+                const double2 w = cmul(v[b][1], __ldg(tw + jb[b]));
+                xl[b][jb[b]] = cadd(v[b][0], w);
+                xl[b][jb[b] + M / 2] = csub(v[b][0], w);
+            }
+            __syncthreads();
+        }
     }
 }
 
-// Forward Stockham autosort FFT of nl lines of length m held in A ([nl][m]);
-// B is scratch of the same size.  Returns the buffer holding the result.
-__device__ double2 *stockham(double2 *A, double2 *B, int m, int nl, const FftDesc &d)
+// Length-n DFT of nl lines held in place in A ([nl][m], first n entries valid;
+// m = 2^L).  inverse selects exp(+2 pi i ...), unnormalised.  Lengths that are
+// not powers of two go through Bluestein's chirp-z identity
+//   X_k = c_k * IFFT_m( FFT_m(x c) * FFT_m(b) )_k,  c_j = exp(-i pi j^2 / n).
+template <int L>
+__device__ void fft_line_set(const FftDesc &d, double2 *A, int nl, bool inverse)
 {
-    int Ns = 1;
-    for (int f = 0; f < d.nfac; f++) {
-        const int R = d.fac[f];
-        const int nb = m / R;
-        const int twstep = m / (Ns * R);
-        for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
-            const int line = t / nb, jb = t - line * nb;
-            const double2 *x = A + (size_t)line * m;
-            double2 *y = B + (size_t)line * m;
-            const int kk = jb % Ns;
-            double2 v[kMaxRadix];
-            for (int r = 0; r < R; r++) v[r] = x[jb + r * nb];
-            if (Ns > 1)
-                for (int r = 1; r < R; r++) v[r] = cmul(v[r], __ldg(d.tw + r * kk * twstep));
-            dft_radix(v, R, d.tw, m);
-            const int base = (jb / Ns) * Ns * R + kk;
-            for (int r = 0; r < R; r++) y[base + r * Ns] = v[r];
-        }
-        __syncthreads();
-        double2 *t = A;
-        A = B;
-        B = t;
-        Ns *= R;
-    }
-    return A;
-}
-
-// Length-n DFT of nl lines (A holds [nl][m], first n entries valid).  inverse
-// selects exp(+2 pi i ...), unnormalised.  Returns the buffer with the result.
-__device__ double2 *fft_lines(const FftDesc &d, double2 *A, double2 *B, int nl, bool inverse)
-{
-    const int n = d.n, m = d.m;
+    constexpr int M = 1 << L;
+    const int n = d.n;
     if (!d.bluestein) {
         if (inverse) {
-            for (int t = threadIdx.x; t < nl * m; t += blockDim.x) A[t].y = -A[t].y;
+            for (int t = threadIdx.x; t < nl * M; t += blockDim.x) A[t].y = -A[t].y;
             __syncthreads();
         }
-        double2 *R0 = stockham(A, B, m, nl, d);
+        fft_pow2<L>(A, nl, d.tw);
         if (inverse) {
-            for (int t = threadIdx.x; t < nl * m; t += blockDim.x) R0[t].y = -R0[t].y;
+            for (int t = threadIdx.x; t < nl * M; t += blockDim.x) A[t].y = -A[t].y;
             __syncthreads();
         }
-        return R0;
+        return;
     }
-    // Bluestein: X_k = c_k * IFFT_m( FFT_m(x c) * FFT_m(b) )_k, c = exp(-i pi j^2/n)
-    for (int t = threadIdx.x; t < nl * m; t += blockDim.x) {
-        const int j = t % m;
+    for (int t = threadIdx.x; t < nl * M; t += blockDim.x) {
+        const int j = t & (M - 1);
         double2 v = A[t];
         if (inverse) v.y = -v.y;
         A[t] = (j < n) ? cmul(v, __ldg(d.chirp + j)) : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    double2 *R1 = stockham(A, B, m, nl, d);
-    for (int t = threadIdx.x; t < nl * m; t += blockDim.x) {
-        const int j = t % m;
-        R1[t] = cconj(cmul(R1[t], __ldg(d.filt + j)));   // conj for IFFT via FFT
-    }
+    fft_pow2<L>(A, nl, d.tw);
+    for (int t = threadIdx.x; t < nl * M; t += blockDim.x)
+        A[t] = cconj(cmul(A[t], __ldg(d.filt + (t & (M - 1)))));   // conj: IFFT via FFT
     __syncthreads();
-    double2 *other = (R1 == A) ? B : A;
-    double2 *R2 = stockham(R1, other, m, nl, d);
-    const double inv_m = 1.0 / (double)m;
-    for (int t = threadIdx.x; t < nl * m; t += blockDim.x) {
-        const int j = t % m;
+    fft_pow2<L>(A, nl, d.tw);
+    const double inv_m = 1.0 / (double)M;
+    for (int t = threadIdx.x; t < nl * M; t += blockDim.x) {
+        const int j = t & (M - 1);
         if (j < n) {
-            double2 v = cconj(R2[t]);
+            double2 v = cconj(A[t]);
             v.x *= inv_m;
             v.y *= inv_m;
             v = cmul(v, __ldg(d.chirp + j));
             if (inverse) v.y = -v.y;
-            R2[t] = v;
+            A[t] = v;
         }
     }
     __syncthreads();
-    return R2;
+}
+
+__device__ void fft_lines(const FftDesc &d, double2 *A, int nl, bool inverse)
+{
+    switch (d.L) {
+    case 2: fft_line_set<2>(d, A, nl, inverse); break;
+    case 3: fft_line_set<3>(d, A, nl, inverse); break;
+    case 4: fft_line_set<4>(d, A, nl, inverse); break;
+    case 5: fft_line_set<5>(d, A, nl, inverse); break;
+    case 6: fft_line_set<6>(d, A, nl, inverse); break;
+    case 7: fft_line_set<7>(d, A, nl, inverse); break;
+    case 8: fft_line_set<8>(d, A, nl, inverse); break;
+    case 9: fft_line_set<9>(d, A, nl, inverse); break;
+    case 10: fft_line_set<10>(d, A, nl, inverse); break;
+    case 11: fft_line_set<11>(d, A, nl, inverse); break;
+    case 12: fft_line_set<12>(d, A, nl, inverse); break;
+    default: break;
+    }
 }
 
 // Poisson source at (i, j, k), k < Nz-1 (pressure.cu:37-95 and 150-321).
@@ -259,7 +301,7 @@ __global__ void __launch_bounds__(256) k_p_rhs_ffty(const PoissonArgs<R> a, int 
     const int nslices = nk + 1;                      // f slices + top-plane pressure
     const int np = (nslices + 1) / 2;
     const int kp = min(KP, np - pair0);
-    double2 *A = smem, *B = smem + (size_t)KP * m1;
+    double2 *A = smem;
     double *Ad = reinterpret_cast<double *>(A);
     const int ns = 2 * kp;
     for (int t = threadIdx.x; t < n1 * ns; t += blockDim.x) {
@@ -271,7 +313,8 @@ __global__ void __launch_bounds__(256) k_p_rhs_ffty(const PoissonArgs<R> a, int 
         Ad[2 * ((size_t)(q >> 1) * m1 + jj) + (q & 1)] = val;
     }
     __syncthreads();
-    double2 *Rb = fft_lines(a.fy, A, B, kp, false);
+    fft_lines(a.fy, A, kp, false);
+    const double2 *Rb = A;
     // split the packed transform into the two half spectra
     for (int t = threadIdx.x; t < kp * h1; t += blockDim.x) {
         const int line = t / h1, s = t - line * h1;
@@ -294,14 +337,15 @@ __global__ void __launch_bounds__(256) k_p_fftx(double2 *__restrict__ G, FftDesc
     const int kk = blockIdx.x;
     const int s0 = blockIdx.y * SC;
     const int sc = min(SC, h1 - s0);
-    double2 *A = smem, *B = smem + (size_t)SC * m0;
+    double2 *A = smem;
     double2 *Gs = G + (size_t)kk * n0 * h1;
     for (int t = threadIdx.x; t < n0 * sc; t += blockDim.x) {
         const int r = t / sc, q = t - r * sc;
         A[(size_t)q * m0 + r] = Gs[(size_t)r * h1 + s0 + q];
     }
     __syncthreads();
-    double2 *Rb = fft_lines(fx, A, B, sc, INV);
+    fft_lines(fx, A, sc, INV);
+    const double2 *Rb = A;
     for (int t = threadIdx.x; t < n0 * sc; t += blockDim.x) {
         const int r = t / sc, q = t - r * sc;
         Gs[(size_t)r * h1 + s0 + q] = Rb[(size_t)q * m0 + r];
@@ -372,7 +416,7 @@ __global__ void __launch_bounds__(256) k_p_iffty_out(const PoissonArgs<R> a, int
     const int pair0 = blockIdx.y * KP;
     const int np = (nk + 1) / 2;
     const int kp = min(KP, np - pair0);
-    double2 *A = smem, *B = smem + (size_t)KP * m1;
+    double2 *A = smem;
     const bool even = (n1 % 2) == 0;
     for (int t = threadIdx.x; t < kp * n1; t += blockDim.x) {
         const int line = t / n1, s = t - line * n1;
@@ -391,7 +435,8 @@ __global__ void __launch_bounds__(256) k_p_iffty_out(const PoissonArgs<R> a, int
         A[(size_t)line * m1 + s] = make_double2(Fa.x - Fb.y, Fa.y + Fb.x);
     }
     __syncthreads();
-    double2 *Rb = fft_lines(a.fy, A, B, kp, true);
+    fft_lines(a.fy, A, kp, true);
+    const double2 *Rb = A;
     const double norm = (double)n0 * (double)n1;
     const int ns = 2 * kp;
     double *p = a.p;
@@ -420,8 +465,8 @@ __global__ void __launch_bounds__(256) k_p_iffty_out(const PoissonArgs<R> a, int
 
 }  // namespace
 
-int poisson_pairs_per_block(int m) { return max(1, min(8, 3072 / m)); }
-int poisson_lines_per_block(int m) { return max(1, min(16, 3072 / m)); }
+int poisson_pairs_per_block(int m) { return max(1, min(16, 6144 / m)); }
+int poisson_lines_per_block(int m) { return max(1, min(16, 6144 / m)); }
 
 template <class R> cudaError_t poisson_set_attributes()
 {
@@ -445,20 +490,20 @@ cudaError_t launch_poisson_impl(const PoissonArgs<R> &a, const double *zt, cudaS
     const int SC = poisson_lines_per_block(a.fx.m);
     const int np1 = (nk + 1 + 1) / 2;
     dim3 g1(n0, (np1 + KP - 1) / KP);
-    k_p_rhs_ffty<R><<<g1, 256, (size_t)2 * KP * a.fy.m * sizeof(double2), s>>>(a, KP);
+    k_p_rhs_ffty<R><<<g1, 256, (size_t)KP * a.fy.m * sizeof(double2), s>>>(a, KP);
     if (ev) cudaEventRecord(ev[0], s);
     dim3 g2(nk + 1, (h1 + SC - 1) / SC);
-    k_p_fftx<false><<<g2, 256, (size_t)2 * SC * a.fx.m * sizeof(double2), s>>>(a.G, a.fx, n0, h1, SC);
+    k_p_fftx<false><<<g2, 256, (size_t)SC * a.fx.m * sizeof(double2), s>>>(a.G, a.fx, n0, h1, SC);
     if (ev) cudaEventRecord(ev[1], s);
     dim3 g3(n0, (h1 + 127) / 128);
     k_p_tridiag<<<g3, 128, 0, s>>>(a.G, a.kx2, a.ky2, zt, n0, h1, nk);
     if (ev) cudaEventRecord(ev[2], s);
     dim3 g4(nk, (h1 + SC - 1) / SC);
-    k_p_fftx<true><<<g4, 256, (size_t)2 * SC * a.fx.m * sizeof(double2), s>>>(a.G, a.fx, n0, h1, SC);
+    k_p_fftx<true><<<g4, 256, (size_t)SC * a.fx.m * sizeof(double2), s>>>(a.G, a.fx, n0, h1, SC);
     if (ev) cudaEventRecord(ev[3], s);
     const int np5 = (nk + 1) / 2;
     dim3 g5(n0, (np5 + KP - 1) / KP);
-    k_p_iffty_out<R><<<g5, 256, (size_t)2 * KP * a.fy.m * sizeof(double2), s>>>(a, KP);
+    k_p_iffty_out<R><<<g5, 256, (size_t)KP * a.fy.m * sizeof(double2), s>>>(a, KP);
     if (ev) cudaEventRecord(ev[4], s);
     return cudaGetLastError();
 }

@@ -37,18 +37,7 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
-// ---- FFT plans: factorisation and tables (setup only) ---------------------
-bool stockham_factors(int m, int *fac, int &nfac)
-{
-    nfac = 0;
-    int r = m;
-    while (r % 4 == 0) { fac[nfac++] = 4; r /= 4; }
-    while (r % 2 == 0) { fac[nfac++] = 2; r /= 2; }
-    for (int p = 3; p <= 17 && r > 1; p += 2)
-        while (r % p == 0) { fac[nfac++] = p; r /= p; }
-    return r == 1 && nfac <= 20;
-}
-
+// ---- FFT plans: power-of-two lengths directly, others by Bluestein (setup only)
 const long double kPiL = 3.141592653589793238462643383279502884L;
 
 struct HostFft {
@@ -61,24 +50,17 @@ HostFft plan_fft(int n)
     HostFft h;
     memset(&h.d, 0, sizeof(h.d));
     h.d.n = n;
-    int fac[20], nf = 0;
-    if (n == 1) {
-        h.d.m = 1;
-        h.d.nfac = 0;
-    } else if (stockham_factors(n, fac, nf)) {
+    if ((n & (n - 1)) == 0) {
         h.d.m = n;
-        h.d.nfac = nf;
-        memcpy(h.d.fac, fac, sizeof(int) * nf);
     } else {
         int m = 1;
         while (m < 2 * n - 1) m <<= 1;
         h.d.m = m;
         h.d.bluestein = 1;
-        stockham_factors(m, fac, nf);
-        h.d.nfac = nf;
-        memcpy(h.d.fac, fac, sizeof(int) * nf);
     }
     const int m = h.d.m;
+    h.d.L = 0;
+    while ((1 << h.d.L) < m) h.d.L++;
     h.tw.resize(m);
     for (int j = 0; j < m; j++) {
         const long double a = -2.0L * kPiL * (long double)j / (long double)m;
@@ -145,12 +127,13 @@ struct wf_ctx {
     std::vector<DevBuf> bufs;
     void *ybuf[2] = {nullptr, nullptr};
     int cur = 0;
-    void *Xa = nullptr, *Xb = nullptr, *acc = nullptr, *scr = nullptr, *utau = nullptr, *bc = nullptr;
+    void *Xa = nullptr, *Xb = nullptr, *acc = nullptr, *utau = nullptr, *bc = nullptr;
     void *Tsrc = nullptr;
     double *p = nullptr, *p_prev = nullptr, *red = nullptr, *d_diag = nullptr;
     double2 *G = nullptr;
     double *d_z = nullptr, *d_zc = nullptr, *d_topo = nullptr, *d_kx2 = nullptr, *d_ky2 = nullptr, *d_zt = nullptr;
     double *d_x = nullptr, *d_y = nullptr;
+    void *d_krow = nullptr;     // [Nz][KROW] in the stencil precision
     int *d_nzy = nullptr, *d_cut = nullptr;
     FftDesc fx, fy;
     Phys ph;
@@ -278,6 +261,53 @@ std::vector<double> tridiag_table(const Parameters &P, const double *z)
     return t;
 }
 
+// Branch-free z-stencil rows for the fused stage kernel (see KRow).
+std::vector<double> krow_table(const Parameters &P, const double *z, const std::vector<double> &zc)
+{
+    const int Nz = P.Nz;
+    std::vector<double> t((size_t)Nz * KROW, 0.0);
+    auto Z = [&](int e, int k) { return zc[(size_t)e * Nz + k]; };
+    for (int k = 0; k < Nz; k++) {
+        double *r = &t[(size_t)k * KROW];
+        // upwind "from below": forward form at k <= 1, backward form above (pde.cu:355-395)
+        if (k <= 1) { r[RKM + 2] = Z(ZF0, k); r[RKM + 3] = Z(ZF1, k); r[RKM + 4] = Z(ZF2, k); }
+        else { r[RKM + 0] = Z(ZB0, k); r[RKM + 1] = Z(ZB1, k); r[RKM + 2] = Z(ZB2, k); }
+        // upwind "from above": backward form at k >= Nz-2, forward form below (pde.cu:397-437)
+        if (k >= Nz - 2) { r[RKP + 0] = Z(ZB0, k); r[RKP + 1] = Z(ZB1, k); r[RKP + 2] = Z(ZB2, k); }
+        else { r[RKP + 2] = Z(ZF0, k); r[RKP + 3] = Z(ZF1, k); r[RKP + 4] = Z(ZF2, k); }
+        r[RD1] = Z(ZC, k);
+        r[RD2 + 0] = Z(ZCM, k);
+        r[RD2 + 1] = Z(ZC0, k);
+        r[RD2 + 2] = Z(ZCP, k);
+        r[RDZ] = Z(ZDZ, k);
+        r[RDEL2] = Z(ZDELTA2, k);
+        r[RZ] = z[k];
+    }
+    return t;
+}
+
+template <class R> PhysR<R> make_physr(const Parameters &P)
+{
+    constexpr double kSigmaSB = 5.670374419e-8;  // Stefan-Boltzmann (reference constants.h:16)
+    PhysR<R> r;
+    r.inv2dx = (R)(1.0 / (2 * P.dx));
+    r.inv2dy = (R)(1.0 / (2 * P.dy));
+    r.invdx2 = (R)(1.0 / (P.dx * P.dx));
+    r.invdy2 = (R)(1.0 / (P.dy * P.dy));
+    r.Trho = (R)P.T_inf * (R)P.rho_inf;
+    r.mu = (R)P.mu; r.kT = (R)P.k; r.Y_f = (R)P.Y_f; r.H_C = (R)P.H_C; r.A = (R)P.A; r.T_act = (R)P.T_act;
+    r.T_pc = (R)P.T_pc; r.h_c = (R)P.h_c; r.alpha_s = (R)P.alpha_s; r.sigma_s = (R)P.sigma_s;
+    r.T_inf = (R)P.T_inf; r.c_p = (R)P.c_p; r.rho_inf = (R)P.rho_inf;
+    r.cd = (R)(0.5 * P.C_d * P.alpha_s * P.sigma_s);
+    r.g = (R)P.g;
+    r.c12 = (R)(12 * kSigmaSB * P.delta);
+    r.c4 = (R)(4 * kSigmaSB * P.delta);
+    r.Pr = (R)P.Pr;
+    r.inv_avd = R(1) / R(26.0);
+    r.T_min = (R)P.T_min; r.T_max = (R)P.T_max; r.Y_min = (R)P.Y_min; r.Y_max = (R)P.Y_max;
+    return r;
+}
+
 Phys make_phys(const Parameters &P)
 {
     Phys ph;
@@ -303,11 +333,12 @@ template <class R> StageArgs<R> stage_args(wf_ctx *c, const void *X, const void 
     StageArgs<R> a;
     a.g = c->geom;
     a.ph = c->ph;
+    a.pr = make_physr<R>(c->P);
+    a.krow = (const R *)c->d_krow;
     a.X = (const R *)X;
     a.yn = (const R *)yn;
     a.acc = (R *)c->acc;
     a.Xout = (R *)Xout;
-    a.scr = (R *)c->scr;
     a.utau = (R *)c->utau;
     a.bc = (R *)c->bc;
     a.method = c->method;
@@ -503,7 +534,7 @@ void drop_graphs(wf_ctx *c)
         }
 }
 
-const char *kPhaseNames[WF_NPHASES] = {"turb_inputs", "stage_rhs", "stage_bc", "p_rhs_ffty", "p_fftx_fwd",
+const char *kPhaseNames[WF_NPHASES] = {"stage_utau", "stage_fused", "stage_bc", "p_rhs_ffty", "p_fftx_fwd",
                                        "p_tridiag", "p_fftx_inv", "p_iffty_out", "project"};
 
 template <class R> wf_status profile_step(wf_ctx *c, cudaEvent_t *ev, int &ne)
@@ -633,7 +664,6 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
         if ((st = dev_alloc(c, &c->Xa, sb)) || (st = dev_alloc(c, &c->acc, sb))) return fail(st);
         if (c->nstages > 2 && (st = dev_alloc(c, &c->Xb, sb))) return fail(st);
     }
-    if ((st = dev_alloc(c, &c->scr, (size_t)kScratchFields * c->N * c->esz))) return fail(st);
     if ((st = dev_alloc(c, &c->utau, (size_t)Nx * Ny * c->esz))) return fail(st);
     if ((st = dev_alloc(c, &c->bc, (size_t)Nx * Ny * kBcSlots * c->esz))) return fail(st);
     if ((st = dev_alloc(c, (void **)&c->p, sizeof(double) * c->N))) return fail(st);
@@ -652,6 +682,19 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
         (st = upload(c, &c->d_nzy, c->hnzy.data(), c->hnzy.size())) || (st = upload(c, &c->d_cut, c->hcut.data(), c->hcut.size())) ||
         (st = upload(c, &c->d_x, c->hx.data(), Nx)) || (st = upload(c, &c->d_y, c->hy.data(), Ny)))
         return fail(st);
+    {
+        const std::vector<double> kr = krow_table(c->P, c->hz.data(), zc);
+        if (precision == WF_FP64) {
+            double *d = nullptr;
+            if ((st = upload(c, &d, kr.data(), kr.size()))) return fail(st);
+            c->d_krow = d;
+        } else {
+            std::vector<float> kf(kr.begin(), kr.end());
+            float *d = nullptr;
+            if ((st = upload(c, &d, kf.data(), kf.size()))) return fail(st);
+            c->d_krow = d;
+        }
+    }
     const HostFft hfx = plan_fft(Nx - 1), hfy = plan_fft(Ny - 1);
     if ((st = upload_fft(c, hfx, c->fx)) || (st = upload_fft(c, hfy, c->fy))) return fail(st);
     if (P->t_source_end > P->t_min && P->t_source_start <= 0)
@@ -662,6 +705,7 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
     c->geom.nzy = c->d_nzy; c->geom.cut = c->d_cut;
     c->ph = make_phys(c->P);
     cudaError_t e = (precision == WF_FP64) ? poisson_set_attributes<double>() : poisson_set_attributes<float>();
+    if (e == cudaSuccess) e = (precision == WF_FP64) ? stage_set_attributes<double>() : stage_set_attributes<float>();
     if (e != cudaSuccess) { set_error("wf_create: %s", cudaGetErrorString(e)); return fail(WF_ERR_CUDA); }
     WF_TRY_CUDA(cudaMemsetAsync(c->p, 0, sizeof(double) * c->N, c->stream));
     WF_TRY_CUDA(cudaStreamSynchronize(c->stream));

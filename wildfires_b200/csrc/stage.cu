@@ -4,16 +4,18 @@
 // Smagorinsky SGS terms, boundary/IBM rules) and folds the RK combination into
 // the same pass (reference solver.cu:14-93, utils.cu:14-21), so no k-buffer is
 // ever stored:
-//   pass 1  k_turb_inputs : per cell, the SGS inputs that neighbours need
-//                           (raw mu_sgs, strain S', divergence source) and the
-//                           wall friction velocity of the k = 0 plane;
-//   pass 2  k_stage_rhs   : per cell, advection + diffusion + forces + reaction
-//                           + SGS divergence, then acc/X_{s+1} updates for every
-//                           cell the boundary rules do not overwrite;
-//   pass 3  k_stage_bc    : per column, the boundary/IBM values of k_s (cut node,
-//                           top, dead nodes) and their RK updates.
+//   k_utau        : per column, wall friction velocity from the k = 0 plane;
+//   k_stage_fused : per tile of cells in shared memory, the SGS inputs on the
+//                   tile and its halo, then advection + diffusion + forces +
+//                   reaction + SGS divergence and the acc / X_{s+1} updates of
+//                   every cell the boundary rules do not overwrite;
+//   k_stage_bc    : per column, the boundary/IBM values of k_s (cut node, top,
+//                   dead nodes) and their RK updates.
+// The right-hand side of cells on the walls (k = 0, k = Nz-1) and below the
+// cut node is never used by the reference (boundary_conditions overwrites it,
+// pde.cu:58-97), so the fused pass evaluates interior stencils only.
 // Arithmetic follows the reference expression by expression; divisions by
-// grid constants are folded into precomputed weights (ZCoef).
+// grid constants are folded into precomputed weights (ZCoef, KRow).
 #include <math.h>
 
 #include "wf_internal.h"
@@ -22,21 +24,13 @@ namespace wf {
 
 namespace {
 
-constexpr double kSigmaSB = 5.670374419e-8;  // Stefan-Boltzmann (reference constants.h:16)
-constexpr double kAVD = 26.0;                // Van Driest constant (constants.h:19)
-
 __device__ __forceinline__ int wrap_p(int v, int n)
 {
-    // periodic index with period n = N-1 for v in [-2, n+2] (pde.cu:227-234)
+    // periodic index with period n = N-1 for v in [-2, 2n+1] (pde.cu:227-234)
     if (v >= n) v -= n;
     if (v >= n) v -= n;
     if (v < 0) v += n;
     return v;
-}
-
-template <class R> __device__ __forceinline__ R zcoef(const double *zc, int e, int Nz, int k)
-{
-    return (R)__ldg(zc + (size_t)e * Nz + k);
 }
 
 template <class R> __device__ __forceinline__ R rmax(R a, R b) { return (a > b) ? a : b; }
@@ -51,66 +45,12 @@ __device__ __forceinline__ float rpow(float x, float y) { return powf(x, y); }
 __device__ __forceinline__ double rfabs(double x) { return fabs(x); }
 __device__ __forceinline__ float rfabs(float x) { return fabsf(x); }
 
-// Values of one field along the column of a cell: k-3 .. k+3 (0 outside).
-template <class R> struct ZN {
-    R m3, m2, m1, c, p1, p2, p3;
-};
+// Van Driest damping f_w = 1 - exp(-z+ / A_VD).  Below the cut-off the
+// exponential is smaller than half an ulp of 1 and the result is exactly 1.
+__device__ __forceinline__ double van_driest(double x) { return x < -37.5 ? 1.0 : 1.0 - exp(x); }
+__device__ __forceinline__ float van_driest(float x) { return x < -17.5f ? 1.0f : 1.0f - expf(x); }
 
-template <class R>
-__device__ __forceinline__ void load_col(ZN<R> &v, const R *__restrict__ col, int k, int Nz, int reach)
-{
-    v.c = col[k];
-    v.m1 = (k > 0) ? col[k - 1] : R(0);
-    v.p1 = (k < Nz - 1) ? col[k + 1] : R(0);
-    v.m2 = (k > 1) ? col[k - 2] : R(0);
-    v.p2 = (k < Nz - 2) ? col[k + 2] : R(0);
-    if (reach >= 3) {
-        v.m3 = (k > 2) ? col[k - 3] : R(0);
-        v.p3 = (k < Nz - 3) ? col[k + 3] : R(0);
-    } else {
-        v.m3 = R(0);
-        v.p3 = R(0);
-    }
-}
-
-// forward / backward one-sided first derivatives on the non-uniform z grid
-template <class R> __device__ __forceinline__ R dz_f(const ZN<R> &v, const double *zc, int Nz, int k)
-{
-    return zcoef<R>(zc, ZF0, Nz, k) * v.c + zcoef<R>(zc, ZF1, Nz, k) * v.p1 + zcoef<R>(zc, ZF2, Nz, k) * v.p2;
-}
-template <class R> __device__ __forceinline__ R dz_b(const ZN<R> &v, const double *zc, int Nz, int k)
-{
-    return zcoef<R>(zc, ZB0, Nz, k) * v.m2 + zcoef<R>(zc, ZB1, Nz, k) * v.m1 + zcoef<R>(zc, ZB2, Nz, k) * v.c;
-}
-// first derivative: one-sided at the walls, central inside (pde.cu:471-576)
-template <class R> __device__ __forceinline__ R dz_1(const ZN<R> &v, const double *zc, int Nz, int k)
-{
-    if (k == 0) return dz_f(v, zc, Nz, k);
-    if (k == Nz - 1) return dz_b(v, zc, Nz, k);
-    return (v.p1 - v.m1) * zcoef<R>(zc, ZC, Nz, k);
-}
-// second derivative (pde.cu:497-575)
-template <class R> __device__ __forceinline__ R dz_2(const ZN<R> &v, const double *zc, int Nz, int k)
-{
-    if (k == 0)
-        return zcoef<R>(zc, ZFF0, Nz, k) * v.c + zcoef<R>(zc, ZFF1, Nz, k) * v.p1 +
-               zcoef<R>(zc, ZFF2, Nz, k) * v.p2 + zcoef<R>(zc, ZFF3, Nz, k) * v.p3;
-    if (k == Nz - 1)
-        return zcoef<R>(zc, ZBB0, Nz, k) * v.m3 + zcoef<R>(zc, ZBB1, Nz, k) * v.m2 +
-               zcoef<R>(zc, ZBB2, Nz, k) * v.m1 + zcoef<R>(zc, ZBB3, Nz, k) * v.c;
-    return zcoef<R>(zc, ZCM, Nz, k) * v.m1 + zcoef<R>(zc, ZC0, Nz, k) * v.c + zcoef<R>(zc, ZCP, Nz, k) * v.p1;
-}
-// upwind one-sided derivatives used for advection (pde.cu:355-437)
-template <class R> __device__ __forceinline__ R dz_km(const ZN<R> &v, const double *zc, int Nz, int k)
-{
-    return (k <= 1) ? dz_f(v, zc, Nz, k) : dz_b(v, zc, Nz, k);
-}
-template <class R> __device__ __forceinline__ R dz_kp(const ZN<R> &v, const double *zc, int Nz, int k)
-{
-    return (k >= Nz - 2) ? dz_b(v, zc, Nz, k) : dz_f(v, zc, Nz, k);
-}
-
-// Temperature source terms shared by both passes (pde.cu:664-711).
+// Temperature source terms (pde.cu:664-711).
 template <class R> struct Thermo {
     R T_RHS_tmp;  // conduction + radiation + reaction, before convection
     R nu;         // molecular kinematic viscosity (Sutherland when enabled)
@@ -120,109 +60,38 @@ template <class R> struct Thermo {
 };
 
 template <class R>
-__device__ __forceinline__ Thermo<R> thermo(const Phys &ph, R T, R T_kp1, const R *__restrict__ Ycol, int k,
+__device__ __forceinline__ Thermo<R> thermo(const PhysR<R> &p, int suth_mu, int suth_k, R T, R T_kp1, R Yc, int k,
                                             int nzy, R Tx, R Ty, R Tz, R lap_T, R dz_k, R rho)
 {
     Thermo<R> o;
-    R mu = (R)ph.mu, kT = (R)ph.kT, dk = R(0);
-    const R T_pc = (R)ph.T_pc, T_inf = (R)ph.T_inf;
-    const R H_step = (T > T_pc) ? R(1) : R(0);
-    o.K_T = (R)ph.A * rexp(-(R)ph.T_act / T) * H_step;
-    R Y = R(0), T_gas = T_inf, T_solid = T_inf;
+    R mu = p.mu, kT = p.kT, dk = R(0);
+    // Arrhenius rate A exp(-T_act/T) H(T - T_pc); exactly 0 below the phase change
+    o.K_T = (T > p.T_pc) ? p.A * rexp(-p.T_act / T) * R(1) : R(0);
+    R Y = R(0), T_gas = p.T_inf, T_solid = p.T_inf;
     if (k <= nzy) {
-        if (k < nzy) Y = Ycol[k];
+        if (k < nzy) Y = Yc;
         else T_gas = T_kp1;
         if (Y > R(0)) T_solid = T;
         else T_gas = T;
     }
-    if (ph.sutherland_viscosity == 1)
-        mu = R(1.716e-5) * rpow(T / R(273.15), R(1.5)) * (R(273.15) + R(110.4)) / (T + R(110.4));
-    if (ph.sutherland_conductivity == 1) {
+    if (suth_mu == 1) mu = R(1.716e-5) * rpow(T / R(273.15), R(1.5)) * (R(273.15) + R(110.4)) / (T + R(110.4));
+    if (suth_k == 1) {
         kT = R(0.0241) * rpow(T / R(273.15), R(1.5)) * (R(273.15) + R(194)) / (T + R(194));
         dk = R(0.0241) * (R(1.5) * rpow(T / R(273.15), R(0.5)) * (R(273.15) + R(194)) / (T + R(194)) -
                           rpow(T / R(273.15), R(1.5)) * (R(273.15) + R(194)) / ((T + R(194)) * (T + R(194))));
     }
     o.nu = mu / rho;
     o.mu = mu;
-    R q = (R)ph.H_C * Y * o.K_T / (R)ph.c_p;
-    const R as = (R)ph.alpha_s * (R)ph.sigma_s;
-    if (as != R(0)) {
+    R q = p.H_C * Y * o.K_T / p.c_p;
+    if (p.alpha_s * p.sigma_s != R(0)) {
         // h_c evaluated per cell (the reference compounds its copy per thread, pde.cu:698)
-        const R h_c = (R)ph.h_c * dz_k * rpow(rfabs(T_gas - T_solid) / dz_k, R(0.25));
-        q = q - h_c * (R)ph.alpha_s * (R)ph.sigma_s * (T_gas - T_solid) /
-                    ((R)ph.c_p * T_inf * (R)ph.rho_inf / T_gas);
+        const R h_c = p.h_c * dz_k * rpow(rfabs(T_gas - T_solid) / dz_k, R(0.25));
+        q = q - h_c * p.alpha_s * p.sigma_s * (T_gas - T_solid) / (p.c_p * p.T_inf * p.rho_inf / T_gas);
     }
-    const R c12 = (R)(12 * kSigmaSB * ph.delta), c4 = (R)(4 * kSigmaSB * ph.delta);
-    o.T_RHS_tmp = (dk + c12 * (T * T) * (Tx * Tx + Ty * Ty + Tz * Tz) + (kT + c4 * (T * T * T)) * lap_T) /
-                      (rho * (R)ph.c_p) + q;
+    o.T_RHS_tmp = (dk + p.c12 * (T * T) * (Tx * Tx + Ty * Ty + Tz * Tz) + (kT + p.c4 * (T * T * T)) * lap_T) /
+                      (rho * p.c_p) + q;
     o.Y = Y;
     return o;
-}
-
-// ---------------------------------------------------------------------------
-// pass 1: SGS inputs (reference RHS kernel, pde.cu:632-772)
-template <class R>
-__global__ void __launch_bounds__(256) k_turb_inputs(const StageArgs<R> a)
-{
-    const Geom &g = a.g;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.N) return;
-    const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz, N = g.N;
-    const int k = c % Nz, col = c / Nz, j = col % Ny, i = col / Ny;
-    const int ip1 = wrap_p(i + 1, Nx - 1), im1 = wrap_p(i - 1, Nx - 1);
-    const int jp1 = wrap_p(j + 1, Ny - 1), jm1 = wrap_p(j - 1, Ny - 1);
-    const R *__restrict__ X = a.X;
-    const size_t cxp = ((size_t)ip1 * Ny + j) * Nz + k, cxm = ((size_t)im1 * Ny + j) * Nz + k;
-    const size_t cyp = ((size_t)i * Ny + jp1) * Nz + k, cym = ((size_t)i * Ny + jm1) * Nz + k;
-    const R inv2dx = (R)(1.0 / (2 * a.ph.dx)), inv2dy = (R)(1.0 / (2 * a.ph.dy));
-    const R invdx2 = (R)(1.0 / (a.ph.dx * a.ph.dx)), invdy2 = (R)(1.0 / (a.ph.dy * a.ph.dy));
-    ZN<R> U, V, W, T;
-    const size_t cb = (size_t)col * Nz;
-    load_col(U, X + cb, k, Nz, 2);
-    load_col(V, X + N + cb, k, Nz, 2);
-    load_col(W, X + 2 * (size_t)N + cb, k, Nz, 2);
-    load_col(T, X + 3 * (size_t)N + cb, k, Nz, 3);
-    const R ux = (X[cxp] - X[cxm]) * inv2dx, uy = (X[cyp] - X[cym]) * inv2dy;
-    const R vx = (X[N + cxp] - X[N + cxm]) * inv2dx, vy = (X[N + cyp] - X[N + cym]) * inv2dy;
-    const R wx = (X[2 * (size_t)N + cxp] - X[2 * (size_t)N + cxm]) * inv2dx;
-    const R wy = (X[2 * (size_t)N + cyp] - X[2 * (size_t)N + cym]) * inv2dy;
-    const R Txp = X[3 * (size_t)N + cxp], Txm = X[3 * (size_t)N + cxm];
-    const R Typ = X[3 * (size_t)N + cyp], Tym = X[3 * (size_t)N + cym];
-    const R Tx = (Txp - Txm) * inv2dx, Ty = (Typ - Tym) * inv2dy;
-    const R Txx = (Txp - R(2) * T.c + Txm) * invdx2, Tyy = (Typ - R(2) * T.c + Tym) * invdy2;
-    const R uz = dz_1(U, g.zc, Nz, k), vz = dz_1(V, g.zc, Nz, k), wz = dz_1(W, g.zc, Nz, k);
-    const R Tz = dz_1(T, g.zc, Nz, k), Tzz = dz_2(T, g.zc, Nz, k);
-    const R rho = (R)a.ph.T_inf * (R)a.ph.rho_inf / T.c;
-    // modified strain S' and |S| (the reference's integer 2/3 removes the trace term)
-    R *scr = a.scr;
-    const R third = R(1) / R(3);
-    (void)third;
-    const R S11 = R(2) * ux / R(3) - (vy + wz) / R(3);
-    const R S22 = R(2) * vy / R(3) - (ux + wz) / R(3);
-    const R S33 = R(2) * wz / R(3) - (ux + vy) / R(3);
-    const R S12 = R(0.5) * (uy + vx), S13 = R(0.5) * (uz + wx), S23 = R(0.5) * (wy + vz);
-    const R mod_S = rsqrt_(R(2) * (ux * ux + vy * vy + wz * wz) + (uz + wx) * (uz + wx) + (vx + uy) * (vx + uy) +
-                           (wy + vz) * (wy + vz));
-    const R dz_k = zcoef<R>(g.zc, ZDZ, Nz, k);
-    const R mu_sgs = rho * zcoef<R>(g.zc, ZDELTA2, Nz, k) * mod_S;
-    const int nzy = __ldg(g.nzy + col);
-    const R lap_T = Txx + Tyy + Tzz;
-    const Thermo<R> th = thermo(a.ph, T.c, T.p1, X + 4 * (size_t)N + (size_t)col * g.NzY, k, nzy, Tx, Ty, Tz,
-                                lap_T, dz_k, rho);
-    scr[c] = mu_sgs;
-    scr[(size_t)N + c] = S11;
-    scr[2 * (size_t)N + c] = S12;
-    scr[3 * (size_t)N + c] = S13;
-    scr[4 * (size_t)N + c] = S22;
-    scr[5 * (size_t)N + c] = S23;
-    scr[6 * (size_t)N + c] = S33;
-    scr[7 * (size_t)N + c] = th.nu * th.T_RHS_tmp / T.c;
-    if (k == 0) {
-        // wall shear from the k = 0 plane (pde.cu:767-772)
-        const R a1 = th.mu * uz, a2 = th.mu * vz;
-        const R tau_w = rsqrt_(a1 * a1 + a2 * a2);
-        a.utau[col] = rsqrt_(tau_w / rho);
-    }
 }
 
 // RK update of one value: returns the next-stage (or final) value, updates acc.
@@ -251,230 +120,386 @@ __device__ __forceinline__ bool stage_reads_acc(int method, int stage)
 }
 
 // ---------------------------------------------------------------------------
-// pass 2: right-hand side + SGS divergence + RK update (pde.cu:139-787,
-// turbulence.cu:255-454)
+// wall friction velocity of every column from its k = 0 plane
+// (pde.cu:767-772: tau_w = sqrt((mu uz)^2 + (mu vz)^2), u_tau = sqrt(tau_w/rho))
 template <class R>
-__global__ void __launch_bounds__(256) k_stage_rhs(const StageArgs<R> a)
+__global__ void __launch_bounds__(128) k_utau(const StageArgs<R> a)
 {
     const Geom &g = a.g;
-    const Phys &ph = a.ph;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.N) return;
-    const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz, N = g.N;
-    const int k = c % Nz, col = c / Nz, j = col % Ny, i = col / Ny;
-    const int ip1 = wrap_p(i + 1, Nx - 1), im1 = wrap_p(i - 1, Nx - 1);
-    const int ip2 = wrap_p(i + 2, Nx - 1), im2 = wrap_p(i - 2, Nx - 1);
-    const int jp1 = wrap_p(j + 1, Ny - 1), jm1 = wrap_p(j - 1, Ny - 1);
-    const int jp2 = wrap_p(j + 2, Ny - 1), jm2 = wrap_p(j - 2, Ny - 1);
-    const R *__restrict__ X = a.X;
-    const size_t cb = (size_t)col * Nz;
-    const size_t cxp = ((size_t)ip1 * Ny + j) * Nz + k, cxm = ((size_t)im1 * Ny + j) * Nz + k;
-    const size_t cxp2 = ((size_t)ip2 * Ny + j) * Nz + k, cxm2 = ((size_t)im2 * Ny + j) * Nz + k;
-    const size_t cyp = ((size_t)i * Ny + jp1) * Nz + k, cym = ((size_t)i * Ny + jm1) * Nz + k;
-    const size_t cyp2 = ((size_t)i * Ny + jp2) * Nz + k, cym2 = ((size_t)i * Ny + jm2) * Nz + k;
-    const R dx = (R)ph.dx, dy = (R)ph.dy;
-    const R inv2dx = (R)(1.0 / (2 * ph.dx)), inv2dy = (R)(1.0 / (2 * ph.dy));
-    const R invdx2 = (R)(1.0 / (ph.dx * ph.dx)), invdy2 = (R)(1.0 / (ph.dy * ph.dy));
-    (void)dx;
-    (void)dy;
-    const double *zc = g.zc;
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= g.Nx * g.Ny) return;
+    const int Nz = g.Nz, N = g.N;
+    const R *X = a.X + (size_t)col * Nz;
+    const R w0 = (R)g.zc[ZF0 * Nz], w1 = (R)g.zc[ZF1 * Nz], w2 = (R)g.zc[ZF2 * Nz];
+    const R uz = w0 * X[0] + w1 * X[1] + w2 * X[2];
+    const R vz = w0 * X[N] + w1 * X[N + 1] + w2 * X[N + 2];
+    const R T = X[3 * (size_t)N];
+    const R rho = a.pr.Trho / T;
+    R mu = a.pr.mu;
+    if (a.ph.sutherland_viscosity == 1)
+        mu = R(1.716e-5) * rpow(T / R(273.15), R(1.5)) * (R(273.15) + R(110.4)) / (T + R(110.4));
+    const R a1 = mu * uz, a2 = mu * vz;
+    const R tau_w = rsqrt_(a1 * a1 + a2 * a2);
+    a.utau[col] = rsqrt_(tau_w / rho);
+}
 
-    R kval[4];    // u, v, w, T right-hand sides
-    R Tx, Ty, Tz, Txx, Tyy, Tzz, rho, nu_t;
-    R Yc = R(0), kY = R(0);
-    const int nzy = __ldg(g.nzy + col);
+// Shared-memory tile of one stage: TI x TJ x KZ cells, state halo 2 (4 fields)
+// and SGS-input halo 1 (8 fields + fuel).  Offsets are relative to the tile
+// origin; (ii, jj, kk) in [-2, T+1] for the state and [-1, T] for the rest.
+template <class R, int TI, int TJ, int KZ> struct Tile {
+    static constexpr int SI = TI + 4, SJ = TJ + 4, SK = KZ + 4, SR = SI * SJ * SK;
+    static constexpr int GI = TI + 2, GJ = TJ + 2, GK = KZ + 2, GR = GI * GJ * GK;
+    static constexpr int NCOL = GI * GJ, CELLS = TI * TJ * KZ;
+    static constexpr size_t bytes()
     {
-        ZN<R> Z[4];
-        R f0[4], fxp[4], fxm[4], fxp2[4], fxm2[4], fyp[4], fym[4], fyp2[4], fym2[4];
-#pragma unroll
-        for (int f = 0; f < 4; f++) {
-            const R *Xf = X + (size_t)f * N;
-            load_col(Z[f], Xf + cb, k, Nz, 3);
-            f0[f] = Z[f].c;
-            fxp[f] = Xf[cxp]; fxm[f] = Xf[cxm]; fxp2[f] = Xf[cxp2]; fxm2[f] = Xf[cxm2];
-            fyp[f] = Xf[cyp]; fym[f] = Xf[cym]; fyp2[f] = Xf[cyp2]; fym2[f] = Xf[cym2];
-        }
-        const R u = f0[0], v = f0[1], w = f0[2], T = f0[3];
-        rho = (R)ph.T_inf * (R)ph.rho_inf / T;
-        const R u_plu = rmax(u, R(0)), u_min = rmin(u, R(0));
-        const R v_plu = rmax(v, R(0)), v_min = rmin(v, R(0));
-        const R w_plu = rmax(w, R(0)), w_min = rmin(w, R(0));
-        R adv[4], lap[4];
-#pragma unroll
-        for (int f = 0; f < 4; f++) {
-            const R im = (R(3) * f0[f] - R(4) * fxm[f] + fxm2[f]) * inv2dx;
-            const R ip = (R(-3) * f0[f] + R(4) * fxp[f] - fxp2[f]) * inv2dx;
-            const R jm = (R(3) * f0[f] - R(4) * fym[f] + fym2[f]) * inv2dy;
-            const R jp = (R(-3) * f0[f] + R(4) * fyp[f] - fyp2[f]) * inv2dy;
-            const R km = dz_km(Z[f], zc, Nz, k), kp = dz_kp(Z[f], zc, Nz, k);
-            adv[f] = (u_plu * im + u_min * ip) + (v_plu * jm + v_min * jp) + (w_plu * km + w_min * kp);
-            const R fxx = (fxp[f] - R(2) * f0[f] + fxm[f]) * invdx2;
-            const R fyy = (fyp[f] - R(2) * f0[f] + fym[f]) * invdy2;
-            const R fzz = dz_2(Z[f], zc, Nz, k);
-            lap[f] = fxx + fyy + fzz;
-            if (f == 3) { Txx = fxx; Tyy = fyy; Tzz = fzz; }
-        }
-        Tx = (fxp[3] - fxm[3]) * inv2dx;
-        Ty = (fyp[3] - fym[3]) * inv2dy;
-        Tz = dz_1(Z[3], zc, Nz, k);
-        const R dz_k = zcoef<R>(zc, ZDZ, Nz, k);
-        const Thermo<R> th = thermo(ph, T, Z[3].p1, X + 4 * (size_t)N + (size_t)col * g.NzY, k, nzy, Tx, Ty, Tz,
-                                    lap[3], dz_k, rho);
-        Yc = th.Y;
-        kY = -(R)ph.Y_f * th.K_T * Yc;
-        const R T_RHS = (ph.temperature_convection == 0) ? th.T_RHS_tmp - (u * Tx + v * Ty + w * Tz)
-                                                          : th.T_RHS_tmp - adv[3];
-        const R mod_U = rsqrt_(u * u + v * v + w * w);
-        const R cd = (R)(0.5 * ph.C_d * ph.alpha_s * ph.sigma_s);
-        const R F_x = -cd * Yc * mod_U * u;
-        const R F_y = -cd * Yc * mod_U * v;
-        const R F_z = (R)ph.g * (rho - (R)ph.rho_inf) / rho - cd * Yc * mod_U * w;
-        nu_t = th.nu;
-        kval[0] = th.nu * lap[0] - adv[0] + F_x;
-        kval[1] = th.nu * lap[1] - adv[1] + F_y;
-        kval[2] = th.nu * lap[2] - adv[2] + F_z;
-        kval[3] = T_RHS;
+        return sizeof(R) * (4 * (size_t)SR + 9 * (size_t)GR + 2 * (size_t)NCOL + (size_t)GK * KROW) +
+               sizeof(int) * 2 * (size_t)NCOL;
     }
-    // ---- SGS divergence with Van Driest damping (turbulence.cu:255-454) ----
-    {
-        const R *__restrict__ S = a.scr;
-        const R nu = (R)ph.mu / rho;
-        (void)nu_t;
-        const R inv_avd_nu = R(1) / (R)kAVD / nu;
-        const double *topo = g.topo;
-        const double zk = __ldg(g.z + k);
-        const R ut0 = a.utau[col];
-        auto zibm = [&](int ci, int kk) -> R {
-            const double h = __ldg(topo + ci);
-            const double d = __ldg(g.z + kk) - h;
-            return (R)(d > 0.0 ? d : 0.0);
-        };
-        (void)zk;
-        auto fw = [&](R zi, R ut) -> R { return R(1) - rexp(-zi * ut * inv_avd_nu); };
-        const int colxp = ip1 * Ny + j, colxm = im1 * Ny + j, colyp = i * Ny + jp1, colym = i * Ny + jm1;
-        R mu_c = S[c];
-        const R S11 = S[(size_t)N + c], S12 = S[2 * (size_t)N + c], S13 = S[3 * (size_t)N + c];
-        const R S22 = S[4 * (size_t)N + c], S23 = S[5 * (size_t)N + c], S33 = S[6 * (size_t)N + c];
-        R mu_xp = S[cxp], mu_xm = S[cxm], mu_yp = S[cyp], mu_ym = S[cym];
-        const R f_c = fw(zibm(col, k), ut0);
-        const R f_xp = fw(zibm(colxp, k), a.utau[colxp]);
-        const R f_xm = fw(zibm(colxm, k), a.utau[colxm]);
-        const R f_yp = fw(zibm(colyp, k), a.utau[colyp]);
-        const R f_ym = fw(zibm(colym, k), a.utau[colym]);
-        mu_c *= f_c * f_c;
-        mu_xm *= f_xm * f_xm;
-        mu_xp *= f_xp * f_xp;
-        mu_ym *= f_ym * f_ym;
-        mu_yp *= f_yp * f_yp;
-        R mu_km1 = 0, S13_km1 = 0, S23_km1 = 0, S33_km1 = 0, dU_km1 = 0;
-        R mu_kp1 = 0, S13_kp1 = 0, S23_kp1 = 0, S33_kp1 = 0, dU_kp1 = 0;
-        if (k > 0) {
-            const size_t m = c - 1;
-            const R f = fw(zibm(col, k - 1), ut0);
-            mu_km1 = S[m] * (f * f);
-            S13_km1 = S[3 * (size_t)N + m]; S23_km1 = S[5 * (size_t)N + m]; S33_km1 = S[6 * (size_t)N + m];
-            dU_km1 = S[7 * (size_t)N + m];
+    R *st;    // [4][SR]  u, v, w, T
+    R *gs;    // [8][GR]  mu_sgs, S11, S12, S13, S22, S23, S33, divU
+    R *gy;    // [GR]     fuel fraction (0 above the column's fuel top)
+    R *kr;    // [GK][KROW] z-stencil rows for k0-1 .. k0+KZ
+    R *ctopo; // [NCOL]   terrain height of the halo-1 columns
+    R *cut_;  // [NCOL]   wall friction velocity of the halo-1 columns
+    int *cnzy, *ccut;
+    __device__ static int s(int ii, int jj, int kk) { return ((ii + 2) * SJ + (jj + 2)) * SK + (kk + 2); }
+    __device__ static int q(int ii, int jj, int kk) { return ((ii + 1) * GJ + (jj + 1)) * GK + (kk + 1); }
+    __device__ static int cq(int ii, int jj) { return (ii + 1) * GJ + (jj + 1); }
+    __device__ R &S(int f, int ii, int jj, int kk) { return st[f * SR + s(ii, jj, kk)]; }
+    __device__ R &G(int f, int ii, int jj, int kk) { return gs[f * GR + q(ii, jj, kk)]; }
+    __device__ R K(int kk, int e) const { return kr[(kk + 1) * KROW + e]; }
+};
+
+// upwind derivative from 5 weights (zero weights leave the sum unchanged)
+template <class R> __device__ __forceinline__ R dz5(const R *w, R m2, R m1, R c, R p1, R p2)
+{
+    return w[0] * m2 + w[1] * m1 + w[2] * c + w[3] * p1 + w[4] * p2;
+}
+
+// One RK stage for a TI x TJ x KZ tile (reference RHS pde.cu:139-787,
+// turbulence.cu:255-454, RK combination solver.cu:14-93):
+//   1. column tables, z rows, stage input with halo 2 -> shared memory
+//   2. SGS inputs (raw mu_sgs, strain S', divergence source) on the tile and
+//      its halo 1 -> shared memory
+//   3. per tile cell: advection, diffusion, forces, reaction, SGS divergence,
+//      RK update.  Cells the boundary rules overwrite (k <= cut node, top) are
+//      left to k_stage_bc; the values it needs are stored in a.bc.
+template <class R, int TI, int TJ, int KZ, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_stage_fused(const StageArgs<R> a)
+{
+    using TL = Tile<R, TI, TJ, KZ>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TL t;
+    t.st = reinterpret_cast<R *>(smem_raw);
+    t.gs = t.st + 4 * TL::SR;
+    t.gy = t.gs + 8 * TL::GR;
+    t.kr = t.gy + TL::GR;
+    t.ctopo = t.kr + TL::GK * KROW;
+    t.cut_ = t.ctopo + TL::NCOL;
+    t.cnzy = reinterpret_cast<int *>(t.cut_ + TL::NCOL);
+    t.ccut = t.cnzy + TL::NCOL;
+    const Geom &g = a.g;
+    const PhysR<R> &p = a.pr;
+    const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz, N = g.N;
+    const int k0 = blockIdx.x * KZ, j0 = blockIdx.y * TJ, i0 = blockIdx.z * TI;
+    const R *__restrict__ X = a.X;
+
+    // ---- 1a. column tables (halo 1) and z-stencil rows
+    for (int c = threadIdx.x; c < TL::NCOL; c += blockDim.x) {
+        const int jj = c % TL::GJ - 1, ii = c / TL::GJ - 1;
+        const int gi = i0 + ii, gj = j0 + jj;
+        R tp = R(0), ut = R(0);
+        int nz = 0, ct = 0;
+        if (gi <= Nx && gj <= Ny) {
+            const int col = wrap_p(gi, Nx - 1) * Ny + wrap_p(gj, Ny - 1);
+            tp = (R)__ldg(g.topo + col);
+            ut = __ldg(a.utau + col);
+            nz = __ldg(g.nzy + col);
+            ct = __ldg(g.cut + col);
         }
-        if (k < Nz - 1) {
-            const size_t m = c + 1;
-            const R f = fw(zibm(col, k + 1), ut0);
-            mu_kp1 = S[m] * (f * f);
-            S13_kp1 = S[3 * (size_t)N + m]; S23_kp1 = S[5 * (size_t)N + m]; S33_kp1 = S[6 * (size_t)N + m];
-            dU_kp1 = S[7 * (size_t)N + m];
+        t.ctopo[c] = tp;
+        t.cut_[c] = ut;
+        t.cnzy[c] = nz;
+        t.ccut[c] = ct;
+    }
+    for (int c = threadIdx.x; c < TL::GK * KROW; c += blockDim.x) {
+        const int gk = k0 - 1 + c / KROW;
+        t.kr[c] = (gk >= 0 && gk < Nz) ? __ldg(a.krow + (size_t)gk * KROW + c % KROW) : R(0);
+    }
+    // ---- 1b. state tile with halo 2 (periodic in x, y; zero outside 0..Nz-1)
+    for (int c = threadIdx.x; c < TL::SR; c += blockDim.x) {
+        const int kk = c % TL::SK - 2, jj = (c / TL::SK) % TL::SJ - 2, ii = c / (TL::SK * TL::SJ) - 2;
+        int gi = i0 + ii, gj = j0 + jj;
+        const int gk = k0 + kk;
+        R v0 = R(0), v1 = R(0), v2 = R(0), v3 = R(0);
+        if (gk >= 0 && gk < Nz && gi <= Nx + 1 && gj <= Ny + 1) {
+            gi = wrap_p(gi, Nx - 1);
+            gj = wrap_p(gj, Ny - 1);
+            const size_t o = ((size_t)gi * Ny + gj) * Nz + gk;
+            v0 = __ldg(X + o);
+            v1 = __ldg(X + N + o);
+            v2 = __ldg(X + 2 * (size_t)N + o);
+            v3 = __ldg(X + 3 * (size_t)N + o);
         }
-        const R mu_x = (mu_xp - mu_xm) * inv2dx, mu_y = (mu_yp - mu_ym) * inv2dy;
-        const R S11_x = (S[(size_t)N + cxp] - S[(size_t)N + cxm]) * inv2dx;
-        const R S12_x = (S[2 * (size_t)N + cxp] - S[2 * (size_t)N + cxm]) * inv2dx;
-        const R S13_x = (S[3 * (size_t)N + cxp] - S[3 * (size_t)N + cxm]) * inv2dx;
-        const R S21_y = (S[2 * (size_t)N + cyp] - S[2 * (size_t)N + cym]) * inv2dy;
-        const R S22_y = (S[4 * (size_t)N + cyp] - S[4 * (size_t)N + cym]) * inv2dy;
-        const R S23_y = (S[5 * (size_t)N + cyp] - S[5 * (size_t)N + cym]) * inv2dy;
-        const R dU_x = (S[7 * (size_t)N + cxp] - S[7 * (size_t)N + cxm]) * inv2dx;
-        const R dU_y = (S[7 * (size_t)N + cyp] - S[7 * (size_t)N + cym]) * inv2dy;
-        R mu_z, S31_z, S32_z, S33_z, dU_z;
-        if (k == 0 || k == Nz - 1) {
-            // one-sided at the walls: neighbours k+1,k+2 (bottom) or k-1,k-2 (top)
-            const int k2 = (k == 0) ? k + 2 : k - 2;
-            const size_t m2 = cb + k2;
-            const R f = fw(zibm(col, k2), ut0);
-            const R mu2 = S[m2] * (f * f);
-            ZN<R> zm, z13, z23, z33, zd;
-            const R dUc = S[7 * (size_t)N + c];
-            if (k == 0) {
-                zm = {0, 0, 0, mu_c, mu_kp1, mu2, 0};
-                z13 = {0, 0, 0, S13, S13_kp1, S[3 * (size_t)N + m2], 0};
-                z23 = {0, 0, 0, S23, S23_kp1, S[5 * (size_t)N + m2], 0};
-                z33 = {0, 0, 0, S33, S33_kp1, S[6 * (size_t)N + m2], 0};
-                zd = {0, 0, 0, dUc, dU_kp1, S[7 * (size_t)N + m2], 0};
-                mu_z = dz_f(zm, zc, Nz, k); S31_z = dz_f(z13, zc, Nz, k); S32_z = dz_f(z23, zc, Nz, k);
-                S33_z = dz_f(z33, zc, Nz, k); dU_z = dz_f(zd, zc, Nz, k);
-            } else {
-                zm = {0, mu2, mu_km1, mu_c, 0, 0, 0};
-                z13 = {0, S[3 * (size_t)N + m2], S13_km1, S13, 0, 0, 0};
-                z23 = {0, S[5 * (size_t)N + m2], S23_km1, S23, 0, 0, 0};
-                z33 = {0, S[6 * (size_t)N + m2], S33_km1, S33, 0, 0, 0};
-                zd = {0, S[7 * (size_t)N + m2], dU_km1, dUc, 0, 0, 0};
-                mu_z = dz_b(zm, zc, Nz, k); S31_z = dz_b(z13, zc, Nz, k); S32_z = dz_b(z23, zc, Nz, k);
-                S33_z = dz_b(z33, zc, Nz, k); dU_z = dz_b(zd, zc, Nz, k);
-            }
+        t.st[c] = v0;
+        t.st[TL::SR + c] = v1;
+        t.st[2 * TL::SR + c] = v2;
+        t.st[3 * TL::SR + c] = v3;
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < TL::GR; c += blockDim.x) {
+        const int kk = c % TL::GK - 1, jj = (c / TL::GK) % TL::GJ - 1, ii = c / (TL::GK * TL::GJ) - 1;
+        const int gi = i0 + ii, gj = j0 + jj, gk = k0 + kk;
+        R y = R(0);
+        if (gk >= 0 && gi <= Nx && gj <= Ny && gk < t.cnzy[TL::cq(ii, jj)]) {
+            const int col = wrap_p(gi, Nx - 1) * Ny + wrap_p(gj, Ny - 1);
+            y = __ldg(X + 4 * (size_t)N + (size_t)col * g.NzY + gk);
+        }
+        t.gy[c] = y;
+    }
+    __syncthreads();
+
+    const int smu = a.ph.sutherland_viscosity, sk = a.ph.sutherland_conductivity;
+
+    // ---- 2. SGS inputs on the tile and its halo 1 (pde.cu:632-765).  Needed
+    //        set: tile columns on k0-1 .. k0+KZ, side columns on k0 .. k0+KZ-1.
+    constexpr int NA = TI * TJ * (KZ + 2), NB = 2 * TJ * KZ, NC = TI * 2 * KZ;
+    for (int c = threadIdx.x; c < NA + NB + NC; c += blockDim.x) {
+        int ii, jj, kk;
+        if (c < NA) {
+            kk = c % (KZ + 2) - 1;
+            jj = (c / (KZ + 2)) % TJ;
+            ii = c / ((KZ + 2) * TJ);
+        } else if (c < NA + NB) {
+            const int d = c - NA;
+            kk = d % KZ;
+            jj = (d / KZ) % TJ;
+            ii = (d / (KZ * TJ)) ? TI : -1;
         } else {
-            const R wc = zcoef<R>(zc, ZC, Nz, k);
-            mu_z = (mu_kp1 - mu_km1) * wc;
-            S31_z = (S13_kp1 - S13_km1) * wc;
-            S32_z = (S23_kp1 - S23_km1) * wc;
-            S33_z = (S33_kp1 - S33_km1) * wc;
-            dU_z = (dU_kp1 - dU_km1) * wc;
+            const int d = c - NA - NB;
+            kk = d % KZ;
+            jj = ((d / KZ) % 2) ? TJ : -1;
+            ii = d / (2 * KZ);
         }
-        const R div_S_x = S11_x + S21_y + S31_z;
-        const R div_S_y = S12_x + S22_y + S32_z;
-        const R div_S_z = S13_x + S23_y + S33_z;
-        const R inv_rho = R(1) / rho;
-        const R sgs_x = R(-2) * (mu_x * S11 + mu_y * S12 + mu_z * S13 + mu_c * div_S_x) * inv_rho;
-        const R sgs_y = R(-2) * (mu_x * S12 + mu_y * S22 + mu_z * S23 + mu_c * div_S_y) * inv_rho;
-        const R sgs_z = R(-2) * (mu_x * S13 + mu_y * S23 + mu_z * S33 + mu_c * div_S_z) * inv_rho;
-        const R sgs_q = -(mu_x * Tx + mu_y * Ty + mu_z * Tz + mu_c * (Txx + Tyy + Tzz)) / (rho * (R)ph.Pr);
-        const R third = R(1) / R(3);
-        (void)third;
-        kval[0] += -sgs_x + dU_x / R(3);
-        kval[1] += -sgs_y + dU_y / R(3);
-        kval[2] += -sgs_z + dU_z / R(3);
-        kval[3] -= sgs_q;
+        const int gk = k0 + kk;
+        if (gk < 0 || gk >= Nz || i0 + ii > Nx || j0 + jj > Ny) continue;
+        const R *pu = &t.S(0, ii, jj, 0), *pv = &t.S(1, ii, jj, 0), *pw = &t.S(2, ii, jj, 0), *pT = &t.S(3, ii, jj, 0);
+        const R ux = (t.S(0, ii + 1, jj, kk) - t.S(0, ii - 1, jj, kk)) * p.inv2dx;
+        const R uy = (t.S(0, ii, jj + 1, kk) - t.S(0, ii, jj - 1, kk)) * p.inv2dy;
+        const R vx = (t.S(1, ii + 1, jj, kk) - t.S(1, ii - 1, jj, kk)) * p.inv2dx;
+        const R vy = (t.S(1, ii, jj + 1, kk) - t.S(1, ii, jj - 1, kk)) * p.inv2dy;
+        const R wx = (t.S(2, ii + 1, jj, kk) - t.S(2, ii - 1, jj, kk)) * p.inv2dx;
+        const R wy = (t.S(2, ii, jj + 1, kk) - t.S(2, ii, jj - 1, kk)) * p.inv2dy;
+        const R Tc = pT[kk];
+        const R Txp = t.S(3, ii + 1, jj, kk), Txm = t.S(3, ii - 1, jj, kk);
+        const R Typ = t.S(3, ii, jj + 1, kk), Tym = t.S(3, ii, jj - 1, kk);
+        const R Tx = (Txp - Txm) * p.inv2dx, Ty = (Typ - Tym) * p.inv2dy;
+        const R Txx = (Txp - R(2) * Tc + Txm) * p.invdx2, Tyy = (Typ - R(2) * Tc + Tym) * p.invdy2;
+        R uz, vz, wz, Tz, Tzz;
+        if (gk > 0 && gk < Nz - 1) {
+            const R wc = t.K(kk, RD1);
+            uz = (pu[kk + 1] - pu[kk - 1]) * wc;
+            vz = (pv[kk + 1] - pv[kk - 1]) * wc;
+            wz = (pw[kk + 1] - pw[kk - 1]) * wc;
+            Tz = (pT[kk + 1] - pT[kk - 1]) * wc;
+            Tzz = t.K(kk, RD2) * pT[kk - 1] + t.K(kk, RD2 + 1) * Tc + t.K(kk, RD2 + 2) * pT[kk + 1];
+        } else {
+            // walls: one-sided stencils from the double table (planes k = 0 and Nz-1 only)
+            const double *zc = g.zc;
+            const bool bot = (gk == 0);
+            auto d1 = [&](const R *f) -> R {
+                if (bot) return (R)zc[ZF0 * Nz] * f[kk] + (R)zc[ZF1 * Nz] * f[kk + 1] + (R)zc[ZF2 * Nz] * f[kk + 2];
+                return (R)zc[ZB0 * Nz + gk] * f[kk - 2] + (R)zc[ZB1 * Nz + gk] * f[kk - 1] + (R)zc[ZB2 * Nz + gk] * f[kk];
+            };
+            uz = d1(pu);
+            vz = d1(pv);
+            wz = d1(pw);
+            Tz = d1(pT);
+            // the backward 4-point form needs k-3, inside the tile unless the
+            // top plane is alone in its tile (then no cell of this tile needs it)
+            const R m3 = (kk >= 1) ? pT[kk - 3] : R(0), p3 = (kk <= KZ - 2) ? pT[kk + 3] : R(0);
+            Tzz = bot ? (R)zc[ZFF0 * Nz] * Tc + (R)zc[ZFF1 * Nz] * pT[kk + 1] + (R)zc[ZFF2 * Nz] * pT[kk + 2] +
+                            (R)zc[ZFF3 * Nz] * p3
+                      : (R)zc[ZBB0 * Nz + gk] * m3 + (R)zc[ZBB1 * Nz + gk] * pT[kk - 2] +
+                            (R)zc[ZBB2 * Nz + gk] * pT[kk - 1] + (R)zc[ZBB3 * Nz + gk] * Tc;
+        }
+        const R rho = p.Trho / Tc;
+        const R S11 = R(2) * ux / R(3) - (vy + wz) / R(3);
+        const R S22 = R(2) * vy / R(3) - (ux + wz) / R(3);
+        const R S33 = R(2) * wz / R(3) - (ux + vy) / R(3);
+        const R mod_S = rsqrt_(R(2) * (ux * ux + vy * vy + wz * wz) + (uz + wx) * (uz + wx) + (vx + uy) * (vx + uy) +
+                               (wy + vz) * (wy + vz));
+        const int nzy = t.cnzy[TL::cq(ii, jj)];
+        const Thermo<R> th = thermo(p, smu, sk, Tc, pT[kk + 1], t.gy[TL::q(ii, jj, kk)], gk, nzy, Tx, Ty, Tz,
+                                    Txx + Tyy + Tzz, t.K(kk, RDZ), rho);
+        t.G(0, ii, jj, kk) = rho * t.K(kk, RDEL2) * mod_S;
+        t.G(1, ii, jj, kk) = S11;
+        t.G(2, ii, jj, kk) = R(0.5) * (uy + vx);
+        t.G(3, ii, jj, kk) = R(0.5) * (uz + wx);
+        t.G(4, ii, jj, kk) = S22;
+        t.G(5, ii, jj, kk) = R(0.5) * (wy + vz);
+        t.G(6, ii, jj, kk) = S33;
+        t.G(7, ii, jj, kk) = th.nu * th.T_RHS_tmp / Tc;
     }
-    // ---- values the column boundary pass needs -----------------------------
-    const int kc = __ldg(g.cut + col);
-    R *bc = a.bc + (size_t)col * kBcSlots;
-    if (k == kc + 1) { bc[0] = kval[3]; bc[2] = (k < nzy) ? kY : R(0); }
-    if (k == kc + 2) { bc[1] = kval[3]; bc[3] = (k < nzy) ? kY : R(0); }
-    if (k == Nz - 2) { bc[4] = kval[0]; bc[5] = kval[1]; bc[6] = kval[2]; bc[7] = kval[3]; }
-    if (k == Nz - 3) { bc[8] = kval[0]; bc[9] = kval[1]; bc[10] = kval[2]; bc[11] = kval[3]; }
-    // ---- RK update of every value the boundary rules leave alone ------------
-    const bool managed = (k <= kc) || (k == Nz - 1);
+    __syncthreads();
+
+    // ---- 3. right-hand side, SGS divergence, RK update per tile cell
     const R an = (R)a.a_next;
     const bool rd = stage_reads_acc(a.method, a.stage), kp = stage_keeps_acc(a.method, a.stage);
-    if (!managed) {
+    for (int c = threadIdx.x; c < TL::CELLS; c += blockDim.x) {
+        const int kk = c % KZ, jj = (c / KZ) % TJ, ii = c / (KZ * TJ);
+        const int gi = i0 + ii, gj = j0 + jj, gk = k0 + kk;
+        if (gi >= Nx || gj >= Ny || gk >= Nz) continue;
+        const int col = gi * Ny + gj;
+        const int cc = TL::cq(ii, jj);
+        const int kc = t.ccut[cc], nzy = t.cnzy[cc];
+        const bool live = (gk > kc) && (gk < Nz - 1);                 // not overwritten by the boundary rules
+        const bool ylive = (gk < g.NzY) && !(gk <= kc && gk < nzy);   // fuel value this pass updates
+        if (!live && !ylive) continue;
+        const size_t cg = (size_t)col * Nz + gk;
+        // start the RK operand loads early
+        R ynv[4], accv[4];
+        if (live) {
 #pragma unroll
-        for (int f = 0; f < 4; f++) {
-            const size_t o = (size_t)f * N + c;
-            R accv = rd ? a.acc[o] : R(0);
-            a.Xout[o] = rk_update(a.method, a.stage, kval[f], a.yn[o], accv, an);
-            if (kp) a.acc[o] = accv;
+            for (int f = 0; f < 4; f++) {
+                ynv[f] = a.yn[(size_t)f * N + cg];
+                accv[f] = rd ? a.acc[(size_t)f * N + cg] : R(0);
+            }
         }
-    }
-    if (k < g.NzY) {
-        // fuel above the column's fuel top is never used; its k-value is 0
-        const bool ymanaged = (k <= kc) && (k < nzy);
-        if (!ymanaged) {
-            const size_t o = 4 * (size_t)N + (size_t)col * g.NzY + k;
-            const R kv = (k < nzy) ? kY : R(0);
-            R accv = rd ? a.acc[o] : R(0);
-            a.Xout[o] = rk_update(a.method, a.stage, kv, a.yn[o], accv, an);
-            if (kp) a.acc[o] = accv;
+        const size_t oY = 4 * (size_t)N + (size_t)col * g.NzY + gk;
+        R ynY = R(0), accY = R(0);
+        if (ylive) {
+            ynY = a.yn[oY];
+            accY = rd ? a.acc[oY] : R(0);
+        }
+        R kY = R(0);
+        if (live) {
+            const R *kmw = &t.kr[(kk + 1) * KROW + RKM], *kpw = &t.kr[(kk + 1) * KROW + RKP];
+            const R d2m = t.K(kk, RD2), d20 = t.K(kk, RD2 + 1), d2p = t.K(kk, RD2 + 2);
+            const R u = t.S(0, ii, jj, kk), v = t.S(1, ii, jj, kk), w = t.S(2, ii, jj, kk), T = t.S(3, ii, jj, kk);
+            const R u_plu = rmax(u, R(0)), u_min = rmin(u, R(0));
+            const R v_plu = rmax(v, R(0)), v_min = rmin(v, R(0));
+            const R w_plu = rmax(w, R(0)), w_min = rmin(w, R(0));
+            // advection (upwind) and Laplacian of one field from the shared tile
+            auto adv_lap = [&](int f, R f0, R &adv, R &fxx, R &fyy, R &fzz, R &fx, R &fy, R &fz) {
+                const R *pc = &t.S(f, ii, jj, 0);
+                const R xm = t.S(f, ii - 1, jj, kk), xp = t.S(f, ii + 1, jj, kk);
+                const R xm2 = t.S(f, ii - 2, jj, kk), xp2 = t.S(f, ii + 2, jj, kk);
+                const R ym = t.S(f, ii, jj - 1, kk), yp = t.S(f, ii, jj + 1, kk);
+                const R ym2 = t.S(f, ii, jj - 2, kk), yp2 = t.S(f, ii, jj + 2, kk);
+                const R zm2 = pc[kk - 2], zm = pc[kk - 1], zp = pc[kk + 1], zp2 = pc[kk + 2];
+                const R im = (R(3) * f0 - R(4) * xm + xm2) * p.inv2dx;
+                const R ip = (R(-3) * f0 + R(4) * xp - xp2) * p.inv2dx;
+                const R jm = (R(3) * f0 - R(4) * ym + ym2) * p.inv2dy;
+                const R jp = (R(-3) * f0 + R(4) * yp - yp2) * p.inv2dy;
+                const R km = dz5(kmw, zm2, zm, f0, zp, zp2), kpv = dz5(kpw, zm2, zm, f0, zp, zp2);
+                adv = (u_plu * im + u_min * ip) + (v_plu * jm + v_min * jp) + (w_plu * km + w_min * kpv);
+                fxx = (xp - R(2) * f0 + xm) * p.invdx2;
+                fyy = (yp - R(2) * f0 + ym) * p.invdy2;
+                fzz = d2m * zm + d20 * f0 + d2p * zp;
+                fx = (xp - xm) * p.inv2dx;
+                fy = (yp - ym) * p.inv2dy;
+                fz = (zp - zm) * t.K(kk, RD1);
+            };
+            R advT, Txx, Tyy, Tzz, Tx, Ty, Tz;
+            adv_lap(3, T, advT, Txx, Tyy, Tzz, Tx, Ty, Tz);
+            const R rho = p.Trho / T;
+            const Thermo<R> th = thermo(p, smu, sk, T, t.S(3, ii, jj, kk + 1), t.gy[TL::q(ii, jj, kk)], gk, nzy, Tx,
+                                        Ty, Tz, Txx + Tyy + Tzz, t.K(kk, RDZ), rho);
+            kY = -p.Y_f * th.K_T * th.Y;
+            R kval[4];
+            kval[3] = (a.ph.temperature_convection == 0) ? th.T_RHS_tmp - (u * Tx + v * Ty + w * Tz)
+                                                         : th.T_RHS_tmp - advT;
+            const R mod_U = rsqrt_(u * u + v * v + w * w);
+            {
+                R adv, fxx, fyy, fzz, fx, fy, fz;
+                adv_lap(0, u, adv, fxx, fyy, fzz, fx, fy, fz);
+                kval[0] = th.nu * (fxx + fyy + fzz) - adv + (-p.cd * th.Y * mod_U * u);
+                adv_lap(1, v, adv, fxx, fyy, fzz, fx, fy, fz);
+                kval[1] = th.nu * (fxx + fyy + fzz) - adv + (-p.cd * th.Y * mod_U * v);
+                adv_lap(2, w, adv, fxx, fyy, fzz, fx, fy, fz);
+                kval[2] = th.nu * (fxx + fyy + fzz) - adv + (p.g * (rho - p.rho_inf) / rho - p.cd * th.Y * mod_U * w);
+            }
+            // ---- SGS divergence with Van Driest damping (turbulence.cu:255-454)
+            {
+                const R nu = p.mu / rho;
+                const R inv_avd_nu = p.inv_avd / nu;
+                const R zk = t.K(kk, RZ);
+                auto zibm = [&](int q, R zz) -> R {
+                    const R d = zz - t.ctopo[q];
+                    return d > R(0) ? d : R(0);
+                };
+                const int qxp = TL::cq(ii + 1, jj), qxm = TL::cq(ii - 1, jj);
+                const int qyp = TL::cq(ii, jj + 1), qym = TL::cq(ii, jj - 1);
+                const R ut0 = t.cut_[cc];
+                const R fc = van_driest(-zibm(cc, zk) * ut0 * inv_avd_nu);
+                const R fxp_ = van_driest(-zibm(qxp, zk) * t.cut_[qxp] * inv_avd_nu);
+                const R fxm_ = van_driest(-zibm(qxm, zk) * t.cut_[qxm] * inv_avd_nu);
+                const R fyp_ = van_driest(-zibm(qyp, zk) * t.cut_[qyp] * inv_avd_nu);
+                const R fym_ = van_driest(-zibm(qym, zk) * t.cut_[qym] * inv_avd_nu);
+                const R fkm = van_driest(-zibm(cc, t.K(kk - 1, RZ)) * ut0 * inv_avd_nu);
+                const R fkp = van_driest(-zibm(cc, t.K(kk + 1, RZ)) * ut0 * inv_avd_nu);
+                const R mu_c = t.G(0, ii, jj, kk) * (fc * fc);
+                const R mu_xp = t.G(0, ii + 1, jj, kk) * (fxp_ * fxp_), mu_xm = t.G(0, ii - 1, jj, kk) * (fxm_ * fxm_);
+                const R mu_yp = t.G(0, ii, jj + 1, kk) * (fyp_ * fyp_), mu_ym = t.G(0, ii, jj - 1, kk) * (fym_ * fym_);
+                const R mu_kp = t.G(0, ii, jj, kk + 1) * (fkp * fkp), mu_km = t.G(0, ii, jj, kk - 1) * (fkm * fkm);
+                const R S11 = t.G(1, ii, jj, kk), S12 = t.G(2, ii, jj, kk), S13 = t.G(3, ii, jj, kk);
+                const R S22 = t.G(4, ii, jj, kk), S23 = t.G(5, ii, jj, kk), S33 = t.G(6, ii, jj, kk);
+                const R wc = t.K(kk, RD1);
+                const R mu_x = (mu_xp - mu_xm) * p.inv2dx, mu_y = (mu_yp - mu_ym) * p.inv2dy, mu_z = (mu_kp - mu_km) * wc;
+                const R S11_x = (t.G(1, ii + 1, jj, kk) - t.G(1, ii - 1, jj, kk)) * p.inv2dx;
+                const R S12_x = (t.G(2, ii + 1, jj, kk) - t.G(2, ii - 1, jj, kk)) * p.inv2dx;
+                const R S13_x = (t.G(3, ii + 1, jj, kk) - t.G(3, ii - 1, jj, kk)) * p.inv2dx;
+                const R S21_y = (t.G(2, ii, jj + 1, kk) - t.G(2, ii, jj - 1, kk)) * p.inv2dy;
+                const R S22_y = (t.G(4, ii, jj + 1, kk) - t.G(4, ii, jj - 1, kk)) * p.inv2dy;
+                const R S23_y = (t.G(5, ii, jj + 1, kk) - t.G(5, ii, jj - 1, kk)) * p.inv2dy;
+                const R S31_z = (t.G(3, ii, jj, kk + 1) - t.G(3, ii, jj, kk - 1)) * wc;
+                const R S32_z = (t.G(5, ii, jj, kk + 1) - t.G(5, ii, jj, kk - 1)) * wc;
+                const R S33_z = (t.G(6, ii, jj, kk + 1) - t.G(6, ii, jj, kk - 1)) * wc;
+                const R dU_x = (t.G(7, ii + 1, jj, kk) - t.G(7, ii - 1, jj, kk)) * p.inv2dx;
+                const R dU_y = (t.G(7, ii, jj + 1, kk) - t.G(7, ii, jj - 1, kk)) * p.inv2dy;
+                const R dU_z = (t.G(7, ii, jj, kk + 1) - t.G(7, ii, jj, kk - 1)) * wc;
+                const R div_S_x = S11_x + S21_y + S31_z;
+                const R div_S_y = S12_x + S22_y + S32_z;
+                const R div_S_z = S13_x + S23_y + S33_z;
+                const R inv_rho = R(1) / rho;
+                const R sgs_x = R(-2) * (mu_x * S11 + mu_y * S12 + mu_z * S13 + mu_c * div_S_x) * inv_rho;
+                const R sgs_y = R(-2) * (mu_x * S12 + mu_y * S22 + mu_z * S23 + mu_c * div_S_y) * inv_rho;
+                const R sgs_z = R(-2) * (mu_x * S13 + mu_y * S23 + mu_z * S33 + mu_c * div_S_z) * inv_rho;
+                const R sgs_q = -(mu_x * Tx + mu_y * Ty + mu_z * Tz + mu_c * (Txx + Tyy + Tzz)) / (rho * p.Pr);
+                kval[0] += -sgs_x + dU_x / R(3);
+                kval[1] += -sgs_y + dU_y / R(3);
+                kval[2] += -sgs_z + dU_z / R(3);
+                kval[3] -= sgs_q;
+            }
+            // values the column boundary pass needs
+            R *bcs = a.bc + (size_t)col * kBcSlots;
+            if (gk == kc + 1) { bcs[0] = kval[3]; bcs[2] = (gk < nzy) ? kY : R(0); }
+            if (gk == kc + 2) { bcs[1] = kval[3]; bcs[3] = (gk < nzy) ? kY : R(0); }
+            if (gk == Nz - 2) { bcs[4] = kval[0]; bcs[5] = kval[1]; bcs[6] = kval[2]; bcs[7] = kval[3]; }
+            if (gk == Nz - 3) { bcs[8] = kval[0]; bcs[9] = kval[1]; bcs[10] = kval[2]; bcs[11] = kval[3]; }
+#pragma unroll
+            for (int f = 0; f < 4; f++) {
+                const size_t o = (size_t)f * N + cg;
+                a.Xout[o] = rk_update(a.method, a.stage, kval[f], ynv[f], accv[f], an);
+                if (kp) a.acc[o] = accv[f];
+            }
+        } else if (gk < nzy) {
+            // fuel cell whose velocity and temperature the boundary rules set (top plane)
+            const R T = t.S(3, ii, jj, kk);
+            const R K_T = (T > p.T_pc) ? p.A * rexp(-p.T_act / T) * R(1) : R(0);
+            kY = -p.Y_f * K_T * t.gy[TL::q(ii, jj, kk)];
+        }
+        if (ylive) {
+            const R kv = (gk < nzy) ? kY : R(0);
+            a.Xout[oY] = rk_update(a.method, a.stage, kv, ynY, accY, an);
+            if (kp) a.acc[oY] = accY;
         }
     }
 }
 
 // ---------------------------------------------------------------------------
-// pass 3: boundary/IBM k-values per column (pde.cu:14-99) and their RK update
+// boundary/IBM k-values per column (pde.cu:14-99) and their RK update
 template <class R>
 __global__ void __launch_bounds__(128) k_stage_bc(const StageArgs<R> a)
 {
@@ -526,14 +551,42 @@ __global__ void __launch_bounds__(128) k_stage_bc(const StageArgs<R> a)
 
 }  // namespace
 
+// Tile shapes: FP32 8 x 16 x 8 cells (two blocks per SM), FP64 8 x 8 x 8 cells
+// (one block per SM).
+template <class R> struct StageCfg;
+template <> struct StageCfg<float> {
+    static constexpr int TI = 8, TJ = 16, KZ = 8, MINB = 2;
+};
+template <> struct StageCfg<double> {
+    static constexpr int TI = 8, TJ = 8, KZ = 8, MINB = 1;
+};
+
+template <class R> size_t stage_smem_bytes()
+{
+    using C = StageCfg<R>;
+    return Tile<R, C::TI, C::TJ, C::KZ>::bytes();
+}
+template size_t stage_smem_bytes<double>();
+template size_t stage_smem_bytes<float>();
+
+template <class R> cudaError_t stage_set_attributes()
+{
+    using C = StageCfg<R>;
+    return cudaFuncSetAttribute(k_stage_fused<R, C::TI, C::TJ, C::KZ, C::MINB>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<R>());
+}
+template cudaError_t stage_set_attributes<double>();
+template cudaError_t stage_set_attributes<float>();
+
 template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t s, cudaEvent_t *ev)
 {
-    const int nb = (a.g.N + 255) / 256;
-    k_turb_inputs<R><<<nb, 256, 0, s>>>(a);
-    if (ev) cudaEventRecord(ev[0], s);
-    k_stage_rhs<R><<<nb, 256, 0, s>>>(a);
-    if (ev) cudaEventRecord(ev[1], s);
+    using C = StageCfg<R>;
     const int ncol = a.g.Nx * a.g.Ny;
+    k_utau<R><<<(ncol + 127) / 128, 128, 0, s>>>(a);
+    if (ev) cudaEventRecord(ev[0], s);
+    dim3 grid((a.g.Nz + C::KZ - 1) / C::KZ, (a.g.Ny + C::TJ - 1) / C::TJ, (a.g.Nx + C::TI - 1) / C::TI);
+    k_stage_fused<R, C::TI, C::TJ, C::KZ, C::MINB><<<grid, 256, stage_smem_bytes<R>(), s>>>(a);
+    if (ev) cudaEventRecord(ev[1], s);
     k_stage_bc<R><<<(ncol + 127) / 128, 128, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[2], s);
     return cudaGetLastError();

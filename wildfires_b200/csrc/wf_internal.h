@@ -48,6 +48,29 @@ struct Phys {
     int variable_density, velocity_correction_fd;
 };
 
+// Model scalars in the stencil precision R, derived once on the host from
+// Phys so kernels do no double->R conversions.
+template <class R> struct PhysR {
+    R inv2dx, inv2dy, invdx2, invdy2;   // 1/(2 dx), 1/(2 dy), 1/dx^2, 1/dy^2
+    R Trho;                             // T_inf rho_inf (rho = Trho / T)
+    R mu, kT, Y_f, H_C, A, T_act, T_pc, h_c, alpha_s, sigma_s;
+    R T_inf, c_p, rho_inf, cd, g, c12, c4, Pr, inv_avd;
+    R T_min, T_max, Y_min, Y_max;
+};
+
+// Per-k row of z-stencil weights in the stencil precision (branch-free
+// interior stencils; one row per k, KROW entries).
+enum KRow {
+    RKM = 0,    // 5 weights (k-2..k+2) of the upwind derivative "from below"
+    RKP = 5,    // 5 weights (k-2..k+2) of the upwind derivative "from above"
+    RD1 = 10,   // 1/(dz_{k-1} + dz_k): central first derivative (f_{k+1} - f_{k-1}) * RD1
+    RD2 = 11,   // 3 weights (k-1..k+1) of the central second derivative
+    RDZ = 14,   // dz_k
+    RDEL2 = 15, // Smagorinsky length squared
+    RZ = 16,    // z_k
+    KROW = 20
+};
+
 // Grid geometry and immersed-boundary tables (device pointers).
 struct Geom {
     int Nx, Ny, Nz, NzY;        // NzY = Nz_Y_max
@@ -60,9 +83,6 @@ struct Geom {
     const int *cut;             // [Nx*Ny] cut node per column
 };
 
-// Number of turbulence-input fields kept between the two stage passes:
-// raw mu_sgs, S11, S12, S13, S22, S23, S33 and the divergence source divU.
-constexpr int kScratchFields = 8;
 // Per-column values the boundary pass needs from the stage pass:
 // T,Y at cut+1, cut+2 (4) and u,v,w,T at Nz-2, Nz-3 (8).
 constexpr int kBcSlots = 12;
@@ -71,11 +91,12 @@ template <class R>
 struct StageArgs {
     Geom g;
     Phys ph;
+    PhysR<R> pr;
+    const R *krow;   // [Nz][KROW] z-stencil weights in precision R
     const R *X;      // stage input state (packed)
     const R *yn;     // state at the start of the step (packed)
     R *acc;          // RK accumulator of k-values (packed)
     R *Xout;         // next stage input, or y_{n+1} after the last stage
-    R *scr;          // [kScratchFields][N]
     R *utau;         // [Nx*Ny] wall friction velocity from the k = 0 plane
     R *bc;           // [Nx*Ny][kBcSlots]
     double a_next;   // c_{s+1} dt of the next stage input, or dt/6 after the last stage
@@ -87,6 +108,7 @@ struct StageArgs {
 // Launch helpers implemented in the .cu files.
 // ev (optional): one event recorded after each of the 3 kernels, for profiling.
 template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t s, cudaEvent_t *ev = nullptr);
+template <class R> cudaError_t stage_set_attributes();
 
 template <class R>
 struct ProjectArgs {
@@ -110,10 +132,9 @@ template <class R> cudaError_t launch_project(const ProjectArgs<R> &a, cudaStrea
 // FFT descriptor for one transform length, tables in device memory.
 struct FftDesc {
     int n;                  // transform length
-    int m;                  // inner (Stockham) length: n, or the Bluestein length
-    int bluestein;
-    int nfac;
-    int fac[20];            // radices of m, applied in order
+    int m;                  // inner power-of-two length: n, or the Bluestein length >= 2n-1
+    int L;                  // log2(m)
+    int bluestein;          // n is not a power of two
     const double2 *tw;      // exp(-2 pi i j / m), j < m
     const double2 *chirp;   // Bluestein: exp(-i pi j^2 / n), j < n
     const double2 *filt;    // Bluestein: FFT_m of the conjugate chirp filter
