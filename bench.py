@@ -13,7 +13,7 @@ model).  The state (670 MB FP32, 1.3 GB FP64) is larger than the 126 MB L2,
 so no explicit L2 flush is needed between timed steps.
 
 Under torchrun (N > 1) every rank advances its own replica of the workload
-(the single-domain step does not shard) and the reported value
+(the single-domain step has no exchange to shard; replicas only) and the reported value
 is the aggregate over ranks, timed as the max over ranks.
 
 --impl reference times the reference's own CPU implementation (its src/cu
@@ -119,7 +119,15 @@ class ClockSampler:
 
 # ---- algorithmic bytes (roofline model) -------------------------------------
 def kernel_bytes(name, P, prec):
-    """Compulsory DRAM bytes per launch of each kernel kind."""
+    """Compulsory DRAM bytes per launch of each kernel kind.
+
+    A state pass touches S = 4 N + N_Y values of s bytes.  Over the four RK4
+    stages the fused stage kernel reads the stage input 3 times (stage 1 reads
+    y_n, which is its input), y_n 4 times and the accumulator 3 times, and
+    writes the accumulator 3 times and the stage output 4 times: 17 S values
+    per step, 17/4 S per launch.  The pressure kernels move the half spectrum
+    G = Nz (Nx-1) ((Ny-1)/2+1) complex FP64 values once in and once out.
+    """
     r = P.rec
     N = r.Nx * r.Ny * r.Nz
     NY = r.Nx * r.Ny * r.Nz_Y_max
@@ -128,10 +136,8 @@ def kernel_bytes(name, P, prec):
     h1 = (r.Ny - 1) // 2 + 1
     G = (r.Nz) * (r.Nx - 1) * h1 * 16          # spectral slab incl. the top-plane slice
     return {
-        # read X (state) + write 8 SGS-input fields
-        "turb_inputs": s * S + 8 * s * N,
-        # read X, SGS inputs, y_n, acc; write acc, X_next (stage 2/3 form)
-        "stage_rhs": s * S + 8 * s * N + 4 * s * S,
+        "stage_fused": 17 * s * S / 4,
+        "stage_utau": 0,
         "stage_bc": 0,
         # read u, v, w (+ top plane of p); write half spectrum
         "p_rhs_ffty": 3 * s * N + G,
@@ -146,7 +152,8 @@ def kernel_bytes(name, P, prec):
 
 
 def step_model_bytes(P, prec):
-    """Algorithmic bytes per cell-step of the whole step (SURVEY model)."""
+    """Algorithmic bytes per cell-step of the whole step: 17 state passes of the
+    RK4 stages, the pressure solve's spectral traffic and the projection."""
     r = P.rec
     s = 4 if prec == "fp32" else 8
     fY = r.Nz_Y_max / r.Nz

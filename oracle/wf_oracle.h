@@ -14,7 +14,7 @@
  * inside Parameters are used as filled by the parameter parser.
  *
  * Deliberate, documented differences from the reference (all inert for the
- * parity inputs, see DESIGN.md "Reference quirks"):
+ * parity inputs):
  *   - the convective heat-transfer coefficient h_c is evaluated per cell from
  *     the parameter value (the reference overwrites its per-thread copy,
  *     src/cu/pde.cu:698, making the product depend on the launch shape);
