@@ -148,6 +148,35 @@ wf_status wf_profile_phases(wf_ctx *ctx, int nsteps, double *ms, int *launches);
 /* Name of kernel kind q ("stage_rhs", "p_fftx_fwd", ...), or NULL. */
 const char *wf_phase_name(int q);
 
+/* ---- pressure solve without device allocation --------------------------- */
+
+/* One FP64 constant-density pressure solve on DEVICE buffers that performs no
+ * device memory allocation.  This entry point has no counterpart in the
+ * reference; it exists for callers that cannot call cudaMalloc -- code running
+ * inside a framework that owns all device memory through its own pool, code
+ * with a device-memory budget fixed in advance, or code that must not pay for
+ * an allocation on its time-critical path.
+ *
+ * y_np1: packed FP64 state on the device (u, v, w are read); p: Nx*Ny*Nz FP64
+ * pressure on the device, read (top plane) and overwritten exactly as by
+ * wf_pressure.  stream: a cudaStream_t (NULL for the legacy default stream).
+ *
+ * All scratch -- the half-spectrum buffer, FFT and tridiagonal tables, grid --
+ * lives in one fixed device array of 64 MiB inside this library; every device
+ * that loads the library holds that array until the process exits.  The
+ * half-spectrum buffer dominates: Nz*(Nx-1)*((Ny-1)/2+1) 16-byte cells, so a
+ * 128 x 128 x 64 grid needs 8 MiB, 257 x 257 x 64 needs 33 MiB, and
+ * 512 x 512 x 128 does not fit; grids that do not fit are rejected with
+ * WF_ERR_ARG and a message naming the size.  Only variable_density = 0 is
+ * accepted.  The first call on a device looks up the array's device address
+ * and configures the kernels; make that first call before any stream capture.
+ * Every call reuses the same array (and static host staging tables), so calls
+ * that overlap on the GPU or run concurrently from several host threads race;
+ * nothing in the array needs to start at zero, each call writes every element
+ * it reads.  The call returns after the table upload, with the solve enqueued
+ * on the stream. */
+wf_status wf_pressure_noalloc(const Parameters *p, const double *y_np1, double *pr, void *stream);
+
 const char *wf_status_string(wf_status s);
 const char *wf_last_error(void);
 
