@@ -3,7 +3,7 @@
 Every .cu/.cpp file under csrc/ is compiled by nvcc into an object under
 _build/ (rebuilt when the file or any header is newer), then linked into
 wildfires_b200/libwildfires_b200.so with the static CUDA runtime.  The ptxas
-resource report of every kernel is written to _build/ptxas.log.
+resource report of every kernel is written to _build/<source>.ptxas.log.
 """
 import os
 import subprocess
@@ -35,7 +35,6 @@ def build(verbose=False, force=False):
     os.makedirs(BUILD, exist_ok=True)
     hdr_mtime = max(os.path.getmtime(h) for h in _headers())
     objs = []
-    logs = []
     for src in _sources():
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         objs.append(obj)
@@ -47,13 +46,11 @@ def build(verbose=False, force=False):
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
-        logs.append("== %s\n%s%s" % (os.path.basename(src), r.stdout, r.stderr))
+        with open(os.path.join(BUILD, os.path.basename(src) + ".ptxas.log"), "w") as f:
+            f.write(r.stdout + r.stderr)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("nvcc failed on %s" % src)
-    if logs:
-        with open(os.path.join(BUILD, "ptxas.log"), "a") as f:
-            f.write("".join(logs))
     newest = max(os.path.getmtime(o) for o in objs)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-ccbin", "/usr/bin/g++"]

@@ -18,6 +18,7 @@
 // G is (Nz-1+1) x (Nx-1) x h1 complex doubles, s fastest, h1 = (Ny-1)/2+1.
 #include <math.h>
 
+#include "fft.cuh"
 #include "wf_internal.h"
 
 namespace wf {
@@ -26,172 +27,19 @@ namespace {
 
 constexpr double kSigmaSB = 5.670374419e-8;
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b)
-{
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+// Resident blocks per SM the FFT kernels are compiled for.  Two blocks (128
+// registers, a few spilled) measured faster than one block with every value of
+// a radix-16 butterfly and its twiddles in registers.
+#ifndef WF_FFT_MIN_BLOCKS
+#define WF_FFT_MIN_BLOCKS 2
+#endif
+constexpr int kFftMinBlocks = WF_FFT_MIN_BLOCKS;
 
-// Forward radix-4 DFT of (a0, a1, a2, a3) in natural output order.
-__device__ __forceinline__ void bfly4(double2 &a0, double2 &a1, double2 &a2, double2 &a3)
-{
-    const double2 s0 = cadd(a0, a2), d0 = csub(a0, a2);
-    const double2 s1 = cadd(a1, a3), d1 = csub(a1, a3);
-    const double2 md1 = make_double2(d1.y, -d1.x);   // -i * d1
-    a0 = cadd(s0, s1);
-    a2 = csub(s0, s1);
-    a1 = cadd(d0, md1);
-    a3 = csub(d0, md1);
-}
-
-// Forward Stockham FFT of length M = 2^L (radix-4 stages, one radix-2 stage
-// when L is odd) on nl lines held in place in shared memory (data[l*M + j]).
-// Blocks have 256 threads; lines go in groups of 1024/M so that every thread
-// owns B4 radix-4 (or B2 radix-2) butterflies per stage, kept in registers
-// between the loads and the stores of the stage.  All index arithmetic is
-// shifts and masks.  tw[j] = exp(-2 pi i j / M).
-template <int L>
-__device__ void fft_pow2(double2 *data, int nl, const double2 *__restrict__ tw)
-{
-    constexpr int M = 1 << L;
-    constexpr int Q = M / 4;
-    constexpr int GL = (M >= 1024) ? 1 : 1024 / M;
-    constexpr int B4 = (M > 1024) ? M / 1024 : 1;
-    constexpr int B2 = (GL * M / 2 + 255) / 256;
-    for (int l0 = 0; l0 < nl; l0 += GL) {
-        const int ng = min(GL, nl - l0);
-        double2 *base = data + (size_t)l0 * M;
-#pragma unroll
-        for (int st = 0; st < L / 2; st++) {
-            const int lns = 2 * st;
-            double2 v[B4][4];
-            int jb[B4];
-            double2 *xl[B4];
-#pragma unroll
-            for (int b = 0; b < B4; b++) {
-                const int t = threadIdx.x + b * 256;
-                jb[b] = -1;
-                if (t < ng * Q) {
-                    jb[b] = t & (Q - 1);
-                    xl[b] = base + (size_t)(t / Q) * M;
-#pragma unroll
-                    for (int r = 0; r < 4; r++) v[b][r] = xl[b][jb[b] + r * Q];
-                }
-            }
-            __syncthreads();
-#pragma unroll
-            for (int b = 0; b < B4; b++) {
-                if (jb[b] < 0) continue;
-                const int j = jb[b], k = j & ((1 << lns) - 1);
-                if (st > 0) {
-                    const int tsh = L - 2 - lns;
-                    v[b][1] = cmul(v[b][1], __ldg(tw + ((1 * k) << tsh)));
-                    v[b][2] = cmul(v[b][2], __ldg(tw + ((2 * k) << tsh)));
-                    v[b][3] = cmul(v[b][3], __ldg(tw + ((3 * k) << tsh)));
-                }
-                bfly4(v[b][0], v[b][1], v[b][2], v[b][3]);
-                const int o = ((j >> lns) << (lns + 2)) + k;
-#pragma unroll
-                for (int r = 0; r < 4; r++) xl[b][o + (r << lns)] = v[b][r];
-            }
-            __syncthreads();
-        }
-        if (L & 1) {
-            // final radix-2 stage: Ns = M/2, twiddle exp(-2 pi i j / M)
-            double2 v[B2][2];
-            int jb[B2];
-            double2 *xl[B2];
-#pragma unroll
-            for (int b = 0; b < B2; b++) {
-                const int t = threadIdx.x + b * 256;
-                jb[b] = -1;
-                if (t < ng * (M / 2)) {
-                    jb[b] = t & (M / 2 - 1);
-                    xl[b] = base + (size_t)(t / (M / 2)) * M;
-                    v[b][0] = xl[b][jb[b]];
-                    v[b][1] = xl[b][jb[b] + M / 2];
-                }
-            }
-            __syncthreads();
-#pragma unroll
-            for (int b = 0; b < B2; b++) {
-                if (jb[b] < 0) continue;
-                const double2 w = cmul(v[b][1], __ldg(tw + jb[b]));
-                xl[b][jb[b]] = cadd(v[b][0], w);
-                xl[b][jb[b] + M / 2] = csub(v[b][0], w);
-            }
-            __syncthreads();
-        }
-    }
-}
-
-// Length-n DFT of nl lines held in place in A ([nl][m], first n entries valid;
-// m = 2^L).  inverse selects exp(+2 pi i ...), unnormalised.  Lengths that are
-// not powers of two go through Bluestein's chirp-z identity
-//   X_k = c_k * IFFT_m( FFT_m(x c) * FFT_m(b) )_k,  c_j = exp(-i pi j^2 / n).
-template <int L>
-__device__ void fft_line_set(const FftDesc &d, double2 *A, int nl, bool inverse)
-{
-    constexpr int M = 1 << L;
-    const int n = d.n;
-    if (!d.bluestein) {
-        if (inverse) {
-            for (int t = threadIdx.x; t < nl * M; t += blockDim.x) A[t].y = -A[t].y;
-            __syncthreads();
-        }
-        fft_pow2<L>(A, nl, d.tw);
-        if (inverse) {
-            for (int t = threadIdx.x; t < nl * M; t += blockDim.x) A[t].y = -A[t].y;
-            __syncthreads();
-        }
-        return;
-    }
-    for (int t = threadIdx.x; t < nl * M; t += blockDim.x) {
-        const int j = t & (M - 1);
-        double2 v = A[t];
-        if (inverse) v.y = -v.y;
-        A[t] = (j < n) ? cmul(v, __ldg(d.chirp + j)) : make_double2(0.0, 0.0);
-    }
-    __syncthreads();
-    fft_pow2<L>(A, nl, d.tw);
-    for (int t = threadIdx.x; t < nl * M; t += blockDim.x)
-        A[t] = cconj(cmul(A[t], __ldg(d.filt + (t & (M - 1)))));   // conj: IFFT via FFT
-    __syncthreads();
-    fft_pow2<L>(A, nl, d.tw);
-    const double inv_m = 1.0 / (double)M;
-    for (int t = threadIdx.x; t < nl * M; t += blockDim.x) {
-        const int j = t & (M - 1);
-        if (j < n) {
-            double2 v = cconj(A[t]);
-            v.x *= inv_m;
-            v.y *= inv_m;
-            v = cmul(v, __ldg(d.chirp + j));
-            if (inverse) v.y = -v.y;
-            A[t] = v;
-        }
-    }
-    __syncthreads();
-}
-
-__device__ void fft_lines(const FftDesc &d, double2 *A, int nl, bool inverse)
-{
-    switch (d.L) {
-    case 2: fft_line_set<2>(d, A, nl, inverse); break;
-    case 3: fft_line_set<3>(d, A, nl, inverse); break;
-    case 4: fft_line_set<4>(d, A, nl, inverse); break;
-    case 5: fft_line_set<5>(d, A, nl, inverse); break;
-    case 6: fft_line_set<6>(d, A, nl, inverse); break;
-    case 7: fft_line_set<7>(d, A, nl, inverse); break;
-    case 8: fft_line_set<8>(d, A, nl, inverse); break;
-    case 9: fft_line_set<9>(d, A, nl, inverse); break;
-    case 10: fft_line_set<10>(d, A, nl, inverse); break;
-    case 11: fft_line_set<11>(d, A, nl, inverse); break;
-    case 12: fft_line_set<12>(d, A, nl, inverse); break;
-    default: break;
-    }
-}
+using fft::cadd;
+using fft::cconj;
+using fft::cmul;
+using fft::csub;
+using fft::pad;
 
 // Poisson source at (i, j, k), k < Nz-1 (pressure.cu:37-95 and 150-321).
 template <class R>
@@ -288,38 +136,90 @@ __device__ double poisson_source(const PoissonArgs<R> &a, int i, int j, int k)
     return rho * (ux + vy + wz - divT) / ph.dt + (rhox * px + rhoy * py + rhoz * pz) / rho;
 }
 
-// P1: source + top plane, forward FFT in y of packed slice pairs.
-template <class R>
-__global__ void __launch_bounds__(256) k_p_rhs_ffty(const PoissonArgs<R> a, int KP)
+// Length-n DFT of the line (buf, jj): one power-of-two FFT when n = M, else
+// Bluestein's chirp-z identity with two length-M FFTs,
+//   X_k = c_k * IFFT_M( FFT_M(x c) * FFT_M(b) )_k,  c_j = exp(-i pi j^2 / n),
+// the inverse FFT taken as conj(FFT(conj(.))).  pre(idx) supplies x[idx] for
+// idx < n and post(idx, X) receives X[idx] for idx < n.  INV selects
+// exp(+2 pi i jk/n), unnormalised.  pre may read buf and post may write it.
+template <int L, bool INV, class Pre, class Post>
+__device__ __forceinline__ void line_dft(const FftDesc &d, double2 *buf, int jj, Pre pre, Post post)
 {
+    if (!d.bluestein) {
+        fft::run<L>(
+            buf, jj, d.tw,
+            [&](int idx) {
+                const double2 v = pre(idx);
+                return INV ? cconj(v) : v;
+            },
+            [&](int idx, double2 v) { post(idx, INV ? cconj(v) : v); });
+        return;
+    }
+    const int n = d.n;
+    const double2 *__restrict__ chirp = d.chirp;
+    const double2 *__restrict__ filt = d.filt;
+    fft::run<L>(
+        buf, jj, d.tw,
+        [&](int idx) {
+            double2 v = make_double2(0.0, 0.0);
+            if (idx < n) {
+                v = pre(idx);
+                if (INV) v = cconj(v);
+                v = cmul(v, __ldg(chirp + idx));
+            }
+            return v;
+        },
+        [&](int idx, double2 v) { buf[pad(idx)] = cconj(cmul(v, __ldg(filt + idx))); });
+    __syncthreads();
+    constexpr double inv_m = 1.0 / (double)(1 << L);
+    fft::run<L>(
+        buf, jj, d.tw, [&](int idx) { return buf[pad(idx)]; },
+        [&](int idx, double2 v) {
+            if (idx < n) {
+                v = cmul(make_double2(v.x * inv_m, -v.y * inv_m), __ldg(chirp + idx));
+                post(idx, INV ? cconj(v) : v);
+            }
+        });
+}
+
+// P1: source + top plane, forward FFT in y of packed slice pairs.  Block
+// (i, pair group): LB complex lines, line q packs slices 2(pair0+q) (real
+// part) and 2(pair0+q)+1 (imaginary part); slice nk is the top-plane pressure.
+template <int L, class R>
+__global__ void __launch_bounds__(256, kFftMinBlocks) k_p_rhs_ffty(const PoissonArgs<R> a)
+{
+    using SH = fft::Shape<L>;
+    constexpr int LB = SH::LB, LS = SH::LS;
     extern __shared__ double2 smem[];
     const Geom &g = a.g;
     const int n0 = g.Nx - 1, n1 = g.Ny - 1, nk = g.Nz - 1, h1 = a.h1;
-    const int m1 = a.fy.m;
     const int i = blockIdx.x;
-    const int pair0 = blockIdx.y * KP;
+    const int pair0 = blockIdx.y * LB;
     const int nslices = nk + 1;                      // f slices + top-plane pressure
-    const int np = (nslices + 1) / 2;
-    const int kp = min(KP, np - pair0);
-    double2 *A = smem;
-    double *Ad = reinterpret_cast<double *>(A);
-    const int ns = 2 * kp;
-    for (int t = threadIdx.x; t < n1 * ns; t += blockDim.x) {
-        const int jj = t / ns, q = t - jj * ns;
+    double *Ad = reinterpret_cast<double *>(smem);
+    for (int t = threadIdx.x; t < n1 * 2 * LB; t += 256) {
+        const int jj = t / (2 * LB), q = t - jj * (2 * LB);
         const int kk = 2 * pair0 + q;
         double val = 0.0;
         if (kk < nk) val = poisson_source(a, i, jj, kk);
         else if (kk == nk) val = a.p[((size_t)i * g.Ny + jj) * g.Nz + (g.Nz - 1)];
-        Ad[2 * ((size_t)(q >> 1) * m1 + jj) + (q & 1)] = val;
+        Ad[2 * ((q >> 1) * LS + pad(jj)) + (q & 1)] = val;
     }
     __syncthreads();
-    fft_lines(a.fy, A, kp, false);
-    const double2 *Rb = A;
-    // split the packed transform into the two half spectra
-    for (int t = threadIdx.x; t < kp * h1; t += blockDim.x) {
+    {
+        const int q = threadIdx.x % LB, jj = threadIdx.x / LB;
+        double2 *buf = smem + q * LS;
+        line_dft<L, false>(
+            a.fy, buf, jj, [&](int idx) { return buf[pad(idx)]; }, [&](int idx, double2 v) { buf[pad(idx)] = v; });
+    }
+    __syncthreads();
+    // split each packed transform into the two half spectra
+    const int kp = min(LB, (nslices + 1) / 2 - pair0);
+    for (int t = threadIdx.x; t < kp * h1; t += 256) {
         const int line = t / h1, s = t - line * h1;
-        const double2 Zs = Rb[(size_t)line * m1 + s];
-        const double2 Zc = cconj(Rb[(size_t)line * m1 + (s == 0 ? 0 : n1 - s)]);
+        const double2 *Rb = smem + line * LS;
+        const double2 Zs = Rb[pad(s)];
+        const double2 Zc = cconj(Rb[pad(s == 0 ? 0 : n1 - s)]);
         const double2 Fa = make_double2(0.5 * (Zs.x + Zc.x), 0.5 * (Zs.y + Zc.y));
         const double2 Fb = make_double2(0.5 * (Zs.y - Zc.y), -0.5 * (Zs.x - Zc.x));
         const int kk0 = 2 * (pair0 + line);
@@ -328,37 +228,34 @@ __global__ void __launch_bounds__(256) k_p_rhs_ffty(const PoissonArgs<R> a, int 
     }
 }
 
-// P2/P4: FFT along x of slices [0, nslices), SC consecutive s per block.
-template <bool INV>
-__global__ void __launch_bounds__(256) k_p_fftx(double2 *__restrict__ G, FftDesc fx, int n0, int h1, int SC)
+// P2/P4: FFT along x of one slice kk, LB consecutive s per block; the lines
+// are read from and written back to G inside the first and last FFT stages.
+template <int L, bool INV>
+__global__ void __launch_bounds__(256, kFftMinBlocks) k_p_fftx(double2 *__restrict__ G, const FftDesc fx, int n0, int h1)
 {
+    using SH = fft::Shape<L>;
     extern __shared__ double2 smem[];
-    const int m0 = fx.m;
-    const int kk = blockIdx.x;
-    const int s0 = blockIdx.y * SC;
-    const int sc = min(SC, h1 - s0);
-    double2 *A = smem;
-    double2 *Gs = G + (size_t)kk * n0 * h1;
-    for (int t = threadIdx.x; t < n0 * sc; t += blockDim.x) {
-        const int r = t / sc, q = t - r * sc;
-        A[(size_t)q * m0 + r] = Gs[(size_t)r * h1 + s0 + q];
-    }
-    __syncthreads();
-    fft_lines(fx, A, sc, INV);
-    const double2 *Rb = A;
-    for (int t = threadIdx.x; t < n0 * sc; t += blockDim.x) {
-        const int r = t / sc, q = t - r * sc;
-        Gs[(size_t)r * h1 + s0 + q] = Rb[(size_t)q * m0 + r];
-    }
+    const int q = threadIdx.x % SH::LB, jj = threadIdx.x / SH::LB;
+    const int s = blockIdx.y * SH::LB + q;
+    const bool act = s < h1;
+    double2 *buf = smem + q * SH::LS;
+    double2 *g = G + (size_t)blockIdx.x * n0 * h1 + (act ? s : 0);
+    line_dft<L, INV>(
+        fx, buf, jj, [&](int idx) { return act ? g[(size_t)idx * h1] : make_double2(0.0, 0.0); },
+        [&](int idx, double2 v) {
+            if (act) g[(size_t)idx * h1] = v;
+        });
 }
 
 // P3: tridiagonal solve in z per (r, s) (pressure.cu:356-390, 473-504, 418-443).
 // zt holds per-k constants: [0..nk) a, [nk..2nk) c, [2nk..3nk) D (b = -(kk + D)),
-// followed by b0, c0base, inv_dz1, half_dz0, cl.
+// followed by b0, c0base, inv_dz1, half_dz0, cl.  The right-hand sides are
+// fetched eight planes ahead of the recurrence so the loads overlap.
 __global__ void __launch_bounds__(128) k_p_tridiag(double2 *__restrict__ G, const double *__restrict__ kx2,
                                                    const double *__restrict__ ky2, const double *__restrict__ zt,
                                                    int n0, int h1, int nk)
 {
+    constexpr int CH = 8;
     const int r = blockIdx.x;
     const int s = blockIdx.y * blockDim.x + threadIdx.x;
     if (s >= h1) return;
@@ -371,80 +268,106 @@ __global__ void __launch_bounds__(128) k_p_tridiag(double2 *__restrict__ G, cons
     double uk[256];
     // row 0 uses the source of slice 1; rows 1..nk-2 their own; the last row
     // subtracts the top pressure divided by its coupling coefficient
-    double2 d0 = g[stride * 1];
+    const double2 pt = g[stride * nk];
+    const double2 d0 = g[stride * 1];
     double2 y = make_double2(half_dz0 * d0.x, half_dz0 * d0.y);
     double u = b0;
     uk[0] = u;
     double cprev = c0base - half_dz0 * kk2 - inv_dz1;   // c[0]
     g[0] = y;
-    for (int k = 1; k < nk; k++) {
-        const double l = za[k - 1] / u;
-        const double bk = -(kk2 + zD[k]);
-        u = bk - l * cprev;
-        uk[k & 255] = u;
-        double2 dk = g[stride * k];
-        if (k == nk - 1) {
-            const double2 pt = g[stride * nk];
-            dk = make_double2(dk.x - pt.x / cl, dk.y - pt.y / cl);
+    for (int k0 = 1; k0 < nk; k0 += CH) {
+        double2 dv[CH];
+#pragma unroll
+        for (int q = 0; q < CH; q++)
+            if (k0 + q < nk) dv[q] = g[stride * (k0 + q)];
+#pragma unroll
+        for (int q = 0; q < CH; q++) {
+            const int k = k0 + q;
+            if (k < nk) {
+                const double l = za[k - 1] / u;
+                const double bk = -(kk2 + zD[k]);
+                u = bk - l * cprev;
+                uk[k & 255] = u;
+                double2 dk = dv[q];
+                if (k == nk - 1) dk = make_double2(dk.x - pt.x / cl, dk.y - pt.y / cl);
+                y = make_double2(dk.x - l * y.x, dk.y - l * y.y);
+                g[stride * k] = y;
+                cprev = zcc[k];
+            }
         }
-        y = make_double2(dk.x - l * y.x, dk.y - l * y.y);
-        g[stride * k] = y;
-        cprev = zcc[k];
     }
     double2 x = make_double2(y.x / u, y.y / u);
     g[stride * (nk - 1)] = x;
-    for (int k = nk - 2; k >= 0; k--) {
-        const double ck = (k == 0) ? (c0base - half_dz0 * kk2 - inv_dz1) : zcc[k];
-        const double2 yk = g[stride * k];
-        const double uu = uk[k & 255];
-        x = make_double2((yk.x - ck * x.x) / uu, (yk.y - ck * x.y) / uu);
-        g[stride * k] = x;
+    for (int k0 = nk - 2; k0 >= 0; k0 -= CH) {
+        double2 yv[CH];
+#pragma unroll
+        for (int q = 0; q < CH; q++)
+            if (k0 - q >= 0) yv[q] = g[stride * (k0 - q)];
+#pragma unroll
+        for (int q = 0; q < CH; q++) {
+            const int k = k0 - q;
+            if (k >= 0) {
+                const double ck = (k == 0) ? (c0base - half_dz0 * kk2 - inv_dz1) : zcc[k];
+                const double uu = uk[k & 255];
+                x = make_double2((yv[q].x - ck * x.x) / uu, (yv[q].y - ck * x.y) / uu);
+                g[stride * k] = x;
+            }
+        }
     }
 }
 
 // P5: inverse FFT in y of packed slice pairs, normalisation, write p and the
 // periodic duplicate planes (pressure.cu:392-416, deterministic here).
-template <class R>
-__global__ void __launch_bounds__(256) k_p_iffty_out(const PoissonArgs<R> a, int KP)
+template <int L, class R>
+__global__ void __launch_bounds__(256, kFftMinBlocks) k_p_iffty_out(const PoissonArgs<R> a)
 {
+    using SH = fft::Shape<L>;
+    constexpr int LB = SH::LB, LS = SH::LS;
     extern __shared__ double2 smem[];
     const Geom &g = a.g;
     const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz;
     const int n0 = Nx - 1, n1 = Ny - 1, nk = Nz - 1, h1 = a.h1;
-    const int m1 = a.fy.m;
     const int i = blockIdx.x;
-    const int pair0 = blockIdx.y * KP;
+    const int pair0 = blockIdx.y * LB;
     const int np = (nk + 1) / 2;
-    const int kp = min(KP, np - pair0);
-    double2 *A = smem;
+    const int kp = min(LB, np - pair0);
     const bool even = (n1 % 2) == 0;
-    for (int t = threadIdx.x; t < kp * n1; t += blockDim.x) {
+    for (int t = threadIdx.x; t < LB * n1; t += 256) {
         const int line = t / n1, s = t - line * n1;
-        const int kk0 = 2 * (pair0 + line), kk1 = kk0 + 1;
-        const int ss = (s < h1) ? s : n1 - s;
-        double2 Fa = a.G[((size_t)kk0 * n0 + i) * h1 + ss];
-        double2 Fb = (kk1 < nk) ? a.G[((size_t)kk1 * n0 + i) * h1 + ss] : make_double2(0.0, 0.0);
-        if (ss == 0 || (even && ss == n1 / 2)) {
-            Fa.y = 0.0;
-            Fb.y = 0.0;
+        double2 val = make_double2(0.0, 0.0);
+        if (line < kp) {
+            const int kk0 = 2 * (pair0 + line), kk1 = kk0 + 1;
+            const int ss = (s < h1) ? s : n1 - s;
+            double2 Fa = a.G[((size_t)kk0 * n0 + i) * h1 + ss];
+            double2 Fb = (kk1 < nk) ? a.G[((size_t)kk1 * n0 + i) * h1 + ss] : make_double2(0.0, 0.0);
+            if (ss == 0 || (even && ss == n1 / 2)) {
+                Fa.y = 0.0;
+                Fb.y = 0.0;
+            }
+            if (s >= h1) {
+                Fa.y = -Fa.y;
+                Fb.y = -Fb.y;
+            }
+            val = make_double2(Fa.x - Fb.y, Fa.y + Fb.x);
         }
-        if (s >= h1) {
-            Fa.y = -Fa.y;
-            Fb.y = -Fb.y;
-        }
-        A[(size_t)line * m1 + s] = make_double2(Fa.x - Fb.y, Fa.y + Fb.x);
+        smem[line * LS + pad(s)] = val;
     }
     __syncthreads();
-    fft_lines(a.fy, A, kp, true);
-    const double2 *Rb = A;
+    {
+        const int q = threadIdx.x % LB, jj = threadIdx.x / LB;
+        double2 *buf = smem + q * LS;
+        line_dft<L, true>(
+            a.fy, buf, jj, [&](int idx) { return buf[pad(idx)]; }, [&](int idx, double2 v) { buf[pad(idx)] = v; });
+    }
+    __syncthreads();
     const double norm = (double)n0 * (double)n1;
     const int ns = 2 * kp;
     double *p = a.p;
-    for (int t = threadIdx.x; t < n1 * ns; t += blockDim.x) {
+    for (int t = threadIdx.x; t < n1 * ns; t += 256) {
         const int jj = t / ns, q = t - jj * ns;
         const int kk = 2 * pair0 + q;
         if (kk >= nk) continue;
-        const double2 zv = Rb[(size_t)(q >> 1) * m1 + jj];
+        const double2 zv = smem[(q >> 1) * LS + pad(jj)];
         const double val = ((q & 1) ? zv.y : zv.x) / norm;
         p[((size_t)i * Ny + jj) * Nz + kk] = val;
         if (jj == 0) p[((size_t)i * Ny + (Ny - 1)) * Nz + kk] = val;
@@ -463,47 +386,95 @@ __global__ void __launch_bounds__(256) k_p_iffty_out(const PoissonArgs<R> a, int
     }
 }
 
+// ---- launch: one kernel instantiation per inner FFT length ----------------
+constexpr int kMinL = 2, kMaxL = 12;
+
+template <class Op, class... A>
+cudaError_t by_length(int L, A &...args)
+{
+    switch (L) {
+    case 2: return Op::template go<2>(args...);
+    case 3: return Op::template go<3>(args...);
+    case 4: return Op::template go<4>(args...);
+    case 5: return Op::template go<5>(args...);
+    case 6: return Op::template go<6>(args...);
+    case 7: return Op::template go<7>(args...);
+    case 8: return Op::template go<8>(args...);
+    case 9: return Op::template go<9>(args...);
+    case 10: return Op::template go<10>(args...);
+    case 11: return Op::template go<11>(args...);
+    case 12: return Op::template go<12>(args...);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <class R>
+struct LaunchP1 {
+    template <int L> static cudaError_t go(const PoissonArgs<R> &a, cudaStream_t &s)
+    {
+        using SH = fft::Shape<L>;
+        const int np = (a.g.Nz - 1 + 2) / 2;
+        k_p_rhs_ffty<L, R><<<dim3(a.g.Nx - 1, (np + SH::LB - 1) / SH::LB), 256, SH::smem_bytes, s>>>(a);
+        return cudaSuccess;
+    }
+};
+template <class R>
+struct LaunchP5 {
+    template <int L> static cudaError_t go(const PoissonArgs<R> &a, cudaStream_t &s)
+    {
+        using SH = fft::Shape<L>;
+        const int np = (a.g.Nz - 1 + 1) / 2;
+        k_p_iffty_out<L, R><<<dim3(a.g.Nx - 1, (np + SH::LB - 1) / SH::LB), 256, SH::smem_bytes, s>>>(a);
+        return cudaSuccess;
+    }
+};
+template <bool INV>
+struct LaunchFx {
+    template <int L> static cudaError_t go(double2 *const &G, const FftDesc &fx, const int &nslices, const int &n0,
+                                           const int &h1, cudaStream_t &s)
+    {
+        using SH = fft::Shape<L>;
+        k_p_fftx<L, INV><<<dim3(nslices, (h1 + SH::LB - 1) / SH::LB), 256, SH::smem_bytes, s>>>(G, fx, n0, h1);
+        return cudaSuccess;
+    }
+};
+
+template <class R, int L>
+cudaError_t set_attributes_for()
+{
+    const int b = (int)fft::Shape<L>::smem_bytes;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_p_rhs_ffty<L, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_p_iffty_out<L, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_p_fftx<L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_p_fftx<L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    if constexpr (L < kMaxL) return set_attributes_for<R, L + 1>();
+    return cudaSuccess;
+}
+
 }  // namespace
 
-int poisson_pairs_per_block(int m) { return max(1, min(16, 6144 / m)); }
-int poisson_lines_per_block(int m) { return max(1, min(16, 6144 / m)); }
-
-template <class R> cudaError_t poisson_set_attributes()
-{
-    const int maxsm = 200 * 1024;
-    cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_p_rhs_ffty<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
-    if ((e = cudaFuncSetAttribute(k_p_iffty_out<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
-    if ((e = cudaFuncSetAttribute(k_p_fftx<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm))) return e;
-    return cudaFuncSetAttribute(k_p_fftx<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-}
+template <class R> cudaError_t poisson_set_attributes() { return set_attributes_for<R, kMinL>(); }
 template cudaError_t poisson_set_attributes<double>();
 template cudaError_t poisson_set_attributes<float>();
 
-// zt: tridiagonal constants (see k_p_tridiag); passed through the G pointer's
-// companion allocation by the caller.
 template <class R>
 cudaError_t launch_poisson_impl(const PoissonArgs<R> &a, const double *zt, cudaStream_t s, cudaEvent_t *ev)
 {
-    const int n0 = a.g.Nx - 1, nk = a.g.Nz - 1, h1 = a.h1;
-    const int KP = poisson_pairs_per_block(a.fy.m);
-    const int SC = poisson_lines_per_block(a.fx.m);
-    const int np1 = (nk + 1 + 1) / 2;
-    dim3 g1(n0, (np1 + KP - 1) / KP);
-    k_p_rhs_ffty<R><<<g1, 256, (size_t)KP * a.fy.m * sizeof(double2), s>>>(a, KP);
+    int n0 = a.g.Nx - 1, nk = a.g.Nz - 1, h1 = a.h1;
+    cudaError_t e;
+    if ((e = by_length<LaunchP1<R>>(a.fy.L, a, s))) return e;
     if (ev) cudaEventRecord(ev[0], s);
-    dim3 g2(nk + 1, (h1 + SC - 1) / SC);
-    k_p_fftx<false><<<g2, 256, (size_t)SC * a.fx.m * sizeof(double2), s>>>(a.G, a.fx, n0, h1, SC);
+    int ns = nk + 1;
+    double2 *G = a.G;
+    if ((e = by_length<LaunchFx<false>>(a.fx.L, G, a.fx, ns, n0, h1, s))) return e;
     if (ev) cudaEventRecord(ev[1], s);
-    dim3 g3(n0, (h1 + 127) / 128);
-    k_p_tridiag<<<g3, 128, 0, s>>>(a.G, a.kx2, a.ky2, zt, n0, h1, nk);
+    k_p_tridiag<<<dim3(n0, (h1 + 127) / 128), 128, 0, s>>>(a.G, a.kx2, a.ky2, zt, n0, h1, nk);
     if (ev) cudaEventRecord(ev[2], s);
-    dim3 g4(nk, (h1 + SC - 1) / SC);
-    k_p_fftx<true><<<g4, 256, (size_t)SC * a.fx.m * sizeof(double2), s>>>(a.G, a.fx, n0, h1, SC);
+    ns = nk;
+    if ((e = by_length<LaunchFx<true>>(a.fx.L, G, a.fx, ns, n0, h1, s))) return e;
     if (ev) cudaEventRecord(ev[3], s);
-    const int np5 = (nk + 1) / 2;
-    dim3 g5(n0, (np5 + KP - 1) / KP);
-    k_p_iffty_out<R><<<g5, 256, (size_t)KP * a.fy.m * sizeof(double2), s>>>(a, KP);
+    if ((e = by_length<LaunchP5<R>>(a.fy.L, a, s))) return e;
     if (ev) cudaEventRecord(ev[4], s);
     return cudaGetLastError();
 }

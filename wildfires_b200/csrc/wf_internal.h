@@ -158,8 +158,6 @@ struct PoissonArgs {
 template <class R>
 cudaError_t launch_poisson_impl(const PoissonArgs<R> &a, const double *zt, cudaStream_t s, cudaEvent_t *ev = nullptr);
 template <class R> cudaError_t poisson_set_attributes();
-int poisson_pairs_per_block(int m);
-int poisson_lines_per_block(int m);
 constexpr int kMaxFftLength = 2048;     // longest supported x or y transform
 constexpr int kMaxZUnknowns = 256;      // longest supported tridiagonal system (Nz-1)
 
