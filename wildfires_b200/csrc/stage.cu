@@ -36,8 +36,21 @@ __device__ __forceinline__ int wrap_p(int v, int n)
 template <class R> __device__ __forceinline__ R rmax(R a, R b) { return (a > b) ? a : b; }
 template <class R> __device__ __forceinline__ R rmin(R a, R b) { return (a < b) ? a : b; }
 
+// Square root, quotient and third.  The FP64 path keeps the reference's
+// correctly rounded operations; the FP32 stencil path uses the PTX
+// approximations (sqrt.approx.f32, div.approx.f32: about 1 ulp, no slow path),
+// well inside its 1e-5 error budget against FP64.
 __device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
-__device__ __forceinline__ float rsqrt_(float x) { return sqrtf(x); }
+__device__ __forceinline__ float rsqrt_(float x)
+{
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double third(double a) { return a / 3.0; }
+__device__ __forceinline__ float third(float a) { return a * (1.0f / 3.0f); }
 __device__ __forceinline__ double rexp(double x) { return exp(x); }
 __device__ __forceinline__ float rexp(float x) { return expf(x); }
 __device__ __forceinline__ double rpow(double x, double y) { return pow(x, y); }
@@ -66,7 +79,7 @@ __device__ __forceinline__ Thermo<R> thermo(const PhysR<R> &p, int suth_mu, int 
     Thermo<R> o;
     R mu = p.mu, kT = p.kT, dk = R(0);
     // Arrhenius rate A exp(-T_act/T) H(T - T_pc); exactly 0 below the phase change
-    o.K_T = (T > p.T_pc) ? p.A * rexp(-p.T_act / T) * R(1) : R(0);
+    o.K_T = (T > p.T_pc) ? p.A * rexp(-fdiv(p.T_act, T)) * R(1) : R(0);
     R Y = R(0), T_gas = p.T_inf, T_solid = p.T_inf;
     if (k <= nzy) {
         if (k < nzy) Y = Yc;
@@ -80,16 +93,16 @@ __device__ __forceinline__ Thermo<R> thermo(const PhysR<R> &p, int suth_mu, int 
         dk = R(0.0241) * (R(1.5) * rpow(T / R(273.15), R(0.5)) * (R(273.15) + R(194)) / (T + R(194)) -
                           rpow(T / R(273.15), R(1.5)) * (R(273.15) + R(194)) / ((T + R(194)) * (T + R(194))));
     }
-    o.nu = mu / rho;
+    o.nu = fdiv(mu, rho);
     o.mu = mu;
-    R q = p.H_C * Y * o.K_T / p.c_p;
+    R q = fdiv(p.H_C * Y * o.K_T, p.c_p);
     if (p.alpha_s * p.sigma_s != R(0)) {
         // h_c evaluated per cell (the reference compounds its copy per thread, pde.cu:698)
         const R h_c = p.h_c * dz_k * rpow(rfabs(T_gas - T_solid) / dz_k, R(0.25));
         q = q - h_c * p.alpha_s * p.sigma_s * (T_gas - T_solid) / (p.c_p * p.T_inf * p.rho_inf / T_gas);
     }
-    o.T_RHS_tmp = (dk + p.c12 * (T * T) * (Tx * Tx + Ty * Ty + Tz * Tz) + (kT + p.c4 * (T * T * T)) * lap_T) /
-                      (rho * p.c_p) + q;
+    o.T_RHS_tmp = fdiv(dk + p.c12 * (T * T) * (Tx * Tx + Ty * Ty + Tz * Tz) + (kT + p.c4 * (T * T * T)) * lap_T,
+                       rho * p.c_p) + q;
     o.Y = Y;
     return o;
 }
@@ -134,13 +147,13 @@ __global__ void __launch_bounds__(128) k_utau(const StageArgs<R> a)
     const R uz = w0 * X[0] + w1 * X[1] + w2 * X[2];
     const R vz = w0 * X[N] + w1 * X[N + 1] + w2 * X[N + 2];
     const R T = X[3 * (size_t)N];
-    const R rho = a.pr.Trho / T;
+    const R rho = fdiv(a.pr.Trho, T);
     R mu = a.pr.mu;
     if (a.ph.sutherland_viscosity == 1)
         mu = R(1.716e-5) * rpow(T / R(273.15), R(1.5)) * (R(273.15) + R(110.4)) / (T + R(110.4));
     const R a1 = mu * uz, a2 = mu * vz;
     const R tau_w = rsqrt_(a1 * a1 + a2 * a2);
-    a.utau[col] = rsqrt_(tau_w / rho);
+    a.utau[col] = rsqrt_(fdiv(tau_w, rho));
 }
 
 // Shared-memory tile of one stage: TI x TJ x KZ cells, state halo 2 (4 fields)
@@ -323,10 +336,10 @@ __global__ void __launch_bounds__(256, MINB) k_stage_fused(const StageArgs<R> a)
                       : (R)zc[ZBB0 * Nz + gk] * m3 + (R)zc[ZBB1 * Nz + gk] * pT[kk - 2] +
                             (R)zc[ZBB2 * Nz + gk] * pT[kk - 1] + (R)zc[ZBB3 * Nz + gk] * Tc;
         }
-        const R rho = p.Trho / Tc;
-        const R S11 = R(2) * ux / R(3) - (vy + wz) / R(3);
-        const R S22 = R(2) * vy / R(3) - (ux + wz) / R(3);
-        const R S33 = R(2) * wz / R(3) - (ux + vy) / R(3);
+        const R rho = fdiv(p.Trho, Tc);
+        const R S11 = third(R(2) * ux) - third(vy + wz);
+        const R S22 = third(R(2) * vy) - third(ux + wz);
+        const R S33 = third(R(2) * wz) - third(ux + vy);
         const R mod_S = rsqrt_(R(2) * (ux * ux + vy * vy + wz * wz) + (uz + wx) * (uz + wx) + (vx + uy) * (vx + uy) +
                                (wy + vz) * (wy + vz));
         const int nzy = t.cnzy[TL::cq(ii, jj)];
@@ -339,7 +352,7 @@ __global__ void __launch_bounds__(256, MINB) k_stage_fused(const StageArgs<R> a)
         t.G(4, ii, jj, kk) = S22;
         t.G(5, ii, jj, kk) = R(0.5) * (wy + vz);
         t.G(6, ii, jj, kk) = S33;
-        t.G(7, ii, jj, kk) = th.nu * th.T_RHS_tmp / Tc;
+        t.G(7, ii, jj, kk) = fdiv(th.nu * th.T_RHS_tmp, Tc);
     }
     __syncthreads();
 
@@ -403,7 +416,7 @@ __global__ void __launch_bounds__(256, MINB) k_stage_fused(const StageArgs<R> a)
             };
             R advT, Txx, Tyy, Tzz, Tx, Ty, Tz;
             adv_lap(3, T, advT, Txx, Tyy, Tzz, Tx, Ty, Tz);
-            const R rho = p.Trho / T;
+            const R rho = fdiv(p.Trho, T);
             const Thermo<R> th = thermo(p, smu, sk, T, t.S(3, ii, jj, kk + 1), t.gy[TL::q(ii, jj, kk)], gk, nzy, Tx,
                                         Ty, Tz, Txx + Tyy + Tzz, t.K(kk, RDZ), rho);
             kY = -p.Y_f * th.K_T * th.Y;
@@ -418,12 +431,12 @@ __global__ void __launch_bounds__(256, MINB) k_stage_fused(const StageArgs<R> a)
                 adv_lap(1, v, adv, fxx, fyy, fzz, fx, fy, fz);
                 kval[1] = th.nu * (fxx + fyy + fzz) - adv + (-p.cd * th.Y * mod_U * v);
                 adv_lap(2, w, adv, fxx, fyy, fzz, fx, fy, fz);
-                kval[2] = th.nu * (fxx + fyy + fzz) - adv + (p.g * (rho - p.rho_inf) / rho - p.cd * th.Y * mod_U * w);
+                kval[2] = th.nu * (fxx + fyy + fzz) - adv + (fdiv(p.g * (rho - p.rho_inf), rho) - p.cd * th.Y * mod_U * w);
             }
             // ---- SGS divergence with Van Driest damping (turbulence.cu:255-454)
             {
-                const R nu = p.mu / rho;
-                const R inv_avd_nu = p.inv_avd / nu;
+                const R nu = fdiv(p.mu, rho);
+                const R inv_avd_nu = fdiv(p.inv_avd, nu);
                 const R zk = t.K(kk, RZ);
                 auto zibm = [&](int q, R zz) -> R {
                     const R d = zz - t.ctopo[q];
@@ -462,14 +475,14 @@ __global__ void __launch_bounds__(256, MINB) k_stage_fused(const StageArgs<R> a)
                 const R div_S_x = S11_x + S21_y + S31_z;
                 const R div_S_y = S12_x + S22_y + S32_z;
                 const R div_S_z = S13_x + S23_y + S33_z;
-                const R inv_rho = R(1) / rho;
+                const R inv_rho = fdiv(R(1), rho);
                 const R sgs_x = R(-2) * (mu_x * S11 + mu_y * S12 + mu_z * S13 + mu_c * div_S_x) * inv_rho;
                 const R sgs_y = R(-2) * (mu_x * S12 + mu_y * S22 + mu_z * S23 + mu_c * div_S_y) * inv_rho;
                 const R sgs_z = R(-2) * (mu_x * S13 + mu_y * S23 + mu_z * S33 + mu_c * div_S_z) * inv_rho;
-                const R sgs_q = -(mu_x * Tx + mu_y * Ty + mu_z * Tz + mu_c * (Txx + Tyy + Tzz)) / (rho * p.Pr);
-                kval[0] += -sgs_x + dU_x / R(3);
-                kval[1] += -sgs_y + dU_y / R(3);
-                kval[2] += -sgs_z + dU_z / R(3);
+                const R sgs_q = -fdiv(mu_x * Tx + mu_y * Ty + mu_z * Tz + mu_c * (Txx + Tyy + Tzz), rho * p.Pr);
+                kval[0] += -sgs_x + third(dU_x);
+                kval[1] += -sgs_y + third(dU_y);
+                kval[2] += -sgs_z + third(dU_z);
                 kval[3] -= sgs_q;
             }
             // values the column boundary pass needs
@@ -487,7 +500,7 @@ __global__ void __launch_bounds__(256, MINB) k_stage_fused(const StageArgs<R> a)
         } else if (gk < nzy) {
             // fuel cell whose velocity and temperature the boundary rules set (top plane)
             const R T = t.S(3, ii, jj, kk);
-            const R K_T = (T > p.T_pc) ? p.A * rexp(-p.T_act / T) * R(1) : R(0);
+            const R K_T = (T > p.T_pc) ? p.A * rexp(-fdiv(p.T_act, T)) * R(1) : R(0);
             kY = -p.Y_f * K_T * t.gy[TL::q(ii, jj, kk)];
         }
         if (ylive) {
@@ -501,11 +514,17 @@ __global__ void __launch_bounds__(256, MINB) k_stage_fused(const StageArgs<R> a)
 // ---------------------------------------------------------------------------
 // boundary/IBM k-values per column (pde.cu:14-99) and their RK update
 template <class R>
-__global__ void __launch_bounds__(128) k_stage_bc(const StageArgs<R> a)
+__global__ void __launch_bounds__(256) k_stage_bc(const StageArgs<R> a)
 {
+    // kBcLanes lanes per column; the column's boundary values -- 4 fields (and
+    // Y where stored) on each dead node k < kc, 5 on the cut node, 4 on the
+    // top -- are enumerated field-major so consecutive lanes touch
+    // consecutive k of one field.
+    constexpr int kBcLanes = 16;
     const Geom &g = a.g;
     const Phys &ph = a.ph;
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    const int col = (blockIdx.x * blockDim.x + threadIdx.x) / kBcLanes;
+    const int lane = threadIdx.x % kBcLanes;
     if (col >= g.Nx * g.Ny) return;
     const int Nz = g.Nz, N = g.N;
     const int kc = __ldg(g.cut + col), nzy = __ldg(g.nzy + col);
@@ -513,39 +532,57 @@ __global__ void __launch_bounds__(128) k_stage_bc(const StageArgs<R> a)
     const double *z = g.z;
     const R an = (R)a.a_next;
     const bool rd = stage_reads_acc(a.method, a.stage), kp = stage_keeps_acc(a.method, a.stage);
-    auto upd = [&](size_t o, R kv) {
+    const size_t cb = (size_t)col * Nz;
+    const size_t cy = 4 * (size_t)N + (size_t)col * g.NzY;
+    const int n_dead = 4 * kc + min(kc, nzy);
+    const int n_items = n_dead + 5 + 4;
+    for (int u = lane; u < n_items; u += kBcLanes) {
+        size_t o;
+        R kv;
+        if (u < n_dead) {
+            // dead nodes below the terrain
+            int f, k;
+            if (u < 4 * kc) {
+                f = u / kc;
+                k = u - f * kc;
+            } else {
+                f = 4;
+                k = u - 4 * kc;
+            }
+            o = (f < 4) ? (size_t)f * N + cb + k : cy + k;
+            const double dv = (f == 0) ? ph.u_dead : (f == 1) ? ph.v_dead : (f == 2) ? ph.w_dead
+                            : (f == 3) ? ph.T_dead : ph.Y_dead;
+            kv = (R)dv;
+        } else if (u < n_dead + 5) {
+            // cut node: no-slip velocity, second-order extrapolated T and Y
+            const int f = u - n_dead;
+            if (f == 4 && kc >= nzy) continue;
+            o = (f < 4) ? (size_t)f * N + cb + kc : cy + kc;
+            kv = R(0);
+            if (f >= 3) {
+                const R A = (R)(z[kc + 1] - z[kc]), B = (R)(z[kc + 2] - z[kc + 1]);
+                R v1, v2;
+                if (f == 3) {
+                    v1 = bc[0];
+                    v2 = bc[1];
+                } else {
+                    v1 = (kc + 1 < nzy) ? bc[2] : R(0);
+                    v2 = (kc + 2 < nzy) ? bc[3] : R(0);
+                }
+                kv = fdiv((A + B) * (A + B) * v1 - A * A * v2, B * (R(2) * A + B));
+            }
+        } else {
+            // top: second-order extrapolation from k = Nz-2, Nz-3
+            const int f = u - n_dead - 5;
+            const int k = Nz - 1;
+            const R a1 = (R)(z[k] - z[k - 1]), a2 = (R)(z[k - 1] - z[k - 2]);
+            const R num = (a2 + a1) * (a2 + a1), den = a2 * (a2 + R(2) * a1), a1s = a1 * a1;
+            o = (size_t)f * N + cb + k;
+            kv = fdiv(num * bc[4 + f] - a1s * bc[8 + f], den);
+        }
         R accv = rd ? a.acc[o] : R(0);
         a.Xout[o] = rk_update(a.method, a.stage, kv, a.yn[o], accv, an);
         if (kp) a.acc[o] = accv;
-    };
-    const size_t cb = (size_t)col * Nz;
-    // cut node
-    {
-        const R A = (R)(z[kc + 1] - z[kc]), B = (R)(z[kc + 2] - z[kc + 1]);
-        const R T1 = bc[0], T2 = bc[1];
-        const R Y1 = (kc + 1 < nzy) ? bc[2] : R(0), Y2 = (kc + 2 < nzy) ? bc[3] : R(0);
-        upd(cb + kc, R(0));
-        upd((size_t)N + cb + kc, R(0));
-        upd(2 * (size_t)N + cb + kc, R(0));
-        upd(3 * (size_t)N + cb + kc, ((A + B) * (A + B) * T1 - A * A * T2) / (B * (R(2) * A + B)));
-        if (kc < nzy)
-            upd(4 * (size_t)N + (size_t)col * g.NzY + kc, ((A + B) * (A + B) * Y1 - A * A * Y2) / (B * (R(2) * A + B)));
-    }
-    // top
-    {
-        const int k = Nz - 1;
-        const R a1 = (R)(z[k] - z[k - 1]), a2 = (R)(z[k - 1] - z[k - 2]);
-        const R num = (a2 + a1) * (a2 + a1), den = a2 * (a2 + R(2) * a1), a1s = a1 * a1;
-#pragma unroll
-        for (int f = 0; f < 4; f++) upd((size_t)f * N + cb + k, (num * bc[4 + f] - a1s * bc[8 + f]) / den);
-    }
-    // dead nodes below the terrain
-    for (int k = 0; k < kc; k++) {
-        upd(cb + k, (R)ph.u_dead);
-        upd((size_t)N + cb + k, (R)ph.v_dead);
-        upd(2 * (size_t)N + cb + k, (R)ph.w_dead);
-        upd(3 * (size_t)N + cb + k, (R)ph.T_dead);
-        if (k < nzy) upd(4 * (size_t)N + (size_t)col * g.NzY + k, (R)ph.Y_dead);
     }
 }
 
@@ -587,7 +624,7 @@ template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t 
     dim3 grid((a.g.Nz + C::KZ - 1) / C::KZ, (a.g.Ny + C::TJ - 1) / C::TJ, (a.g.Nx + C::TI - 1) / C::TI);
     k_stage_fused<R, C::TI, C::TJ, C::KZ, C::MINB><<<grid, 256, stage_smem_bytes<R>(), s>>>(a);
     if (ev) cudaEventRecord(ev[1], s);
-    k_stage_bc<R><<<(ncol + 127) / 128, 128, 0, s>>>(a);
+    k_stage_bc<R><<<(ncol + 15) / 16, 256, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[2], s);
     return cudaGetLastError();
 }
