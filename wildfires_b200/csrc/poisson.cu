@@ -67,9 +67,9 @@ __device__ double poisson_source(const PoissonArgs<R> &a, int i, int j, int k)
             const double wzf = (k == 0) ? zc[ZF0 * Nz] * (double)W[c] + zc[ZF1 * Nz] * (double)W[c + 1] +
                                               zc[ZF2 * Nz] * (double)W[c + 2]
                                         : ((double)W[c + 1] - (double)W[c - 1]) * zc[ZC * Nz + k];
-            const double uxf = (0.5 * (u_ip1 + u) - 0.5 * (u + u_im1)) * (1.0 / ph.dx);
-            const double vyf = (0.5 * (v_jp1 + v) - 0.5 * (v + v_jm1)) * (1.0 / ph.dy);
-            return (uxf + vyf + wzf) * (ph.rho_inf / ph.dt);
+            const double uxf = (0.5 * (u_ip1 + u) - 0.5 * (u + u_im1)) * a.inv_dx;
+            const double vyf = (0.5 * (v_jp1 + v) - 0.5 * (v + v_jm1)) * a.inv_dy;
+            return (uxf + vyf + wzf) * a.rho_dt;
         }
     }
     double wz;

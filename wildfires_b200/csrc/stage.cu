@@ -157,31 +157,93 @@ __global__ void __launch_bounds__(128) k_utau(const StageArgs<R> a)
 }
 
 // Shared-memory tile of one stage: TI x TJ x KZ cells, state halo 2 (4 fields)
-// and SGS-input halo 1 (8 fields + fuel).  Offsets are relative to the tile
-// origin; (ii, jj, kk) in [-2, T+1] for the state and [-1, T] for the rest.
+// and SGS-input halo 1 (8 fields).  Offsets are relative to the tile origin;
+// (ii, jj, kk) in [-2, T+1] for the state and [-1, T] for the rest.  Both
+// arrays are stored j-fastest with a row stride of TJ+4: a warp covering
+// 8 consecutive k x 4 consecutive j then touches 32 distinct banks (FP32).
+// The fuel fraction is read from global memory where a column has fuel.
 template <class R, int TI, int TJ, int KZ> struct Tile {
     static constexpr int SI = TI + 4, SJ = TJ + 4, SK = KZ + 4, SR = SI * SJ * SK;
-    static constexpr int GI = TI + 2, GJ = TJ + 2, GK = KZ + 2, GR = GI * GJ * GK;
+    static constexpr int GI = TI + 2, GJ = TJ + 2, GK = KZ + 2, GJP = SJ, GR = GI * GK * GJP;
+    static constexpr int ZS = SJ;   // z stride of the state tile
     static constexpr int NCOL = GI * GJ, CELLS = TI * TJ * KZ;
-    static constexpr size_t bytes()
-    {
-        return sizeof(R) * (4 * (size_t)SR + 9 * (size_t)GR + 2 * (size_t)NCOL + (size_t)GK * KROW) +
-               sizeof(int) * 2 * (size_t)NCOL;
-    }
-    R *st;    // [4][SR]  u, v, w, T
-    R *gs;    // [8][GR]  mu_sgs, S11, S12, S13, S22, S23, S33, divU
-    R *gy;    // [GR]     fuel fraction (0 above the column's fuel top)
-    R *kr;    // [GK][KROW] z-stencil rows for k0-1 .. k0+KZ
-    R *ctopo; // [NCOL]   terrain height of the halo-1 columns
-    R *cut_;  // [NCOL]   wall friction velocity of the halo-1 columns
+    static constexpr size_t up16(size_t b) { return (b + 15) / 16 * 16; }
+    static constexpr size_t O_KR = up16(sizeof(R) * 4 * (size_t)SR);
+    static constexpr size_t O_TOPO = O_KR + up16(sizeof(R) * (size_t)GK * KROW);
+    static constexpr size_t O_UT = O_TOPO + up16(sizeof(double) * (size_t)NCOL);
+    static constexpr size_t O_NZY = O_UT + up16(sizeof(R) * (size_t)NCOL);
+    static constexpr size_t O_CUT = O_NZY + up16(sizeof(int) * (size_t)NCOL);
+    static constexpr size_t BUF = O_CUT + up16(sizeof(int) * (size_t)NCOL);
+    static constexpr size_t bytes() { return BUF + up16(sizeof(R) * 8 * (size_t)GR); }
+    R *st;         // [4][SR]  u, v, w, T
+    R *kr;         // [GK][KROW] z-stencil rows for k0-1 .. k0+KZ
+    double *ctopo; // [NCOL]   terrain height of the halo-1 columns
+    R *cut_;       // [NCOL]   wall friction velocity of the halo-1 columns
     int *cnzy, *ccut;
-    __device__ static int s(int ii, int jj, int kk) { return ((ii + 2) * SJ + (jj + 2)) * SK + (kk + 2); }
-    __device__ static int q(int ii, int jj, int kk) { return ((ii + 1) * GJ + (jj + 1)) * GK + (kk + 1); }
+    R *gs;         // [8][GR]  mu_sgs, S11, S12, S13, S22, S23, S33, divU (shared by both buffers)
+    __device__ void bind(unsigned char *buf, R *sgs)
+    {
+        st = reinterpret_cast<R *>(buf);
+        kr = reinterpret_cast<R *>(buf + O_KR);
+        ctopo = reinterpret_cast<double *>(buf + O_TOPO);
+        cut_ = reinterpret_cast<R *>(buf + O_UT);
+        cnzy = reinterpret_cast<int *>(buf + O_NZY);
+        ccut = reinterpret_cast<int *>(buf + O_CUT);
+        gs = sgs;
+    }
+    __device__ static int s(int ii, int jj, int kk) { return ((ii + 2) * SK + (kk + 2)) * SJ + (jj + 2); }
+    __device__ static int q(int ii, int jj, int kk) { return ((ii + 1) * GK + (kk + 1)) * GJP + (jj + 1); }
     __device__ static int cq(int ii, int jj) { return (ii + 1) * GJ + (jj + 1); }
     __device__ R &S(int f, int ii, int jj, int kk) { return st[f * SR + s(ii, jj, kk)]; }
     __device__ R &G(int f, int ii, int jj, int kk) { return gs[f * GR + q(ii, jj, kk)]; }
     __device__ R K(int kk, int e) const { return kr[(kk + 1) * KROW + e]; }
 };
+
+// Asynchronous global -> shared copies (cp.async, sm_80+ PTX).  src_bytes 0
+// writes zeros without reading, which gives the tile its zero halo in z.
+template <int B>
+__device__ __forceinline__ void cp_async(void *dst, const void *src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(d), "l"(src), "n"(B), "r"(valid ? B : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Issue the copies of one tile's inputs into buffer t (one commit group).
+// Periodic in x and y (period N-1), zero outside 0..Nz-1 in z.
+template <class R, class TL, int NT>
+__device__ __forceinline__ void issue_tile(const StageArgs<R> &a, TL &t, int i0, int j0, int k0)
+{
+    const Geom &g = a.g;
+    const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz, N = g.N;
+    const R *__restrict__ X = a.X;
+    for (int c = threadIdx.x; c < TL::NCOL; c += NT) {
+        const int jj = c % TL::GJ - 1, ii = c / TL::GJ - 1;
+        const int gi = i0 + ii, gj = j0 + jj;
+        const bool ok = gi <= Nx && gj <= Ny;
+        const int col = ok ? wrap_p(gi, Nx - 1) * Ny + wrap_p(gj, Ny - 1) : 0;
+        cp_async<8>(t.ctopo + c, g.topo + col, ok);
+        cp_async<sizeof(R)>(t.cut_ + c, a.utau + col, ok);
+        cp_async<4>(t.cnzy + c, g.nzy + col, ok);
+        cp_async<4>(t.ccut + c, g.cut + col, ok);
+    }
+    for (int c = threadIdx.x; c < TL::GK * KROW; c += NT) {
+        const int gk = k0 - 1 + c / KROW;
+        const bool ok = gk >= 0 && gk < Nz;
+        cp_async<sizeof(R)>(t.kr + c, a.krow + (ok ? (size_t)gk * KROW + c % KROW : 0), ok);
+    }
+    for (int c = threadIdx.x; c < TL::SR; c += NT) {
+        const int kk = c % TL::SK - 2, jj = (c / TL::SK) % TL::SJ - 2, ii = c / (TL::SK * TL::SJ) - 2;
+        const int gk = k0 + kk;
+        const bool ok = gk >= 0 && gk < Nz && i0 + ii <= Nx + 1 && j0 + jj <= Ny + 1;
+        const size_t o = ok ? ((size_t)wrap_p(i0 + ii, Nx - 1) * Ny + wrap_p(j0 + jj, Ny - 1)) * Nz + gk : 0;
+#pragma unroll
+        for (int f = 0; f < 4; f++) cp_async<sizeof(R)>(t.st + f * TL::SR + TL::s(ii, jj, kk), X + (size_t)f * N + o, ok);
+    }
+    cp_async_commit();
+}
 
 // upwind derivative from 5 weights (zero weights leave the sum unchanged)
 template <class R> __device__ __forceinline__ R dz5(const R *w, R m2, R m1, R c, R p1, R p2)
@@ -189,327 +251,303 @@ template <class R> __device__ __forceinline__ R dz5(const R *w, R m2, R m1, R c,
     return w[0] * m2 + w[1] * m1 + w[2] * c + w[3] * p1 + w[4] * p2;
 }
 
-// One RK stage for a TI x TJ x KZ tile (reference RHS pde.cu:139-787,
-// turbulence.cu:255-454, RK combination solver.cu:14-93):
-//   1. column tables, z rows, stage input with halo 2 -> shared memory
+// One RK stage over TI x TJ x KZ tiles (reference RHS pde.cu:139-787,
+// turbulence.cu:255-454, RK combination solver.cu:14-93).  Persistent: each
+// block walks tiles blockIdx.x, + gridDim.x, ...; while it computes one tile
+// the inputs of its next tile arrive in the other buffer.  Per tile:
+//   1. column tables, z rows, stage input with halo 2, fuel with halo 1
+//      -> shared memory (issued one tile ahead)
 //   2. SGS inputs (raw mu_sgs, strain S', divergence source) on the tile and
 //      its halo 1 -> shared memory
 //   3. per tile cell: advection, diffusion, forces, reaction, SGS divergence,
 //      RK update.  Cells the boundary rules overwrite (k <= cut node, top) are
 //      left to k_stage_bc; the values it needs are stored in a.bc.
-template <class R, int TI, int TJ, int KZ, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_stage_fused(const StageArgs<R> a)
+template <class R, int TI, int TJ, int KZ, int NT>
+__global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_stage_fused(const StageArgs<R> a, int ntk, int ntj, int nti)
 {
     using TL = Tile<R, TI, TJ, KZ>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    TL t;
-    t.st = reinterpret_cast<R *>(smem_raw);
-    t.gs = t.st + 4 * TL::SR;
-    t.gy = t.gs + 8 * TL::GR;
-    t.kr = t.gy + TL::GR;
-    t.ctopo = t.kr + TL::GK * KROW;
-    t.cut_ = t.ctopo + TL::NCOL;
-    t.cnzy = reinterpret_cast<int *>(t.cut_ + TL::NCOL);
-    t.ccut = t.cnzy + TL::NCOL;
+    R *sgs = reinterpret_cast<R *>(smem_raw + TL::BUF);
     const Geom &g = a.g;
     const PhysR<R> &p = a.pr;
     const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz, N = g.N;
-    const int k0 = blockIdx.x * KZ, j0 = blockIdx.y * TJ, i0 = blockIdx.z * TI;
     const R *__restrict__ X = a.X;
+    const int ntiles = ntk * ntj * nti;
+    int tile = blockIdx.x;
+    if (tile >= ntiles) return;
+    {
+        TL t0;
+        t0.bind(smem_raw, sgs);
+        issue_tile<R, TL, NT>(a, t0, (tile / (ntk * ntj)) * TI, ((tile / ntk) % ntj) * TJ, (tile % ntk) * KZ);
+    }
+    for (int it = 0; tile < ntiles; tile += gridDim.x, it++) {
+        TL t;
+        t.bind(smem_raw, sgs);
+        const int k0 = (tile % ntk) * KZ, j0 = ((tile / ntk) % ntj) * TJ, i0 = (tile / (ntk * ntj)) * TI;
+        const int nxt = tile + gridDim.x;
+        (void)nxt;
+            cp_async_commit();   // empty group keeps the wait below uniform
+        cp_async_wait<1>();      // this tile's group has landed
+        __syncthreads();
 
-    // ---- 1a. column tables (halo 1) and z-stencil rows
-    for (int c = threadIdx.x; c < TL::NCOL; c += blockDim.x) {
-        const int jj = c % TL::GJ - 1, ii = c / TL::GJ - 1;
-        const int gi = i0 + ii, gj = j0 + jj;
-        R tp = R(0), ut = R(0);
-        int nz = 0, ct = 0;
-        if (gi <= Nx && gj <= Ny) {
-            const int col = wrap_p(gi, Nx - 1) * Ny + wrap_p(gj, Ny - 1);
-            tp = (R)__ldg(g.topo + col);
-            ut = __ldg(a.utau + col);
-            nz = __ldg(g.nzy + col);
-            ct = __ldg(g.cut + col);
-        }
-        t.ctopo[c] = tp;
-        t.cut_[c] = ut;
-        t.cnzy[c] = nz;
-        t.ccut[c] = ct;
-    }
-    for (int c = threadIdx.x; c < TL::GK * KROW; c += blockDim.x) {
-        const int gk = k0 - 1 + c / KROW;
-        t.kr[c] = (gk >= 0 && gk < Nz) ? __ldg(a.krow + (size_t)gk * KROW + c % KROW) : R(0);
-    }
-    // ---- 1b. state tile with halo 2 (periodic in x, y; zero outside 0..Nz-1)
-    for (int c = threadIdx.x; c < TL::SR; c += blockDim.x) {
-        const int kk = c % TL::SK - 2, jj = (c / TL::SK) % TL::SJ - 2, ii = c / (TL::SK * TL::SJ) - 2;
-        int gi = i0 + ii, gj = j0 + jj;
-        const int gk = k0 + kk;
-        R v0 = R(0), v1 = R(0), v2 = R(0), v3 = R(0);
-        if (gk >= 0 && gk < Nz && gi <= Nx + 1 && gj <= Ny + 1) {
-            gi = wrap_p(gi, Nx - 1);
-            gj = wrap_p(gj, Ny - 1);
-            const size_t o = ((size_t)gi * Ny + gj) * Nz + gk;
-            v0 = __ldg(X + o);
-            v1 = __ldg(X + N + o);
-            v2 = __ldg(X + 2 * (size_t)N + o);
-            v3 = __ldg(X + 3 * (size_t)N + o);
-        }
-        t.st[c] = v0;
-        t.st[TL::SR + c] = v1;
-        t.st[2 * TL::SR + c] = v2;
-        t.st[3 * TL::SR + c] = v3;
-    }
-    __syncthreads();
-    for (int c = threadIdx.x; c < TL::GR; c += blockDim.x) {
-        const int kk = c % TL::GK - 1, jj = (c / TL::GK) % TL::GJ - 1, ii = c / (TL::GK * TL::GJ) - 1;
-        const int gi = i0 + ii, gj = j0 + jj, gk = k0 + kk;
-        R y = R(0);
-        if (gk >= 0 && gi <= Nx && gj <= Ny && gk < t.cnzy[TL::cq(ii, jj)]) {
-            const int col = wrap_p(gi, Nx - 1) * Ny + wrap_p(gj, Ny - 1);
-            y = __ldg(X + 4 * (size_t)N + (size_t)col * g.NzY + gk);
-        }
-        t.gy[c] = y;
-    }
-    __syncthreads();
+        const int smu = a.ph.sutherland_viscosity, sk = a.ph.sutherland_conductivity;
 
-    const int smu = a.ph.sutherland_viscosity, sk = a.ph.sutherland_conductivity;
-
-    // ---- 2. SGS inputs on the tile and its halo 1 (pde.cu:632-765).  Needed
-    //        set: tile columns on k0-1 .. k0+KZ, side columns on k0 .. k0+KZ-1.
-    constexpr int NA = TI * TJ * (KZ + 2), NB = 2 * TJ * KZ, NC = TI * 2 * KZ;
-    for (int c = threadIdx.x; c < NA + NB + NC; c += blockDim.x) {
-        int ii, jj, kk;
-        if (c < NA) {
-            kk = c % (KZ + 2) - 1;
-            jj = (c / (KZ + 2)) % TJ;
-            ii = c / ((KZ + 2) * TJ);
-        } else if (c < NA + NB) {
-            const int d = c - NA;
-            kk = d % KZ;
-            jj = (d / KZ) % TJ;
-            ii = (d / (KZ * TJ)) ? TI : -1;
-        } else {
-            const int d = c - NA - NB;
-            kk = d % KZ;
-            jj = ((d / KZ) % 2) ? TJ : -1;
-            ii = d / (2 * KZ);
-        }
-        const int gk = k0 + kk;
-        if (gk < 0 || gk >= Nz || i0 + ii > Nx || j0 + jj > Ny) continue;
-        const R *pu = &t.S(0, ii, jj, 0), *pv = &t.S(1, ii, jj, 0), *pw = &t.S(2, ii, jj, 0), *pT = &t.S(3, ii, jj, 0);
-        const R ux = (t.S(0, ii + 1, jj, kk) - t.S(0, ii - 1, jj, kk)) * p.inv2dx;
-        const R uy = (t.S(0, ii, jj + 1, kk) - t.S(0, ii, jj - 1, kk)) * p.inv2dy;
-        const R vx = (t.S(1, ii + 1, jj, kk) - t.S(1, ii - 1, jj, kk)) * p.inv2dx;
-        const R vy = (t.S(1, ii, jj + 1, kk) - t.S(1, ii, jj - 1, kk)) * p.inv2dy;
-        const R wx = (t.S(2, ii + 1, jj, kk) - t.S(2, ii - 1, jj, kk)) * p.inv2dx;
-        const R wy = (t.S(2, ii, jj + 1, kk) - t.S(2, ii, jj - 1, kk)) * p.inv2dy;
-        const R Tc = pT[kk];
-        const R Txp = t.S(3, ii + 1, jj, kk), Txm = t.S(3, ii - 1, jj, kk);
-        const R Typ = t.S(3, ii, jj + 1, kk), Tym = t.S(3, ii, jj - 1, kk);
-        const R Tx = (Txp - Txm) * p.inv2dx, Ty = (Typ - Tym) * p.inv2dy;
-        const R Txx = (Txp - R(2) * Tc + Txm) * p.invdx2, Tyy = (Typ - R(2) * Tc + Tym) * p.invdy2;
-        R uz, vz, wz, Tz, Tzz;
-        if (gk > 0 && gk < Nz - 1) {
-            const R wc = t.K(kk, RD1);
-            uz = (pu[kk + 1] - pu[kk - 1]) * wc;
-            vz = (pv[kk + 1] - pv[kk - 1]) * wc;
-            wz = (pw[kk + 1] - pw[kk - 1]) * wc;
-            Tz = (pT[kk + 1] - pT[kk - 1]) * wc;
-            Tzz = t.K(kk, RD2) * pT[kk - 1] + t.K(kk, RD2 + 1) * Tc + t.K(kk, RD2 + 2) * pT[kk + 1];
-        } else {
-            // walls: one-sided stencils from the double table (planes k = 0 and Nz-1 only)
-            const double *zc = g.zc;
-            const bool bot = (gk == 0);
-            auto d1 = [&](const R *f) -> R {
-                if (bot) return (R)zc[ZF0 * Nz] * f[kk] + (R)zc[ZF1 * Nz] * f[kk + 1] + (R)zc[ZF2 * Nz] * f[kk + 2];
-                return (R)zc[ZB0 * Nz + gk] * f[kk - 2] + (R)zc[ZB1 * Nz + gk] * f[kk - 1] + (R)zc[ZB2 * Nz + gk] * f[kk];
-            };
-            uz = d1(pu);
-            vz = d1(pv);
-            wz = d1(pw);
-            Tz = d1(pT);
-            // the backward 4-point form needs k-3, inside the tile unless the
-            // top plane is alone in its tile (then no cell of this tile needs it)
-            const R m3 = (kk >= 1) ? pT[kk - 3] : R(0), p3 = (kk <= KZ - 2) ? pT[kk + 3] : R(0);
-            Tzz = bot ? (R)zc[ZFF0 * Nz] * Tc + (R)zc[ZFF1 * Nz] * pT[kk + 1] + (R)zc[ZFF2 * Nz] * pT[kk + 2] +
-                            (R)zc[ZFF3 * Nz] * p3
-                      : (R)zc[ZBB0 * Nz + gk] * m3 + (R)zc[ZBB1 * Nz + gk] * pT[kk - 2] +
-                            (R)zc[ZBB2 * Nz + gk] * pT[kk - 1] + (R)zc[ZBB3 * Nz + gk] * Tc;
-        }
-        const R rho = fdiv(p.Trho, Tc);
-        const R S11 = third(R(2) * ux) - third(vy + wz);
-        const R S22 = third(R(2) * vy) - third(ux + wz);
-        const R S33 = third(R(2) * wz) - third(ux + vy);
-        const R mod_S = rsqrt_(R(2) * (ux * ux + vy * vy + wz * wz) + (uz + wx) * (uz + wx) + (vx + uy) * (vx + uy) +
-                               (wy + vz) * (wy + vz));
-        const int nzy = t.cnzy[TL::cq(ii, jj)];
-        const Thermo<R> th = thermo(p, smu, sk, Tc, pT[kk + 1], t.gy[TL::q(ii, jj, kk)], gk, nzy, Tx, Ty, Tz,
-                                    Txx + Tyy + Tzz, t.K(kk, RDZ), rho);
-        t.G(0, ii, jj, kk) = rho * t.K(kk, RDEL2) * mod_S;
-        t.G(1, ii, jj, kk) = S11;
-        t.G(2, ii, jj, kk) = R(0.5) * (uy + vx);
-        t.G(3, ii, jj, kk) = R(0.5) * (uz + wx);
-        t.G(4, ii, jj, kk) = S22;
-        t.G(5, ii, jj, kk) = R(0.5) * (wy + vz);
-        t.G(6, ii, jj, kk) = S33;
-        t.G(7, ii, jj, kk) = fdiv(th.nu * th.T_RHS_tmp, Tc);
-    }
-    __syncthreads();
-
-    // ---- 3. right-hand side, SGS divergence, RK update per tile cell
-    const R an = (R)a.a_next;
-    const bool rd = stage_reads_acc(a.method, a.stage), kp = stage_keeps_acc(a.method, a.stage);
-    for (int c = threadIdx.x; c < TL::CELLS; c += blockDim.x) {
-        const int kk = c % KZ, jj = (c / KZ) % TJ, ii = c / (KZ * TJ);
-        const int gi = i0 + ii, gj = j0 + jj, gk = k0 + kk;
-        if (gi >= Nx || gj >= Ny || gk >= Nz) continue;
-        const int col = gi * Ny + gj;
-        const int cc = TL::cq(ii, jj);
-        const int kc = t.ccut[cc], nzy = t.cnzy[cc];
-        const bool live = (gk > kc) && (gk < Nz - 1);                 // not overwritten by the boundary rules
-        const bool ylive = (gk < g.NzY) && !(gk <= kc && gk < nzy);   // fuel value this pass updates
-        if (!live && !ylive) continue;
-        const size_t cg = (size_t)col * Nz + gk;
-        // start the RK operand loads early
-        R ynv[4], accv[4];
-        if (live) {
-#pragma unroll
-            for (int f = 0; f < 4; f++) {
-                ynv[f] = a.yn[(size_t)f * N + cg];
-                accv[f] = rd ? a.acc[(size_t)f * N + cg] : R(0);
+        // ---- 2. SGS inputs on the tile and its halo 1 (pde.cu:632-765).  Needed
+        //        set: tile columns on k0-1 .. k0+KZ, side columns on k0 .. k0+KZ-1.
+        //        Enumerated so that each warp covers 8 consecutive k x 4 j where
+        //        it can: tile columns k0-1..k0+6, tile columns k0+7..k0+8,
+        //        x-side columns, y-side columns.
+        static_assert(KZ == 8, "phase-2 enumeration assumes 8 planes per tile");
+        constexpr int NA1 = TI * TJ * 8, NA2 = TI * TJ * 2, NB = 2 * TJ * KZ, NC = TI * 2 * KZ;
+        for (int c = threadIdx.x; c < NA1 + NA2 + NB + NC; c += NT) {
+            int ii, jj, kk;
+            if (c < NA1) {
+                kk = c % 8 - 1;
+                jj = (c / 8) % TJ;
+                ii = c / (8 * TJ);
+            } else if (c < NA1 + NA2) {
+                const int d = c - NA1;
+                kk = 7 + d % 2;
+                jj = (d / 2) % TJ;
+                ii = d / (2 * TJ);
+            } else if (c < NA1 + NA2 + NB) {
+                const int d = c - NA1 - NA2;
+                kk = d % KZ;
+                jj = (d / KZ) % TJ;
+                ii = (d / (KZ * TJ)) ? TI : -1;
+            } else {
+                const int d = c - NA1 - NA2 - NB;
+                kk = d % KZ;
+                jj = ((d / KZ) % 2) ? TJ : -1;
+                ii = d / (2 * KZ);
             }
-        }
-        const size_t oY = 4 * (size_t)N + (size_t)col * g.NzY + gk;
-        R ynY = R(0), accY = R(0);
-        if (ylive) {
-            ynY = a.yn[oY];
-            accY = rd ? a.acc[oY] : R(0);
-        }
-        R kY = R(0);
-        if (live) {
-            const R *kmw = &t.kr[(kk + 1) * KROW + RKM], *kpw = &t.kr[(kk + 1) * KROW + RKP];
-            const R d2m = t.K(kk, RD2), d20 = t.K(kk, RD2 + 1), d2p = t.K(kk, RD2 + 2);
-            const R u = t.S(0, ii, jj, kk), v = t.S(1, ii, jj, kk), w = t.S(2, ii, jj, kk), T = t.S(3, ii, jj, kk);
-            const R u_plu = rmax(u, R(0)), u_min = rmin(u, R(0));
-            const R v_plu = rmax(v, R(0)), v_min = rmin(v, R(0));
-            const R w_plu = rmax(w, R(0)), w_min = rmin(w, R(0));
-            // advection (upwind) and Laplacian of one field from the shared tile
-            auto adv_lap = [&](int f, R f0, R &adv, R &fxx, R &fyy, R &fzz, R &fx, R &fy, R &fz) {
-                const R *pc = &t.S(f, ii, jj, 0);
-                const R xm = t.S(f, ii - 1, jj, kk), xp = t.S(f, ii + 1, jj, kk);
-                const R xm2 = t.S(f, ii - 2, jj, kk), xp2 = t.S(f, ii + 2, jj, kk);
-                const R ym = t.S(f, ii, jj - 1, kk), yp = t.S(f, ii, jj + 1, kk);
-                const R ym2 = t.S(f, ii, jj - 2, kk), yp2 = t.S(f, ii, jj + 2, kk);
-                const R zm2 = pc[kk - 2], zm = pc[kk - 1], zp = pc[kk + 1], zp2 = pc[kk + 2];
-                const R im = (R(3) * f0 - R(4) * xm + xm2) * p.inv2dx;
-                const R ip = (R(-3) * f0 + R(4) * xp - xp2) * p.inv2dx;
-                const R jm = (R(3) * f0 - R(4) * ym + ym2) * p.inv2dy;
-                const R jp = (R(-3) * f0 + R(4) * yp - yp2) * p.inv2dy;
-                const R km = dz5(kmw, zm2, zm, f0, zp, zp2), kpv = dz5(kpw, zm2, zm, f0, zp, zp2);
-                adv = (u_plu * im + u_min * ip) + (v_plu * jm + v_min * jp) + (w_plu * km + w_min * kpv);
-                fxx = (xp - R(2) * f0 + xm) * p.invdx2;
-                fyy = (yp - R(2) * f0 + ym) * p.invdy2;
-                fzz = d2m * zm + d20 * f0 + d2p * zp;
-                fx = (xp - xm) * p.inv2dx;
-                fy = (yp - ym) * p.inv2dy;
-                fz = (zp - zm) * t.K(kk, RD1);
-            };
-            R advT, Txx, Tyy, Tzz, Tx, Ty, Tz;
-            adv_lap(3, T, advT, Txx, Tyy, Tzz, Tx, Ty, Tz);
-            const R rho = fdiv(p.Trho, T);
-            const Thermo<R> th = thermo(p, smu, sk, T, t.S(3, ii, jj, kk + 1), t.gy[TL::q(ii, jj, kk)], gk, nzy, Tx,
-                                        Ty, Tz, Txx + Tyy + Tzz, t.K(kk, RDZ), rho);
-            kY = -p.Y_f * th.K_T * th.Y;
-            R kval[4];
-            kval[3] = (a.ph.temperature_convection == 0) ? th.T_RHS_tmp - (u * Tx + v * Ty + w * Tz)
-                                                         : th.T_RHS_tmp - advT;
-            const R mod_U = rsqrt_(u * u + v * v + w * w);
-            {
-                R adv, fxx, fyy, fzz, fx, fy, fz;
-                adv_lap(0, u, adv, fxx, fyy, fzz, fx, fy, fz);
-                kval[0] = th.nu * (fxx + fyy + fzz) - adv + (-p.cd * th.Y * mod_U * u);
-                adv_lap(1, v, adv, fxx, fyy, fzz, fx, fy, fz);
-                kval[1] = th.nu * (fxx + fyy + fzz) - adv + (-p.cd * th.Y * mod_U * v);
-                adv_lap(2, w, adv, fxx, fyy, fzz, fx, fy, fz);
-                kval[2] = th.nu * (fxx + fyy + fzz) - adv + (fdiv(p.g * (rho - p.rho_inf), rho) - p.cd * th.Y * mod_U * w);
-            }
-            // ---- SGS divergence with Van Driest damping (turbulence.cu:255-454)
-            {
-                const R nu = fdiv(p.mu, rho);
-                const R inv_avd_nu = fdiv(p.inv_avd, nu);
-                const R zk = t.K(kk, RZ);
-                auto zibm = [&](int q, R zz) -> R {
-                    const R d = zz - t.ctopo[q];
-                    return d > R(0) ? d : R(0);
-                };
-                const int qxp = TL::cq(ii + 1, jj), qxm = TL::cq(ii - 1, jj);
-                const int qyp = TL::cq(ii, jj + 1), qym = TL::cq(ii, jj - 1);
-                const R ut0 = t.cut_[cc];
-                const R fc = van_driest(-zibm(cc, zk) * ut0 * inv_avd_nu);
-                const R fxp_ = van_driest(-zibm(qxp, zk) * t.cut_[qxp] * inv_avd_nu);
-                const R fxm_ = van_driest(-zibm(qxm, zk) * t.cut_[qxm] * inv_avd_nu);
-                const R fyp_ = van_driest(-zibm(qyp, zk) * t.cut_[qyp] * inv_avd_nu);
-                const R fym_ = van_driest(-zibm(qym, zk) * t.cut_[qym] * inv_avd_nu);
-                const R fkm = van_driest(-zibm(cc, t.K(kk - 1, RZ)) * ut0 * inv_avd_nu);
-                const R fkp = van_driest(-zibm(cc, t.K(kk + 1, RZ)) * ut0 * inv_avd_nu);
-                const R mu_c = t.G(0, ii, jj, kk) * (fc * fc);
-                const R mu_xp = t.G(0, ii + 1, jj, kk) * (fxp_ * fxp_), mu_xm = t.G(0, ii - 1, jj, kk) * (fxm_ * fxm_);
-                const R mu_yp = t.G(0, ii, jj + 1, kk) * (fyp_ * fyp_), mu_ym = t.G(0, ii, jj - 1, kk) * (fym_ * fym_);
-                const R mu_kp = t.G(0, ii, jj, kk + 1) * (fkp * fkp), mu_km = t.G(0, ii, jj, kk - 1) * (fkm * fkm);
-                const R S11 = t.G(1, ii, jj, kk), S12 = t.G(2, ii, jj, kk), S13 = t.G(3, ii, jj, kk);
-                const R S22 = t.G(4, ii, jj, kk), S23 = t.G(5, ii, jj, kk), S33 = t.G(6, ii, jj, kk);
+            const int gk = k0 + kk;
+            if (gk < 0 || gk >= Nz || i0 + ii > Nx || j0 + jj > Ny) continue;
+            const R *pu = &t.S(0, ii, jj, 0), *pv = &t.S(1, ii, jj, 0), *pw = &t.S(2, ii, jj, 0), *pT = &t.S(3, ii, jj, 0);
+            const R ux = (t.S(0, ii + 1, jj, kk) - t.S(0, ii - 1, jj, kk)) * p.inv2dx;
+            const R uy = (t.S(0, ii, jj + 1, kk) - t.S(0, ii, jj - 1, kk)) * p.inv2dy;
+            const R vx = (t.S(1, ii + 1, jj, kk) - t.S(1, ii - 1, jj, kk)) * p.inv2dx;
+            const R vy = (t.S(1, ii, jj + 1, kk) - t.S(1, ii, jj - 1, kk)) * p.inv2dy;
+            const R wx = (t.S(2, ii + 1, jj, kk) - t.S(2, ii - 1, jj, kk)) * p.inv2dx;
+            const R wy = (t.S(2, ii, jj + 1, kk) - t.S(2, ii, jj - 1, kk)) * p.inv2dy;
+            constexpr int ZS = TL::ZS;
+            const R Tc = pT[kk * ZS];
+            const R Txp = t.S(3, ii + 1, jj, kk), Txm = t.S(3, ii - 1, jj, kk);
+            const R Typ = t.S(3, ii, jj + 1, kk), Tym = t.S(3, ii, jj - 1, kk);
+            const R Tx = (Txp - Txm) * p.inv2dx, Ty = (Typ - Tym) * p.inv2dy;
+            const R Txx = (Txp - R(2) * Tc + Txm) * p.invdx2, Tyy = (Typ - R(2) * Tc + Tym) * p.invdy2;
+            R uz, vz, wz, Tz, Tzz;
+            if (gk > 0 && gk < Nz - 1) {
                 const R wc = t.K(kk, RD1);
-                const R mu_x = (mu_xp - mu_xm) * p.inv2dx, mu_y = (mu_yp - mu_ym) * p.inv2dy, mu_z = (mu_kp - mu_km) * wc;
-                const R S11_x = (t.G(1, ii + 1, jj, kk) - t.G(1, ii - 1, jj, kk)) * p.inv2dx;
-                const R S12_x = (t.G(2, ii + 1, jj, kk) - t.G(2, ii - 1, jj, kk)) * p.inv2dx;
-                const R S13_x = (t.G(3, ii + 1, jj, kk) - t.G(3, ii - 1, jj, kk)) * p.inv2dx;
-                const R S21_y = (t.G(2, ii, jj + 1, kk) - t.G(2, ii, jj - 1, kk)) * p.inv2dy;
-                const R S22_y = (t.G(4, ii, jj + 1, kk) - t.G(4, ii, jj - 1, kk)) * p.inv2dy;
-                const R S23_y = (t.G(5, ii, jj + 1, kk) - t.G(5, ii, jj - 1, kk)) * p.inv2dy;
-                const R S31_z = (t.G(3, ii, jj, kk + 1) - t.G(3, ii, jj, kk - 1)) * wc;
-                const R S32_z = (t.G(5, ii, jj, kk + 1) - t.G(5, ii, jj, kk - 1)) * wc;
-                const R S33_z = (t.G(6, ii, jj, kk + 1) - t.G(6, ii, jj, kk - 1)) * wc;
-                const R dU_x = (t.G(7, ii + 1, jj, kk) - t.G(7, ii - 1, jj, kk)) * p.inv2dx;
-                const R dU_y = (t.G(7, ii, jj + 1, kk) - t.G(7, ii, jj - 1, kk)) * p.inv2dy;
-                const R dU_z = (t.G(7, ii, jj, kk + 1) - t.G(7, ii, jj, kk - 1)) * wc;
-                const R div_S_x = S11_x + S21_y + S31_z;
-                const R div_S_y = S12_x + S22_y + S32_z;
-                const R div_S_z = S13_x + S23_y + S33_z;
-                const R inv_rho = fdiv(R(1), rho);
-                const R sgs_x = R(-2) * (mu_x * S11 + mu_y * S12 + mu_z * S13 + mu_c * div_S_x) * inv_rho;
-                const R sgs_y = R(-2) * (mu_x * S12 + mu_y * S22 + mu_z * S23 + mu_c * div_S_y) * inv_rho;
-                const R sgs_z = R(-2) * (mu_x * S13 + mu_y * S23 + mu_z * S33 + mu_c * div_S_z) * inv_rho;
-                const R sgs_q = -fdiv(mu_x * Tx + mu_y * Ty + mu_z * Tz + mu_c * (Txx + Tyy + Tzz), rho * p.Pr);
-                kval[0] += -sgs_x + third(dU_x);
-                kval[1] += -sgs_y + third(dU_y);
-                kval[2] += -sgs_z + third(dU_z);
-                kval[3] -= sgs_q;
+                uz = (pu[(kk + 1) * ZS] - pu[(kk - 1) * ZS]) * wc;
+                vz = (pv[(kk + 1) * ZS] - pv[(kk - 1) * ZS]) * wc;
+                wz = (pw[(kk + 1) * ZS] - pw[(kk - 1) * ZS]) * wc;
+                Tz = (pT[(kk + 1) * ZS] - pT[(kk - 1) * ZS]) * wc;
+                Tzz = t.K(kk, RD2) * pT[(kk - 1) * ZS] + t.K(kk, RD2 + 1) * Tc + t.K(kk, RD2 + 2) * pT[(kk + 1) * ZS];
+            } else {
+                // walls: one-sided stencils from the double table (planes k = 0 and Nz-1 only)
+                const double *zc = g.zc;
+                const bool bot = (gk == 0);
+                auto d1 = [&](const R *f) -> R {
+                    if (bot) return (R)zc[ZF0 * Nz] * f[kk * ZS] + (R)zc[ZF1 * Nz] * f[(kk + 1) * ZS] + (R)zc[ZF2 * Nz] * f[(kk + 2) * ZS];
+                    return (R)zc[ZB0 * Nz + gk] * f[(kk - 2) * ZS] + (R)zc[ZB1 * Nz + gk] * f[(kk - 1) * ZS] + (R)zc[ZB2 * Nz + gk] * f[kk * ZS];
+                };
+                uz = d1(pu);
+                vz = d1(pv);
+                wz = d1(pw);
+                Tz = d1(pT);
+                // the backward 4-point form needs k-3, inside the tile unless the
+                // top plane is alone in its tile (then no cell of this tile needs it)
+                const R m3 = (kk >= 1) ? pT[(kk - 3) * ZS] : R(0), p3 = (kk <= KZ - 2) ? pT[(kk + 3) * ZS] : R(0);
+                Tzz = bot ? (R)zc[ZFF0 * Nz] * Tc + (R)zc[ZFF1 * Nz] * pT[(kk + 1) * ZS] + (R)zc[ZFF2 * Nz] * pT[(kk + 2) * ZS] +
+                                (R)zc[ZFF3 * Nz] * p3
+                          : (R)zc[ZBB0 * Nz + gk] * m3 + (R)zc[ZBB1 * Nz + gk] * pT[(kk - 2) * ZS] +
+                                (R)zc[ZBB2 * Nz + gk] * pT[(kk - 1) * ZS] + (R)zc[ZBB3 * Nz + gk] * Tc;
             }
-            // values the column boundary pass needs
-            R *bcs = a.bc + (size_t)col * kBcSlots;
-            if (gk == kc + 1) { bcs[0] = kval[3]; bcs[2] = (gk < nzy) ? kY : R(0); }
-            if (gk == kc + 2) { bcs[1] = kval[3]; bcs[3] = (gk < nzy) ? kY : R(0); }
-            if (gk == Nz - 2) { bcs[4] = kval[0]; bcs[5] = kval[1]; bcs[6] = kval[2]; bcs[7] = kval[3]; }
-            if (gk == Nz - 3) { bcs[8] = kval[0]; bcs[9] = kval[1]; bcs[10] = kval[2]; bcs[11] = kval[3]; }
-#pragma unroll
-            for (int f = 0; f < 4; f++) {
-                const size_t o = (size_t)f * N + cg;
-                a.Xout[o] = rk_update(a.method, a.stage, kval[f], ynv[f], accv[f], an);
-                if (kp) a.acc[o] = accv[f];
+            const R rho = fdiv(p.Trho, Tc);
+            const R S11 = third(R(2) * ux) - third(vy + wz);
+            const R S22 = third(R(2) * vy) - third(ux + wz);
+            const R S33 = third(R(2) * wz) - third(ux + vy);
+            const R mod_S = rsqrt_(R(2) * (ux * ux + vy * vy + wz * wz) + (uz + wx) * (uz + wx) + (vx + uy) * (vx + uy) +
+                                   (wy + vz) * (wy + vz));
+            const int nzy = t.cnzy[TL::cq(ii, jj)];
+            // fuel fraction of the stage input (used only below the column's fuel top)
+            const R Yq = (gk < nzy) ? X[4 * (size_t)N + (size_t)(wrap_p(i0 + ii, Nx - 1) * Ny + wrap_p(j0 + jj, Ny - 1)) * g.NzY + gk]
+                                    : R(0);
+            const Thermo<R> th = thermo(p, smu, sk, Tc, pT[(kk + 1) * ZS], Yq, gk, nzy, Tx, Ty, Tz,
+                                        Txx + Tyy + Tzz, t.K(kk, RDZ), rho);
+            t.G(0, ii, jj, kk) = rho * t.K(kk, RDEL2) * mod_S;
+            t.G(1, ii, jj, kk) = S11;
+            t.G(2, ii, jj, kk) = R(0.5) * (uy + vx);
+            t.G(3, ii, jj, kk) = R(0.5) * (uz + wx);
+            t.G(4, ii, jj, kk) = S22;
+            t.G(5, ii, jj, kk) = R(0.5) * (wy + vz);
+            t.G(6, ii, jj, kk) = S33;
+            t.G(7, ii, jj, kk) = fdiv(th.nu * th.T_RHS_tmp, Tc);
+        }
+        __syncthreads();
+
+        // ---- 3. right-hand side, SGS divergence, RK update per tile cell
+        const R an = (R)a.a_next;
+        const bool rd = stage_reads_acc(a.method, a.stage), kp = stage_keeps_acc(a.method, a.stage);
+        for (int c = threadIdx.x; c < TL::CELLS; c += NT) {
+            const int kk = c % KZ, jj = (c / KZ) % TJ, ii = c / (KZ * TJ);
+            const int gi = i0 + ii, gj = j0 + jj, gk = k0 + kk;
+            if (gi >= Nx || gj >= Ny || gk >= Nz) continue;
+            const int col = gi * Ny + gj;
+            const int cc = TL::cq(ii, jj);
+            const int kc = t.ccut[cc], nzy = t.cnzy[cc];
+            const bool live = (gk > kc) && (gk < Nz - 1);                 // not overwritten by the boundary rules
+            const bool ylive = (gk < g.NzY) && !(gk <= kc && gk < nzy);   // fuel value this pass updates
+            if (!live && !ylive) continue;
+            const size_t cg = (size_t)col * Nz + gk;
+            // start the RK operand loads early
+            R ynv[4], accv[4];
+            if (live) {
+    #pragma unroll
+                for (int f = 0; f < 4; f++) {
+                    ynv[f] = a.yn[(size_t)f * N + cg];
+                    accv[f] = rd ? a.acc[(size_t)f * N + cg] : R(0);
+                }
             }
-        } else if (gk < nzy) {
-            // fuel cell whose velocity and temperature the boundary rules set (top plane)
-            const R T = t.S(3, ii, jj, kk);
-            const R K_T = (T > p.T_pc) ? p.A * rexp(-fdiv(p.T_act, T)) * R(1) : R(0);
-            kY = -p.Y_f * K_T * t.gy[TL::q(ii, jj, kk)];
+            const size_t oY = 4 * (size_t)N + (size_t)col * g.NzY + gk;
+            R ynY = R(0), accY = R(0);
+            if (ylive) {
+                ynY = a.yn[oY];
+                accY = rd ? a.acc[oY] : R(0);
+            }
+            R kY = R(0);
+            // fuel fraction of the stage input (used only below the column's fuel top)
+            const R Yx = (gk < nzy) ? X[4 * (size_t)N + (size_t)col * g.NzY + gk] : R(0);
+            if (live) {
+                const R *kmw = &t.kr[(kk + 1) * KROW + RKM], *kpw = &t.kr[(kk + 1) * KROW + RKP];
+                const R d2m = t.K(kk, RD2), d20 = t.K(kk, RD2 + 1), d2p = t.K(kk, RD2 + 2);
+                const R u = t.S(0, ii, jj, kk), v = t.S(1, ii, jj, kk), w = t.S(2, ii, jj, kk), T = t.S(3, ii, jj, kk);
+                const R u_plu = rmax(u, R(0)), u_min = rmin(u, R(0));
+                const R v_plu = rmax(v, R(0)), v_min = rmin(v, R(0));
+                const R w_plu = rmax(w, R(0)), w_min = rmin(w, R(0));
+                // advection (upwind) and Laplacian of one field from the shared tile
+                auto adv_lap = [&](int f, R f0, R &adv, R &fxx, R &fyy, R &fzz, R &fx, R &fy, R &fz) {
+                    const R *pc = &t.S(f, ii, jj, 0);
+                    const R xm = t.S(f, ii - 1, jj, kk), xp = t.S(f, ii + 1, jj, kk);
+                    const R xm2 = t.S(f, ii - 2, jj, kk), xp2 = t.S(f, ii + 2, jj, kk);
+                    const R ym = t.S(f, ii, jj - 1, kk), yp = t.S(f, ii, jj + 1, kk);
+                    const R ym2 = t.S(f, ii, jj - 2, kk), yp2 = t.S(f, ii, jj + 2, kk);
+                    constexpr int ZS = TL::ZS;
+                    const R zm2 = pc[(kk - 2) * ZS], zm = pc[(kk - 1) * ZS], zp = pc[(kk + 1) * ZS], zp2 = pc[(kk + 2) * ZS];
+                    const R im = (R(3) * f0 - R(4) * xm + xm2) * p.inv2dx;
+                    const R ip = (R(-3) * f0 + R(4) * xp - xp2) * p.inv2dx;
+                    const R jm = (R(3) * f0 - R(4) * ym + ym2) * p.inv2dy;
+                    const R jp = (R(-3) * f0 + R(4) * yp - yp2) * p.inv2dy;
+                    const R km = dz5(kmw, zm2, zm, f0, zp, zp2), kpv = dz5(kpw, zm2, zm, f0, zp, zp2);
+                    adv = (u_plu * im + u_min * ip) + (v_plu * jm + v_min * jp) + (w_plu * km + w_min * kpv);
+                    fxx = (xp - R(2) * f0 + xm) * p.invdx2;
+                    fyy = (yp - R(2) * f0 + ym) * p.invdy2;
+                    fzz = d2m * zm + d20 * f0 + d2p * zp;
+                    fx = (xp - xm) * p.inv2dx;
+                    fy = (yp - ym) * p.inv2dy;
+                    fz = (zp - zm) * t.K(kk, RD1);
+                };
+                R advT, Txx, Tyy, Tzz, Tx, Ty, Tz;
+                adv_lap(3, T, advT, Txx, Tyy, Tzz, Tx, Ty, Tz);
+                const R rho = fdiv(p.Trho, T);
+                const Thermo<R> th = thermo(p, smu, sk, T, t.S(3, ii, jj, kk + 1), Yx, gk, nzy, Tx,
+                                            Ty, Tz, Txx + Tyy + Tzz, t.K(kk, RDZ), rho);
+                kY = -p.Y_f * th.K_T * th.Y;
+                R kval[4];
+                kval[3] = (a.ph.temperature_convection == 0) ? th.T_RHS_tmp - (u * Tx + v * Ty + w * Tz)
+                                                             : th.T_RHS_tmp - advT;
+                const R mod_U = rsqrt_(u * u + v * v + w * w);
+                {
+                    R adv, fxx, fyy, fzz, fx, fy, fz;
+                    adv_lap(0, u, adv, fxx, fyy, fzz, fx, fy, fz);
+                    kval[0] = th.nu * (fxx + fyy + fzz) - adv + (-p.cd * th.Y * mod_U * u);
+                    adv_lap(1, v, adv, fxx, fyy, fzz, fx, fy, fz);
+                    kval[1] = th.nu * (fxx + fyy + fzz) - adv + (-p.cd * th.Y * mod_U * v);
+                    adv_lap(2, w, adv, fxx, fyy, fzz, fx, fy, fz);
+                    kval[2] = th.nu * (fxx + fyy + fzz) - adv + (fdiv(p.g * (rho - p.rho_inf), rho) - p.cd * th.Y * mod_U * w);
+                }
+                // ---- SGS divergence with Van Driest damping (turbulence.cu:255-454)
+                {
+                    const R nu = fdiv(p.mu, rho);
+                    const R inv_avd_nu = fdiv(p.inv_avd, nu);
+                    const R zk = t.K(kk, RZ);
+                    auto zibm = [&](int q, R zz) -> R {
+                        const R d = zz - (R)t.ctopo[q];
+                        return d > R(0) ? d : R(0);
+                    };
+                    const int qxp = TL::cq(ii + 1, jj), qxm = TL::cq(ii - 1, jj);
+                    const int qyp = TL::cq(ii, jj + 1), qym = TL::cq(ii, jj - 1);
+                    const R ut0 = t.cut_[cc];
+                    const R fc = van_driest(-zibm(cc, zk) * ut0 * inv_avd_nu);
+                    const R fxp_ = van_driest(-zibm(qxp, zk) * t.cut_[qxp] * inv_avd_nu);
+                    const R fxm_ = van_driest(-zibm(qxm, zk) * t.cut_[qxm] * inv_avd_nu);
+                    const R fyp_ = van_driest(-zibm(qyp, zk) * t.cut_[qyp] * inv_avd_nu);
+                    const R fym_ = van_driest(-zibm(qym, zk) * t.cut_[qym] * inv_avd_nu);
+                    const R fkm = van_driest(-zibm(cc, t.K(kk - 1, RZ)) * ut0 * inv_avd_nu);
+                    const R fkp = van_driest(-zibm(cc, t.K(kk + 1, RZ)) * ut0 * inv_avd_nu);
+                    const R mu_c = t.G(0, ii, jj, kk) * (fc * fc);
+                    const R mu_xp = t.G(0, ii + 1, jj, kk) * (fxp_ * fxp_), mu_xm = t.G(0, ii - 1, jj, kk) * (fxm_ * fxm_);
+                    const R mu_yp = t.G(0, ii, jj + 1, kk) * (fyp_ * fyp_), mu_ym = t.G(0, ii, jj - 1, kk) * (fym_ * fym_);
+                    const R mu_kp = t.G(0, ii, jj, kk + 1) * (fkp * fkp), mu_km = t.G(0, ii, jj, kk - 1) * (fkm * fkm);
+                    const R S11 = t.G(1, ii, jj, kk), S12 = t.G(2, ii, jj, kk), S13 = t.G(3, ii, jj, kk);
+                    const R S22 = t.G(4, ii, jj, kk), S23 = t.G(5, ii, jj, kk), S33 = t.G(6, ii, jj, kk);
+                    const R wc = t.K(kk, RD1);
+                    const R mu_x = (mu_xp - mu_xm) * p.inv2dx, mu_y = (mu_yp - mu_ym) * p.inv2dy, mu_z = (mu_kp - mu_km) * wc;
+                    const R S11_x = (t.G(1, ii + 1, jj, kk) - t.G(1, ii - 1, jj, kk)) * p.inv2dx;
+                    const R S12_x = (t.G(2, ii + 1, jj, kk) - t.G(2, ii - 1, jj, kk)) * p.inv2dx;
+                    const R S13_x = (t.G(3, ii + 1, jj, kk) - t.G(3, ii - 1, jj, kk)) * p.inv2dx;
+                    const R S21_y = (t.G(2, ii, jj + 1, kk) - t.G(2, ii, jj - 1, kk)) * p.inv2dy;
+                    const R S22_y = (t.G(4, ii, jj + 1, kk) - t.G(4, ii, jj - 1, kk)) * p.inv2dy;
+                    const R S23_y = (t.G(5, ii, jj + 1, kk) - t.G(5, ii, jj - 1, kk)) * p.inv2dy;
+                    const R S31_z = (t.G(3, ii, jj, kk + 1) - t.G(3, ii, jj, kk - 1)) * wc;
+                    const R S32_z = (t.G(5, ii, jj, kk + 1) - t.G(5, ii, jj, kk - 1)) * wc;
+                    const R S33_z = (t.G(6, ii, jj, kk + 1) - t.G(6, ii, jj, kk - 1)) * wc;
+                    const R dU_x = (t.G(7, ii + 1, jj, kk) - t.G(7, ii - 1, jj, kk)) * p.inv2dx;
+                    const R dU_y = (t.G(7, ii, jj + 1, kk) - t.G(7, ii, jj - 1, kk)) * p.inv2dy;
+                    const R dU_z = (t.G(7, ii, jj, kk + 1) - t.G(7, ii, jj, kk - 1)) * wc;
+                    const R div_S_x = S11_x + S21_y + S31_z;
+                    const R div_S_y = S12_x + S22_y + S32_z;
+                    const R div_S_z = S13_x + S23_y + S33_z;
+                    const R inv_rho = fdiv(R(1), rho);
+                    const R sgs_x = R(-2) * (mu_x * S11 + mu_y * S12 + mu_z * S13 + mu_c * div_S_x) * inv_rho;
+                    const R sgs_y = R(-2) * (mu_x * S12 + mu_y * S22 + mu_z * S23 + mu_c * div_S_y) * inv_rho;
+                    const R sgs_z = R(-2) * (mu_x * S13 + mu_y * S23 + mu_z * S33 + mu_c * div_S_z) * inv_rho;
+                    const R sgs_q = -fdiv(mu_x * Tx + mu_y * Ty + mu_z * Tz + mu_c * (Txx + Tyy + Tzz), rho * p.Pr);
+                    kval[0] += -sgs_x + third(dU_x);
+                    kval[1] += -sgs_y + third(dU_y);
+                    kval[2] += -sgs_z + third(dU_z);
+                    kval[3] -= sgs_q;
+                }
+                // values the column boundary pass needs
+                R *bcs = a.bc + (size_t)col * kBcSlots;
+                if (gk == kc + 1) { bcs[0] = kval[3]; bcs[2] = (gk < nzy) ? kY : R(0); }
+                if (gk == kc + 2) { bcs[1] = kval[3]; bcs[3] = (gk < nzy) ? kY : R(0); }
+                if (gk == Nz - 2) { bcs[4] = kval[0]; bcs[5] = kval[1]; bcs[6] = kval[2]; bcs[7] = kval[3]; }
+                if (gk == Nz - 3) { bcs[8] = kval[0]; bcs[9] = kval[1]; bcs[10] = kval[2]; bcs[11] = kval[3]; }
+    #pragma unroll
+                for (int f = 0; f < 4; f++) {
+                    const size_t o = (size_t)f * N + cg;
+                    a.Xout[o] = rk_update(a.method, a.stage, kval[f], ynv[f], accv[f], an);
+                    if (kp) a.acc[o] = accv[f];
+                }
+            } else if (gk < nzy) {
+                // fuel cell whose velocity and temperature the boundary rules set (top plane)
+                const R T = t.S(3, ii, jj, kk);
+                const R K_T = (T > p.T_pc) ? p.A * rexp(-fdiv(p.T_act, T)) * R(1) : R(0);
+                kY = -p.Y_f * K_T * Yx;
+            }
+            if (ylive) {
+                const R kv = (gk < nzy) ? kY : R(0);
+                a.Xout[oY] = rk_update(a.method, a.stage, kv, ynY, accY, an);
+                if (kp) a.acc[oY] = accY;
+            }
         }
-        if (ylive) {
-            const R kv = (gk < nzy) ? kY : R(0);
-            a.Xout[oY] = rk_update(a.method, a.stage, kv, ynY, accY, an);
-            if (kp) a.acc[oY] = accY;
-        }
+        __syncthreads();         // buffer and SGS inputs free for the next tiles
     }
+    cp_async_wait<0>();
 }
+
 
 // ---------------------------------------------------------------------------
 // boundary/IBM k-values per column (pde.cu:14-99) and their RK update
@@ -592,11 +630,13 @@ __global__ void __launch_bounds__(256) k_stage_bc(const StageArgs<R> a)
 // (one block per SM).
 template <class R> struct StageCfg;
 template <> struct StageCfg<float> {
-    static constexpr int TI = 8, TJ = 16, KZ = 8, MINB = 2;
+    static constexpr int TI = 8, TJ = 16, KZ = 8, NT = 256;
 };
 template <> struct StageCfg<double> {
-    static constexpr int TI = 8, TJ = 8, KZ = 8, MINB = 1;
+    static constexpr int TI = 8, TJ = 8, KZ = 8, NT = 256;
 };
+
+int g_stage_sms = 0;   // multiprocessors of the device, read at set-up
 
 template <class R> size_t stage_smem_bytes()
 {
@@ -609,7 +649,11 @@ template size_t stage_smem_bytes<float>();
 template <class R> cudaError_t stage_set_attributes()
 {
     using C = StageCfg<R>;
-    return cudaFuncSetAttribute(k_stage_fused<R, C::TI, C::TJ, C::KZ, C::MINB>,
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (!e) e = cudaDeviceGetAttribute(&g_stage_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e) return e;
+    return cudaFuncSetAttribute(k_stage_fused<R, C::TI, C::TJ, C::KZ, C::NT>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<R>());
 }
 template cudaError_t stage_set_attributes<double>();
@@ -621,8 +665,10 @@ template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t 
     const int ncol = a.g.Nx * a.g.Ny;
     k_utau<R><<<(ncol + 127) / 128, 128, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[0], s);
-    dim3 grid((a.g.Nz + C::KZ - 1) / C::KZ, (a.g.Ny + C::TJ - 1) / C::TJ, (a.g.Nx + C::TI - 1) / C::TI);
-    k_stage_fused<R, C::TI, C::TJ, C::KZ, C::MINB><<<grid, 256, stage_smem_bytes<R>(), s>>>(a);
+    const int ntk = (a.g.Nz + C::KZ - 1) / C::KZ, ntj = (a.g.Ny + C::TJ - 1) / C::TJ, nti = (a.g.Nx + C::TI - 1) / C::TI;
+    const int ntiles = ntk * ntj * nti;
+    const int blocks = ntiles;
+    k_stage_fused<R, C::TI, C::TJ, C::KZ, C::NT><<<blocks, C::NT, stage_smem_bytes<R>(), s>>>(a, ntk, ntj, nti);
     if (ev) cudaEventRecord(ev[1], s);
     k_stage_bc<R><<<(ncol + 15) / 16, 256, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[2], s);
