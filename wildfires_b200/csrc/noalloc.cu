@@ -215,9 +215,6 @@ extern "C" wf_status wf_pressure_noalloc(const Parameters *P, const double *y_np
     a.fy.chirp = fy.bluestein ? base + oChy : nullptr;
     a.fy.filt = fy.bluestein ? base + oFly : nullptr;
     a.h1 = h1;
-    a.inv_dx = 1.0 / P->dx;
-    a.inv_dy = 1.0 / P->dy;
-    a.rho_dt = P->rho_inf / P->dt;
     e = launch_poisson_impl<double>(a, reinterpret_cast<const double *>(base + oZt), s);
     if (e) {
         set_error("wf_pressure_noalloc: %s", cudaGetErrorString(e));

@@ -59,19 +59,6 @@ __device__ double poisson_source(const PoissonArgs<R> &a, int i, int j, int k)
     const double u_im1 = U[cxm], u_ip1 = U[cxp];
     const double v_jm1 = U[(size_t)N + cym], v_jp1 = U[(size_t)N + cyp];
     const R *W = U + 2 * (size_t)N;
-    if constexpr (sizeof(R) == 4) {
-        // FP32 stencil path, constant density: the same FP64 source with the
-        // divisions by grid constants replaced by precomputed weights.
-        if (ph.variable_density == 0) {
-            const double *zc = g.zc;
-            const double wzf = (k == 0) ? zc[ZF0 * Nz] * (double)W[c] + zc[ZF1 * Nz] * (double)W[c + 1] +
-                                              zc[ZF2 * Nz] * (double)W[c + 2]
-                                        : ((double)W[c + 1] - (double)W[c - 1]) * zc[ZC * Nz + k];
-            const double uxf = (0.5 * (u_ip1 + u) - 0.5 * (u + u_im1)) * a.inv_dx;
-            const double vyf = (0.5 * (v_jp1 + v) - 0.5 * (v + v_jm1)) * a.inv_dy;
-            return (uxf + vyf + wzf) * a.rho_dt;
-        }
-    }
     double wz;
     double dzk_f = 0, dzkp1_f = 0, dzkp2_f = 0, dzkm1_c = 0, dzk_c = 0;
     if (k == 0) {

@@ -365,9 +365,6 @@ template <class R> PoissonArgs<R> poisson_args(wf_ctx *c, const void *y1, const 
     a.fx = c->fx;
     a.fy = c->fy;
     a.h1 = c->h1;
-    a.inv_dx = 1.0 / c->ph.dx;
-    a.inv_dy = 1.0 / c->ph.dy;
-    a.rho_dt = c->ph.rho_inf / c->ph.dt;
     return a;
 }
 

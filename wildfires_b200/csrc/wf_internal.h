@@ -152,8 +152,6 @@ struct PoissonArgs {
     const double *ky2;      // [Ny-1] ky^2
     FftDesc fx, fy;         // x: length Nx-1, y: length Ny-1
     int h1;                 // (Ny-1)/2 + 1
-    double inv_dx, inv_dy;  // 1/dx, 1/dy (FP32 stencil path source)
-    double rho_dt;          // rho_inf / dt (FP32 stencil path source)
 };
 // zt: tridiagonal constants per k (layout documented at k_p_tridiag).
 // ev (optional): one event recorded after each of the 5 kernels, for profiling.
