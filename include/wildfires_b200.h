@@ -135,6 +135,19 @@ wf_status wf_phi(wf_ctx *ctx, const double *R_old, double *R_new);
  * Returns the number of solves in *iters (may be NULL). */
 wf_status wf_pressure(wf_ctx *ctx, const double *y_np1, const double *y_n, double *pr, int *iters);
 
+/* The RK stages of one step without the pressure solve and the projection
+ * (RK4 / RK2 / euler, solver.cu:59-93): y_np1 from y_n on host buffers. */
+wf_status wf_rk(wf_ctx *ctx, const double *y_n, double *y_np1);
+
+/* What solve_pressure_iterative reports after the last wf_pressure or step
+ * that waited on the host (pressure.cu:596-597): the max-norm change of the
+ * last iterate and the iteration count in the reference's convention (the
+ * index of the converged iterate, or pressure_solver_iter). */
+wf_status wf_pressure_report(const wf_ctx *ctx, double *error, int *max_iter);
+
+/* The operator-level entries above use the context's state buffers as
+ * scratch: after them, upload a state before calling wf_step again. */
+
 /* Number of kernel launches one wf_step(ctx, 1) enqueues. */
 int wf_launches_per_step(const wf_ctx *ctx);
 

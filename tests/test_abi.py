@@ -21,6 +21,24 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(L, name), name
 
 
+def test_dropin_archive_defines_every_declared_entry_point():
+    """include/wf_dropin.h: the reference's C++ entry points, with the
+    reference's parameter types, defined by libwildfires_b200_dropin.a."""
+    import subprocess
+    header = open(os.path.join(ROOT, "include", "wf_dropin.h")).read()
+    header = re.sub(r"/\*.*?\*/", "", header, flags=re.S)
+    declared = set(re.findall(r"^void\s+(\w+)\s*\(", header, flags=re.M))
+    assert declared == {"create_y_0", "solve_PDE", "Phi", "euler", "RK2", "RK4", "solve_pressure",
+                        "solve_pressure_iterative"}
+    archive = os.path.join(ROOT, "wildfires_b200", "libwildfires_b200_dropin.a")
+    out = subprocess.run(["nm", "-C", "--defined-only", archive], capture_output=True, text=True, check=True).stdout
+    defined = {m.group(1): m.group(2) for m in re.finditer(r" T (\w+)\(([^)]*)\)", out)}
+    for name in declared:
+        assert name in defined, name
+        assert "_parameters" in defined[name], (name, defined[name])   # takes the record by value
+    assert defined["solve_PDE"] == "double*, double*, _parameters"
+
+
 def test_parser_defaults_and_override(params_from_text):
     P = params_from_text("Nx = 8\nNy = 9\nNz = 10\nNt = 4\nx_max = 7\ny_max = 8\nz_max = 9\nt_max = 1\n"
                          "C_s = 0.1\nC_s = 0.3\nunknown_key = 5\nT_min = 290\nmethod = RK2\n")

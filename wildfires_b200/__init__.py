@@ -163,6 +163,20 @@ class Solver:
         check(lib().wf_phi(self._h, _ptr(R_old), _ptr(out)), "wf_phi")
         return out
 
+    def rk(self, y_n):
+        """The RK stages of one step (no pressure solve, no projection)."""
+        y_n = np.ascontiguousarray(y_n, dtype=np.float64)
+        out = np.empty(self.S)
+        check(lib().wf_rk(self._h, _ptr(y_n), _ptr(out)), "wf_rk")
+        return out
+
+    def pressure_report(self):
+        """(error, max_iter) as the reference's iterative pressure solve reports them."""
+        e = C.c_double()
+        m = C.c_int()
+        check(lib().wf_pressure_report(self._h, C.byref(e), C.byref(m)), "wf_pressure_report")
+        return e.value, m.value
+
     def pressure(self, y_np1, y_n, p):
         a = np.ascontiguousarray(y_np1, dtype=np.float64)
         b = np.ascontiguousarray(y_n, dtype=np.float64)

@@ -22,7 +22,7 @@ EXPORTS = [
     "wf_download_state", "wf_step", "wf_synchronize", "wf_time", "wf_diagnostics",
     "wf_device_state", "wf_stream", "wf_phi", "wf_pressure", "wf_launches_per_step",
     "wf_status_string", "wf_last_error", "wf_profile_phases", "wf_phase_name",
-    "wf_pressure_noalloc",
+    "wf_pressure_noalloc", "wf_rk", "wf_pressure_report",
 ]
 
 
@@ -85,6 +85,8 @@ def lib():
         "wf_profile_phases": (C.c_int, [vp, C.c_int, dp, C.POINTER(C.c_int)]),
         "wf_phase_name": (C.c_char_p, [C.c_int]),
         "wf_pressure_noalloc": (C.c_int, [P, vp, vp, vp]),
+        "wf_rk": (C.c_int, [vp, dp, dp]),
+        "wf_pressure_report": (C.c_int, [vp, dp, C.POINTER(C.c_int)]),
         "wf_last_error": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():

@@ -14,6 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libwildfires_b200.so")
+DROPIN = os.path.join(HERE, "libwildfires_b200_dropin.a")
 NVCC = os.environ.get("WF_NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "-I" + os.path.join(ROOT, "include"),
@@ -60,7 +61,32 @@ def build(verbose=False, force=False):
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("link failed")
+    _build_dropin(verbose, force)
     return LIB
+
+
+def _build_dropin(verbose=False, force=False):
+    """libwildfires_b200_dropin.a: the reference's C++ solver entry points
+    (include/wf_dropin.h) for programs that link the reference's other objects."""
+    src = os.path.join(HERE, "dropin", "dropin.cu")
+    obj = os.path.join(BUILD, "dropin.o")
+    hdr_mtime = max(os.path.getmtime(h) for h in _headers())
+    if not force and os.path.exists(DROPIN) and os.path.getmtime(DROPIN) >= max(os.path.getmtime(src), hdr_mtime):
+        return DROPIN
+    cmd = [NVCC] + COMMON + ["-c", src, "-o", obj]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed on %s" % src)
+    if os.path.exists(DROPIN):
+        os.remove(DROPIN)
+    r = subprocess.run(["ar", "rcs", DROPIN, obj], capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("ar failed")
+    return DROPIN
 
 
 if __name__ == "__main__":

@@ -144,6 +144,8 @@ struct wf_ctx {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int launches = 0;
     int last_iters = 0;
+    double last_err = 0.0;   // max |p_m - p_{m-1}| of the last iteration (variable density)
+    int last_ref_iter = 0;   // iteration count as solve_pressure_iterative reports it
 };
 
 namespace wfs {
@@ -413,18 +415,25 @@ template <class R> wf_status enqueue_pressure(wf_ctx *c, const void *y1, const v
     const int maxit = c->P.pressure_solver_iter;
     const bool use_tol = !fixed_only && c->P.pressure_solver_tol >= 0;
     int m = 0;
+    bool converged = false;
+    double h = 0;
     for (m = 0; m < maxit; m++) {
-        if (use_tol) WF_TRY_CUDA(cudaMemcpyAsync(c->p_prev, c->p, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, s));
+        // the change of the last iterate is measured whenever the host waits anyway
+        const bool measure = use_tol || (!fixed_only && m == maxit - 1);
+        if (measure) WF_TRY_CUDA(cudaMemcpyAsync(c->p_prev, c->p, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, s));
         WF_TRY_CUDA(launch_poisson_impl<R>(a, c->d_zt, s));
-        if (use_tol) {
+        if (measure) {
             WF_TRY_CUDA(launch_maxdiff(c->p, c->p_prev, c->N, c->red, s));
-            double h = 0;
             WF_TRY_CUDA(cudaMemcpyAsync(&h, c->red, sizeof(double), cudaMemcpyDeviceToHost, s));
             WF_TRY_CUDA(cudaStreamSynchronize(s));
-            if (h <= c->P.pressure_solver_tol) { m++; break; }
+            if (use_tol && h <= c->P.pressure_solver_tol) { converged = true; break; }
         }
     }
-    if (iters) *iters = m;
+    if (!fixed_only) {
+        c->last_err = h;
+        c->last_ref_iter = converged ? m : maxit;   // pressure.cu:564-600 reports the breaking index
+    }
+    if (iters) *iters = converged ? m + 1 : m;
     return WF_OK;
 }
 
@@ -907,6 +916,27 @@ wf_status wf_pressure(wf_ctx *c, const double *y_np1, const double *y_n, double 
     WF_TRY_CUDA(cudaMemcpyAsync(pr, c->p, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
     WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
     if (iters) *iters = it;
+    drop_graphs(c);
+    return WF_OK;
+}
+
+wf_status wf_pressure_report(const wf_ctx *c, double *error, int *max_iter)
+{
+    if (!c) { set_error("wf_pressure_report: null context"); return WF_ERR_ARG; }
+    if (error) *error = c->last_err;
+    if (max_iter) *max_iter = c->last_ref_iter;
+    return WF_OK;
+}
+
+wf_status wf_rk(wf_ctx *c, const double *y_n, double *y_np1)
+{
+    if (!c || !y_n || !y_np1) { set_error("wf_rk: null argument"); return WF_ERR_ARG; }
+    void *yn = c->ybuf[1 - c->cur], *y1 = c->ybuf[c->cur];
+    wf_status st = put_state(c, yn, y_n);
+    if (st) return st;
+    st = (c->prec == WF_FP64) ? enqueue_stages<double>(c, yn, y1) : enqueue_stages<float>(c, yn, y1);
+    if (st) return st;
+    if ((st = get_state(c, y_np1, y1))) return st;
     drop_graphs(c);
     return WF_OK;
 }
