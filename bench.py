@@ -50,6 +50,21 @@ def parse_args():
     return ap.parse_args()
 
 
+def build_params_only(name, **kw):
+    """The parsed parameter record of a workload (terrain applied), without fields."""
+    from wildfires_b200 import configs, read_parameters
+    case = configs.CASES[name](**kw)
+    d = tempfile.mkdtemp(prefix="wf_bench_")
+    path = os.path.join(d, "parameters.txt")
+    with open(path, "w") as f:
+        f.write(configs.param_text(case.params))
+    P = read_parameters(path)
+    topo = case.topography(P)
+    if topo is not None:
+        P.set_topography(topo)
+    return P
+
+
 def build_case(name, **kw):
     from wildfires_b200 import configs, read_parameters
     case = configs.CASES[name](**kw)
@@ -63,6 +78,15 @@ def build_case(name, **kw):
         P.set_topography(topo)
     y0, p0 = case.fields(P)
     return case, P, y0, p0
+
+
+def workload_config(name, P, prec, world):
+    """The `config` object both arms print for the same workload."""
+    r = P.rec
+    S = 4 * r.Nx * r.Ny * r.Nz + r.Nx * r.Ny * r.Nz_Y_max
+    return {"workload": workload_name(name, P, prec), "grid": [r.Nx, r.Ny, r.Nz], "cells": r.Nx * r.Ny * r.Nz,
+            "dt": r.dt, "l2": "inputs larger than L2 (state %.0f MB), no flush" % (S * (4 if prec == "fp32" else 8) / 1e6),
+            "parallelism": "replicas x%d" % world}
 
 
 def workload_name(name, P, prec):
@@ -377,10 +401,7 @@ def run_ours(args):
             "warmup": W, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64" if args.precision == "fp32" else "f64",
             "data": "synthetic (seeded fields; no dataset exists for this model)",
-            "config": {"workload": workload_name(args.config, P, args.precision),
-                       "grid": [r.Nx, r.Ny, r.Nz], "cells": cells, "dt": r.dt,
-                       "l2": "inputs larger than L2 (state %.0f MB), no flush" % (sol.S * (4 if args.precision == "fp32" else 8) / 1e6),
-                       "parallelism": "replicas x%d" % world},
+            "config": workload_config(args.config, P, args.precision, world),
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roof,
             "kernels": kernels, "cpu_baseline": cpu, "clocks": clk, "fp64": fp64,
         }
@@ -406,7 +427,8 @@ def run_reference(args):
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(cpu["seconds"] / cpu["steps"] * 1e3, 2), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded fields)",
-           "config": {"workload": "%s (reference CPU path, bounded sample)" % args.config},
+           "config": workload_config(args.config, build_params_only(args.config), args.precision,
+                                     int(os.environ.get("WORLD_SIZE", "1"))),
            "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
            "e2e": {"value": round(cpu["value"], 4), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)

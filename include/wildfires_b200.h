@@ -124,6 +124,25 @@ wf_status wf_device_state(wf_ctx *ctx, void **y, double **pr);
 /* The CUDA stream (cudaStream_t) the context enqueues on. */
 void *wf_stream(wf_ctx *ctx);
 
+/* ---- ensembles of independent members ------------------------------------ */
+
+/* An ensemble steps independent members (their own grids, terrain, wind,
+ * ignition, fuel) together: each ensemble step is one CUDA graph whose
+ * branches are the members' steps, run concurrently on the GPU.  There is no
+ * reference counterpart (the reference runs one scenario per process). */
+typedef struct wf_ensemble wf_ensemble;
+
+/* Create one member context per record of members[0 .. n_members). */
+wf_status wf_ensemble_create(const Parameters *members, int n_members, int precision, wf_ensemble **out);
+wf_status wf_ensemble_destroy(wf_ensemble *e);
+int wf_ensemble_size(const wf_ensemble *e);
+/* Member i as a context: upload, download and diagnose it with the wf_ctx
+ * calls; owned by the ensemble (do not destroy it). */
+wf_ctx *wf_ensemble_member(wf_ensemble *e, int i);
+/* Advance every member nsteps steps. */
+wf_status wf_ensemble_step(wf_ensemble *e, int nsteps);
+wf_status wf_ensemble_synchronize(wf_ensemble *e);
+
 /* ---- operator-level entry points (used by the parity tests) ------------- */
 
 /* One right-hand-side evaluation R_new = Phi(R_old) on host buffers (packed

@@ -18,7 +18,7 @@ import numpy as np
 from ._abi import WF_FP32_STENCIL, WF_FP64, WfDiag, WfError, check, lib
 from ._params import Parameters
 
-__all__ = ["Params", "Solver", "read_parameters", "WfError", "Parameters"]
+__all__ = ["Params", "Solver", "Ensemble", "read_parameters", "WfError", "Parameters"]
 
 _dp = C.POINTER(C.c_double)
 
@@ -204,3 +204,64 @@ class Solver:
         n = (C.c_int * WF_NPHASES)()
         check(lib().wf_profile_phases(self._h, int(nsteps), ms, n), "wf_profile_phases")
         return {lib().wf_phase_name(q).decode(): (ms[q], n[q]) for q in range(WF_NPHASES)}
+
+
+class _Member(Solver):
+    """A member context owned by an Ensemble (not destroyed on its own)."""
+
+    def __init__(self, params, handle, precision):
+        self.params = params
+        self.precision = precision
+        self._h = handle
+        r = params.rec
+        self.N = r.Nx * r.Ny * r.Nz
+        self.S = params.state_size
+
+    def close(self):
+        self._h = None
+
+
+class Ensemble:
+    """Independent members stepped together (one CUDA graph per ensemble step,
+    one concurrent branch per member)."""
+
+    def __init__(self, params_list, precision="fp32"):
+        prec = {"fp64": WF_FP64, "fp32": WF_FP32_STENCIL}[precision]
+        self.params = list(params_list)
+        recs = (Parameters * len(self.params))(*[p.rec for p in self.params])
+        h = C.c_void_p()
+        check(lib().wf_ensemble_create(recs, len(self.params), prec, C.byref(h)), "wf_ensemble_create")
+        self._h = h
+        self.members = [_Member(p, C.c_void_p(lib().wf_ensemble_member(h, i)), precision)
+                        for i, p in enumerate(self.params)]
+
+    def __len__(self):
+        return len(self.members)
+
+    def __getitem__(self, i):
+        return self.members[i]
+
+    def step(self, n=1):
+        check(lib().wf_ensemble_step(self._h, int(n)), "wf_ensemble_step")
+
+    def synchronize(self):
+        check(lib().wf_ensemble_synchronize(self._h), "wf_ensemble_synchronize")
+
+    def close(self):
+        if self._h:
+            lib().wf_ensemble_destroy(self._h)
+            self._h = None
+            for m in self.members:
+                m.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -23,6 +23,8 @@ EXPORTS = [
     "wf_device_state", "wf_stream", "wf_phi", "wf_pressure", "wf_launches_per_step",
     "wf_status_string", "wf_last_error", "wf_profile_phases", "wf_phase_name",
     "wf_pressure_noalloc", "wf_rk", "wf_pressure_report",
+    "wf_ensemble_create", "wf_ensemble_destroy", "wf_ensemble_size", "wf_ensemble_member",
+    "wf_ensemble_step", "wf_ensemble_synchronize",
 ]
 
 
@@ -86,6 +88,12 @@ def lib():
         "wf_phase_name": (C.c_char_p, [C.c_int]),
         "wf_pressure_noalloc": (C.c_int, [P, vp, vp, vp]),
         "wf_rk": (C.c_int, [vp, dp, dp]),
+        "wf_ensemble_create": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(vp)]),
+        "wf_ensemble_destroy": (C.c_int, [vp]),
+        "wf_ensemble_size": (C.c_int, [vp]),
+        "wf_ensemble_member": (vp, [vp, C.c_int]),
+        "wf_ensemble_step": (C.c_int, [vp, C.c_int]),
+        "wf_ensemble_synchronize": (C.c_int, [vp]),
         "wf_pressure_report": (C.c_int, [vp, dp, C.POINTER(C.c_int)]),
         "wf_last_error": (C.c_char_p, []),
     }

@@ -234,7 +234,91 @@ def hills8(Nx=512, Ny=512, Nz=128, Nt=1000, dt=0.003, seed=1234, L=800.0, H=60.0
     return Case("hills8", params, fields, topography)
 
 
+# ---- ensemble members (uneven grids, varied wind, terrain, ignition, fuel) ----------
+ENSEMBLE_SIZES = (96, 128, 160, 192, 256)
+
+
+def scenario(Nx, Ny, Nz=64, Nt=300, dt=0.005, seed=0, dx=1.5625, z_max=19.6875, jitter=0.0, **kw):
+    """One ensemble member: Nx x Ny x Nz with dx = dy = 1.5625 m and dz =
+    0.3125 m, 0-4 seeded Gaussian hills (1-4 m), log wind of u_r ~ U(2, 10) m/s
+    at a random direction, 1-3 hot spots (+500 K, sigma 3 m) and per-column fuel
+    Y ~ U(0.5, 1)."""
+    Lx, Ly = (Nx - 1) * dx, (Ny - 1) * dx
+    params = base_params(Nx, Ny, Nz, Nt, Lx, Ly, z_max, Nt * dt, **kw)
+    rng0 = np.random.default_rng(seed)
+    nh = int(rng0.integers(0, 5))
+    hills = [(rng0.uniform(0, Lx), rng0.uniform(0, Ly), rng0.uniform(1, 4), rng0.uniform(10, 40)) for _ in range(nh)]
+    u_r = rng0.uniform(2, 10)
+    theta = rng0.uniform(0, 2 * math.pi)
+    spots = rng0.uniform(0, 1, size=(int(rng0.integers(1, 4)), 2))
+    fuel_seed = int(rng0.integers(1 << 30))
+
+    def topography(P):
+        if not hills:
+            return None
+        x, y, _ = _grid(P)
+        X, Yg = np.meshgrid(x, y, indexing="ij")
+        h = np.zeros_like(X)
+        for (cx, cy, hh, wd) in hills:
+            ddx = (X - cx + Lx / 2) % Lx - Lx / 2
+            ddy = (Yg - cy + Ly / 2) % Ly - Ly / 2
+            h += hh * np.exp(-(ddx ** 2 + ddy ** 2) / (2 * wd ** 2))
+        return h
+
+    def fields(P):
+        x, y, z = _grid(P)
+        topo = _topo_array(P)
+        X, Yg, Z = np.meshgrid(x, y, z, indexing="ij")
+        hgt = Z - topo[:, :, None]
+        speed = log_wind(hgt, u_r)
+        u = speed * math.cos(theta)
+        v = speed * math.sin(theta)
+        w = np.zeros_like(u)
+        heat = np.zeros_like(u)
+        for (a, b) in spots:
+            cx, cy = a * Lx, b * Ly
+            ddx = (X - cx + Lx / 2) % Lx - Lx / 2
+            ddy = (Yg - cy + Ly / 2) % Ly - Ly / 2
+            heat = np.maximum(heat, np.where(hgt < 1.0, 500.0 * np.exp(-(ddx ** 2 + ddy ** 2) / (2 * 3.0 ** 2)), 0.0))
+        T = T_AMB + heat
+        frng = np.random.default_rng(fuel_seed)
+        Ycol = frng.uniform(0.5, 1.0, size=(P.rec.Nx, P.rec.Ny))
+        Y = np.broadcast_to(Ycol[:, :, None], u.shape).copy()
+        rng = np.random.default_rng(seed + 1)
+        return _finish(P, u, v, w, T, Y, rng, jitter)
+
+    return Case("scenario", params, fields, topography)
+
+
+def ensemble(n=64, seed=2024, sizes=ENSEMBLE_SIZES, **kw):
+    """n members with Nx, Ny drawn from `sizes` (seeded)."""
+    rng = np.random.default_rng(seed)
+    return [scenario(int(rng.choice(sizes)), int(rng.choice(sizes)), seed=int(rng.integers(1 << 30)), **kw)
+            for _ in range(n)]
+
+
 CASES = {"flat": flat, "hill": hill, "hills8": hills8}
+
+
+def materialize(case):
+    """Parse the case's parameters with the library, apply its terrain and build
+    its initial state: returns (P, y0, p0)."""
+    import shutil
+    import tempfile
+    from . import read_parameters
+    d = tempfile.mkdtemp(prefix="wf_case_")
+    try:
+        path = os.path.join(d, "parameters.txt")
+        with open(path, "w") as f:
+            f.write(param_text(case.params))
+        P = read_parameters(path)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    topo = case.topography(P)
+    if topo is not None:
+        P.set_topography(topo)
+    y0, p0 = case.fields(P)
+    return P, y0, p0
 
 
 def write_case(case, directory, P=None, input_subdir="in/"):

@@ -920,6 +920,146 @@ wf_status wf_pressure(wf_ctx *c, const double *y_np1, const double *y_n, double 
     return WF_OK;
 }
 
+// ---- ensemble: independent members stepped together -----------------------
+// One CUDA graph per ensemble step holds every member's step as a branch of
+// its own (the members' streams fork from and join back to one stream), so the
+// GPU runs the members' kernels concurrently and one graph launch replaces
+// 18 launches per member.  Members whose step is not static (ignition source
+// active, host-checked pressure tolerance) are enqueued eagerly on their own
+// streams instead.
+}  // extern "C"
+
+struct wf_ensemble {
+    std::vector<wf_ctx *> m;
+    cudaStream_t master = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int parity = 0;
+};
+
+namespace wfs {
+
+void ensemble_drop_graphs(wf_ensemble *e)
+{
+    for (int q = 0; q < 2; q++)
+        if (e->graph[q]) {
+            cudaGraphExecDestroy(e->graph[q]);
+            e->graph[q] = nullptr;
+        }
+}
+
+wf_status ensemble_enqueue(wf_ensemble *e, bool fixed_only)
+{
+    WF_TRY_CUDA(cudaEventRecord(e->fork, e->master));
+    for (size_t i = 0; i < e->m.size(); i++) {
+        wf_ctx *c = e->m[i];
+        WF_TRY_CUDA(cudaStreamWaitEvent(c->stream, e->fork, 0));
+        wf_status st = enqueue_step_any(c, c->cur, c->n + 1, fixed_only);
+        if (st) return st;
+        WF_TRY_CUDA(cudaEventRecord(e->join[i], c->stream));
+        WF_TRY_CUDA(cudaStreamWaitEvent(e->master, e->join[i], 0));
+    }
+    return WF_OK;
+}
+
+}  // namespace wfs
+
+extern "C" {
+
+wf_status wf_ensemble_create(const Parameters *members, int n_members, int precision, wf_ensemble **out)
+{
+    if (!members || n_members < 1 || !out) { set_error("wf_ensemble_create: invalid argument"); return WF_ERR_ARG; }
+    *out = nullptr;
+    wf_ensemble *e = new wf_ensemble();
+    auto fail = [&](wf_status st) {
+        wf_ensemble_destroy(e);
+        return st;
+    };
+    if (cudaStreamCreateWithFlags(&e->master, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) {
+        set_error("wf_ensemble_create: stream or event creation failed");
+        return fail(WF_ERR_CUDA);
+    }
+    for (int i = 0; i < n_members; i++) {
+        wf_ctx *c = nullptr;
+        wf_status st = wf_create(&members[i], precision, &c);
+        if (st) return fail(st);
+        e->m.push_back(c);
+        cudaEvent_t ev;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            set_error("wf_ensemble_create: event creation failed");
+            return fail(WF_ERR_CUDA);
+        }
+        e->join.push_back(ev);
+    }
+    *out = e;
+    return WF_OK;
+}
+
+wf_status wf_ensemble_destroy(wf_ensemble *e)
+{
+    if (!e) return WF_OK;
+    if (e->master) cudaStreamSynchronize(e->master);
+    ensemble_drop_graphs(e);
+    for (wf_ctx *c : e->m) wf_destroy(c);
+    for (cudaEvent_t ev : e->join) cudaEventDestroy(ev);
+    if (e->fork) cudaEventDestroy(e->fork);
+    if (e->master) cudaStreamDestroy(e->master);
+    delete e;
+    return WF_OK;
+}
+
+int wf_ensemble_size(const wf_ensemble *e) { return e ? (int)e->m.size() : 0; }
+
+wf_ctx *wf_ensemble_member(wf_ensemble *e, int i)
+{
+    return (e && i >= 0 && i < (int)e->m.size()) ? e->m[i] : nullptr;
+}
+
+wf_status wf_ensemble_step(wf_ensemble *e, int nsteps)
+{
+    if (!e || nsteps < 0) { set_error("wf_ensemble_step: invalid argument"); return WF_ERR_ARG; }
+    for (int q = 0; q < nsteps; q++) {
+        bool same = true, fixed = true;
+        for (wf_ctx *c : e->m) {
+            same = same && c->cur == e->m[0]->cur;
+            fixed = fixed && step_is_static(c, c->n + 1);
+        }
+        if (same && fixed) {
+            cudaGraphExec_t &ge = e->graph[e->m[0]->cur];
+            if (!ge) {
+                cudaGraph_t gph;
+                WF_TRY_CUDA(cudaStreamBeginCapture(e->master, cudaStreamCaptureModeThreadLocal));
+                wf_status st = ensemble_enqueue(e, true);
+                cudaError_t err = cudaStreamEndCapture(e->master, &gph);
+                if (st) return st;
+                if (err != cudaSuccess) { set_error("wf_ensemble_step: capture failed: %s", cudaGetErrorString(err)); return WF_ERR_CUDA; }
+                err = cudaGraphInstantiate(&ge, gph, 0);
+                cudaGraphDestroy(gph);
+                if (err != cudaSuccess) { set_error("wf_ensemble_step: instantiate failed: %s", cudaGetErrorString(err)); return WF_ERR_CUDA; }
+            }
+            WF_TRY_CUDA(cudaGraphLaunch(ge, e->master));
+        } else {
+            wf_status st = ensemble_enqueue(e, false);
+            if (st) return st;
+        }
+        for (wf_ctx *c : e->m) {
+            c->cur = 1 - c->cur;
+            c->n += 1;
+        }
+    }
+    return WF_OK;
+}
+
+wf_status wf_ensemble_synchronize(wf_ensemble *e)
+{
+    if (!e) return WF_ERR_ARG;
+    WF_TRY_CUDA(cudaStreamSynchronize(e->master));
+    for (wf_ctx *c : e->m) WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+    return WF_OK;
+}
+
 wf_status wf_pressure_report(const wf_ctx *c, double *error, int *max_iter)
 {
     if (!c) { set_error("wf_pressure_report: null context"); return WF_ERR_ARG; }
