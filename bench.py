@@ -47,6 +47,9 @@ def parse_args():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--ensemble", type=int, default=0, metavar="M",
+                    help="instead: M seeded members of uneven grids (Nx, Ny in 96..256, Nz = 64), "
+                         "one graph launch per ensemble step against the members stepped one by one")
     return ap.parse_args()
 
 
@@ -435,8 +438,58 @@ def run_reference(args):
     return out
 
 
+def run_ensemble(args):
+    """Ensemble throughput: all members per step in one graph launch (concurrent
+    member branches) against the same members stepped one after another, each
+    step of each member a graph launch followed by a wait."""
+    import torch
+    from wildfires_b200 import Ensemble, configs
+    torch.cuda.set_device(0)
+    members = configs.ensemble(args.ensemble, Nt=300)
+    built = [configs.materialize(c) for c in members]
+    cells = sum(P.rec.Nx * P.rec.Ny * P.rec.Nz for P, _, _ in built)
+    with Ensemble([b[0] for b in built], args.precision) as ens:
+        for i, (P, y0, p0) in enumerate(built):
+            ens[i].upload(y0, p0)
+        ens.step(args.warmup)
+        for m in ens.members:
+            m.step(args.warmup)
+        ens.synchronize()
+        clk = ClockSampler(0)
+        clk.start()
+        t0 = time.perf_counter()
+        ens.step(args.steps)
+        ens.synchronize()
+        t_ens = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            for m in ens.members:
+                m.step(1)
+                m.synchronize()
+        t_ser = time.perf_counter() - t0
+        clocks = clk.stop()
+    v_ens = cells * args.steps / t_ens / 1e6
+    v_ser = cells * args.steps / t_ser / 1e6
+    sizes = sorted({(P.rec.Nx, P.rec.Ny) for P, _, _ in built})
+    out = {"metric": "ensemble Mcell-steps/s", "value": round(v_ens, 2), "unit": "Mcell-steps/s", "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_ens / args.steps * 1e3, 3),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32+f64" if args.precision == "fp32" else "f64", "data": "synthetic (seeded members)",
+           "config": {"workload": "ensemble of %d members, Nx, Ny in {96..256}, Nz = 64, %s" % (len(built), args.precision),
+                      "cells": cells, "grids": len(sizes)},
+           "serial": {"value": round(v_ser, 2), "ms_per_step": round(t_ser / args.steps * 1e3, 3),
+                      "how": "each member: one graph launch per step, then a wait, members one after another"},
+           "speedup_over_serial": round(t_ser / t_ens, 3),
+           "timing": "host wall clock around a device synchronisation (one GPU)", "clocks": clocks}
+    print(json.dumps(out), flush=True)
+    return out
+
+
 def main():
     args = parse_args()
+    if args.ensemble:
+        run_ensemble(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

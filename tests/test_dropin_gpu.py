@@ -2,8 +2,15 @@
 functions.o, input.o, output.o, logs.o and utils.o linked against the B200
 solver's C++ entry points (include/wf_dropin.h) instead of the reference's
 solver, pde, turbulence and pressure objects (oracle/Makefile target
-`dropin`).  Both programs run the same parameter file and inputs; the fields
-they save must agree to the FP64 gate (1e-10 relative, per field).
+`dropin`), run on a parameter file and input fields the way the reference's
+program is run.
+
+Gates: (1) the fields it saves match the reference's own solver built for the
+host (oracle/_ref/ref_host, deterministic) to 1e-12 per field; (2) they are as
+close to the reference's GPU program on the same inputs as that host build is
+(within 1.5x).  The reference's GPU build is not reproducible run to run on
+these grids (two runs of the same binary on the same inputs differ by up to
+1e-2 in w after 10 steps), so it cannot be the 1e-12 anchor.
 """
 import glob
 import os
@@ -12,6 +19,7 @@ import subprocess
 import numpy as np
 import pytest
 
+import ref_runner
 from conftest import field_errors
 
 pytestmark = pytest.mark.gpu
@@ -41,21 +49,26 @@ def _fields(save, P, n):
     return y, np.fromfile(os.path.join(save, "p.bin.%d" % n))
 
 
-@pytest.mark.skipif(not (os.path.exists(DROPIN) and os.path.exists(REFMAIN)),
+@pytest.mark.skipif(not (os.path.exists(DROPIN) and os.path.exists(REFMAIN) and ref_runner.available("host")),
                     reason="reference objects were not available when oracle/Makefile ran")
 def test_reference_main_links_and_matches(tmp_path, params_from_text):
     from wildfires_b200 import configs
-    case = configs.hill(Nx=33, Ny=33, Nz=16, Nt=10, NT=5, L=100.0, H=20.0, jitter=0.2, seed=3)
+    case = configs.hill(Nx=33, Ny=33, Nz=16, Nt=10, NT=10, L=100.0, H=20.0, jitter=0.2, seed=3)
     P = params_from_text(configs.param_text(case.params))
     ours, _ = _run(DROPIN, case, tmp_path / "dropin")
-    ref, _ = _run(REFMAIN, case, tmp_path / "reference")
-    for n in (1, 2):   # saves at steps 5 and 10
-        y_o, p_o = _fields(ours, P, n)
-        y_r, p_r = _fields(ref, P, n)
-        errs = field_errors(P, y_o, y_r)
-        bad = {f: e for f, e in errs.items() if e[0] > 1e-10 or e[1] > 1e-10}
-        assert not bad, (n, bad)
-        assert np.max(np.abs(p_o - p_r)) <= 1e-10 * np.max(np.abs(p_r))
+    ref1, _ = _run(REFMAIN, case, tmp_path / "reference1")
+    ref2, _ = _run(REFMAIN, case, tmp_path / "reference2")
+    y_o, p_o = _fields(ours, P, 1)
+    host = ref_runner.run(case, "step", flavour="host")
+    for f, (linf, l2) in field_errors(P, y_o, host["y"]).items():
+        assert linf <= 1e-12 and l2 <= 1e-12, (f, linf, l2)
+    assert np.max(np.abs(p_o - host["p"])) <= 1e-12 * np.max(np.abs(host["p"]))
+    y1, _ = _fields(ref1, P, 1)
+    y2, _ = _fields(ref2, P, 1)
+    spread = field_errors(P, y1, y2)
+    host_gap = field_errors(P, host["y"], y1)
+    for f, (linf, l2) in field_errors(P, y_o, y1).items():
+        assert l2 <= 1.5 * host_gap[f][1] + 1e-12, (f, l2, host_gap[f], spread[f])
     # the drop-in reported through the reference's own logging
     log = open(os.path.join(ours, "log.txt")).read()
     assert "Solver time" in log
