@@ -439,15 +439,39 @@ def run_reference(args):
 
 
 def run_ensemble(args):
-    """Ensemble throughput: all members per step in one graph launch (concurrent
-    member branches) against the same members stepped one after another, each
-    step of each member a graph launch followed by a wait."""
+    """Ensemble throughput.  --ensemble M: M seeded members per GPU (weak
+    scaling), partitioned across ranks by cells x steps with no collective
+    while stepping.  On each rank: all of its members per step in one graph
+    launch (concurrent member branches), then the same members stepped one
+    after another (a graph launch and a wait each) for comparison."""
     import torch
+    import torch.distributed as dist
     from wildfires_b200 import Ensemble, configs
-    torch.cuda.set_device(0)
-    members = configs.ensemble(args.ensemble, Nt=300)
-    built = [configs.materialize(c) for c in members]
-    cells = sum(P.rec.Nx * P.rec.Ny * P.rec.Nz for P, _, _ in built)
+    from wildfires_b200.sharding import partition
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    members = configs.ensemble(args.ensemble * world, Nt=300)
+    costs = [m.params["Nx"] * m.params["Ny"] * m.params["Nz"] for m in members]
+    mine = partition(costs, world)[rank]
+    built = [configs.materialize(members[i]) for i in mine]
+    cells_local = sum(P.rec.Nx * P.rec.Ny * P.rec.Nz for P, _, _ in built)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     with Ensemble([b[0] for b in built], args.precision) as ens:
         for i, (P, y0, p0) in enumerate(built):
             ens[i].upload(y0, p0)
@@ -455,32 +479,44 @@ def run_ensemble(args):
         for m in ens.members:
             m.step(args.warmup)
         ens.synchronize()
-        clk = ClockSampler(0)
-        clk.start()
+        clk = ClockSampler(local) if rank == 0 else None
+        if clk:
+            clk.start()
+        barrier()
         t0 = time.perf_counter()
         ens.step(args.steps)
         ens.synchronize()
-        t_ens = time.perf_counter() - t0
+        t_ens = max_over_ranks(time.perf_counter() - t0)
+        barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
             for m in ens.members:
                 m.step(1)
                 m.synchronize()
-        t_ser = time.perf_counter() - t0
-        clocks = clk.stop()
+        t_ser = max_over_ranks(time.perf_counter() - t0)
+        clocks = clk.stop() if clk else None
+    cells = cells_local
+    if world > 1:
+        t = torch.tensor([float(cells_local)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        cells = int(t.item())
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
     v_ens = cells * args.steps / t_ens / 1e6
     v_ser = cells * args.steps / t_ser / 1e6
-    sizes = sorted({(P.rec.Nx, P.rec.Ny) for P, _, _ in built})
-    out = {"metric": "ensemble Mcell-steps/s", "value": round(v_ens, 2), "unit": "Mcell-steps/s", "n_gpus": 1,
+    out = {"metric": "ensemble Mcell-steps/s", "value": round(v_ens, 2), "unit": "Mcell-steps/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_ens / args.steps * 1e3, 3),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f32+f64" if args.precision == "fp32" else "f64", "data": "synthetic (seeded members)",
-           "config": {"workload": "ensemble of %d members, Nx, Ny in {96..256}, Nz = 64, %s" % (len(built), args.precision),
-                      "cells": cells, "grids": len(sizes)},
+           "config": {"workload": "ensemble of %d members per GPU, Nx, Ny in {96..256}, Nz = 64, %s"
+                                  % (args.ensemble, args.precision),
+                      "members": len(members), "cells": cells,
+                      "parallelism": "members partitioned over %d ranks, no collective while stepping" % world},
            "serial": {"value": round(v_ser, 2), "ms_per_step": round(t_ser / args.steps * 1e3, 3),
                       "how": "each member: one graph launch per step, then a wait, members one after another"},
            "speedup_over_serial": round(t_ser / t_ens, 3),
-           "timing": "host wall clock around a device synchronisation (one GPU)", "clocks": clocks}
+           "timing": "host wall clock around a device synchronisation, max over ranks", "clocks": clocks}
     print(json.dumps(out), flush=True)
     return out
 
