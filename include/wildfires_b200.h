@@ -124,6 +124,33 @@ wf_status wf_device_state(wf_ctx *ctx, void **y, double **pr);
 /* The CUDA stream (cudaStream_t) the context enqueues on. */
 void *wf_stream(wf_ctx *ctx);
 
+/* ---- learned subgrid closure (no reference counterpart) ------------------- */
+
+/* The Smagorinsky eddy viscosity mu_sgs = rho C_s^2 Delta^2 |S| (pde.cu:745)
+ * or a learned local coefficient in place of C_s^2: an MLP 12 -> 64 -> 64 -> 1
+ * (GELU, softplus output) of the resolved strain rate, vorticity and grad T,
+ * evaluated for every cell before each RK stage on BF16 tensor cores with
+ * FP32 accumulation. */
+#define WF_CLOSURE_SMAGORINSKY 0
+#define WF_CLOSURE_MLP 1
+/* Number of floats in a closure parameter vector: W1[64][12], b1[64],
+ * W2[64][64], b2[64], W3[64], b3, then 12 feature scales. */
+int wf_closure_param_count(void);
+/* Select the closure of a context; params (host, wf_closure_param_count()
+ * floats) is copied.  WF_CLOSURE_SMAGORINSKY ignores params. */
+wf_status wf_set_closure(wf_ctx *ctx, int kind, const float *params);
+/* The learned coefficient of every cell of a packed host state (N values). */
+wf_status wf_closure_coefficients(wf_ctx *ctx, const double *y, double *coef);
+/* Training on the current device with the library's own kernels.  x: n x 12
+ * normalised features (row-major), y: n target coefficients.  Loss: mean
+ * squared error of softplus(MLP(x)) against y. */
+wf_status wf_mlp_loss_grad(const float *theta, const float *x, const float *y, size_t n, double *loss, float *grad);
+/* steps Adam steps (lr, beta 0.9 / 0.999) on minibatches of a seeded
+ * permutation per epoch; theta is updated in place (feature scales kept);
+ * loss_history (steps values, may be NULL) receives each batch's loss. */
+wf_status wf_mlp_train(float *theta, const float *x, const float *y, size_t n, int steps, int batch, float lr,
+                       unsigned long long seed, double *loss_history);
+
 /* ---- ensembles of independent members ------------------------------------ */
 
 /* An ensemble steps independent members (their own grids, terrain, wind,

@@ -25,6 +25,7 @@ EXPORTS = [
     "wf_pressure_noalloc", "wf_rk", "wf_pressure_report",
     "wf_ensemble_create", "wf_ensemble_destroy", "wf_ensemble_size", "wf_ensemble_member",
     "wf_ensemble_step", "wf_ensemble_synchronize",
+    "wf_closure_param_count", "wf_set_closure", "wf_closure_coefficients", "wf_mlp_loss_grad", "wf_mlp_train",
 ]
 
 
@@ -62,6 +63,7 @@ def lib():
     L = C.CDLL(LIB_PATH)
     P = C.POINTER(Parameters)
     dp = C.POINTER(C.c_double)
+    fp = C.POINTER(C.c_float)
     vp = C.c_void_p
     sig = {
         "wf_read_parameters": (C.c_int, [C.c_char_p, P]),
@@ -94,6 +96,11 @@ def lib():
         "wf_ensemble_member": (vp, [vp, C.c_int]),
         "wf_ensemble_step": (C.c_int, [vp, C.c_int]),
         "wf_ensemble_synchronize": (C.c_int, [vp]),
+        "wf_closure_param_count": (C.c_int, []),
+        "wf_set_closure": (C.c_int, [vp, C.c_int, fp]),
+        "wf_closure_coefficients": (C.c_int, [vp, dp, dp]),
+        "wf_mlp_loss_grad": (C.c_int, [fp, fp, fp, C.c_size_t, dp, fp]),
+        "wf_mlp_train": (C.c_int, [fp, fp, fp, C.c_size_t, C.c_int, C.c_int, C.c_float, C.c_ulonglong, dp]),
         "wf_pressure_report": (C.c_int, [vp, dp, C.POINTER(C.c_int)]),
         "wf_last_error": (C.c_char_p, []),
     }

@@ -146,6 +146,9 @@ struct wf_ctx {
     int last_iters = 0;
     double last_err = 0.0;   // max |p_m - p_{m-1}| of the last iteration (variable density)
     int last_ref_iter = 0;   // iteration count as solve_pressure_iterative reports it
+    int closure = 0;         // WF_CLOSURE_SMAGORINSKY / WF_CLOSURE_MLP
+    void *coef = nullptr;    // [N] learned coefficient (stencil precision)
+    float *d_theta = nullptr;
 };
 
 namespace wfs {
@@ -284,6 +287,7 @@ std::vector<double> krow_table(const Parameters &P, const double *z, const std::
         r[RDZ] = Z(ZDZ, k);
         r[RDEL2] = Z(ZDELTA2, k);
         r[RZ] = z[k];
+        r[RDD2] = pow(P.dx * P.dy * Z(ZDZ, k), 2.0 / 3.0);
     }
     return t;
 }
@@ -346,6 +350,8 @@ template <class R> StageArgs<R> stage_args(wf_ctx *c, const void *X, const void 
     a.method = c->method;
     a.stage = stage;
     a.a_prev = 0.0;
+    a.coef = c->closure ? (R *)c->coef : nullptr;
+    a.theta = c->d_theta;
     const double dt = c->P.dt;
     if (c->method == 0) a.a_next = dt;
     else if (c->method == 1) a.a_next = (stage == 1) ? dt : 0.5 * dt;
@@ -1057,6 +1063,158 @@ wf_status wf_ensemble_synchronize(wf_ensemble *e)
     if (!e) return WF_ERR_ARG;
     WF_TRY_CUDA(cudaStreamSynchronize(e->master));
     for (wf_ctx *c : e->m) WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+    return WF_OK;
+}
+
+// ---- learned closure --------------------------------------------------------
+int wf_closure_param_count(void) { return closure_param_count(); }
+
+wf_status wf_set_closure(wf_ctx *c, int kind, const float *params)
+{
+    if (!c || (kind != WF_CLOSURE_SMAGORINSKY && kind != WF_CLOSURE_MLP) || (kind == WF_CLOSURE_MLP && !params)) {
+        set_error("wf_set_closure: invalid argument");
+        return WF_ERR_ARG;
+    }
+    drop_graphs(c);
+    if (kind == WF_CLOSURE_SMAGORINSKY) {
+        c->closure = 0;
+        c->launches = c->nstages * 3 + 5 + 1;
+        return WF_OK;
+    }
+    wf_status st;
+    if (!c->d_theta) {
+        void *p = nullptr;
+        if ((st = dev_alloc(c, &p, sizeof(float) * closure_param_count()))) return st;
+        c->d_theta = (float *)p;
+        if ((st = dev_alloc(c, &c->coef, c->esz * (size_t)c->N))) return st;
+    }
+    WF_TRY_CUDA(cudaMemcpy(c->d_theta, params, sizeof(float) * closure_param_count(), cudaMemcpyHostToDevice));
+    c->closure = 1;
+    c->launches = c->nstages * 4 + 5 + 1;
+    return WF_OK;
+}
+
+wf_status wf_closure_coefficients(wf_ctx *c, const double *y, double *coef)
+{
+    if (!c || !y || !coef) { set_error("wf_closure_coefficients: null argument"); return WF_ERR_ARG; }
+    if (!c->closure) { set_error("wf_closure_coefficients: no learned closure set"); return WF_ERR_ARG; }
+    void *in = c->ybuf[1 - c->cur];
+    wf_status st = put_state(c, in, y);
+    if (st) return st;
+    cudaError_t e = (c->prec == WF_FP64)
+                        ? launch_closure_coef<double>((const double *)in, c->geom, c->ph.dx, c->ph.dy, c->d_theta,
+                                                      (double *)c->coef, c->stream)
+                        : launch_closure_coef<float>((const float *)in, c->geom, c->ph.dx, c->ph.dy, c->d_theta,
+                                                     (float *)c->coef, c->stream);
+    if (e) { set_error("wf_closure_coefficients: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
+    if (c->prec == WF_FP64) {
+        WF_TRY_CUDA(cudaMemcpyAsync(coef, c->coef, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
+        WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+    } else {
+        std::vector<float> h(c->N);
+        WF_TRY_CUDA(cudaMemcpyAsync(h.data(), c->coef, sizeof(float) * c->N, cudaMemcpyDeviceToHost, c->stream));
+        WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+        for (int q = 0; q < c->N; q++) coef[q] = h[q];
+    }
+    drop_graphs(c);
+    return WF_OK;
+}
+
+}  // extern "C"
+
+namespace wfs {
+
+// Device scratch of the training entry points, released on every path.
+struct TrainBuffers {
+    std::vector<void *> p;
+    void *get(size_t bytes)
+    {
+        void *q = nullptr;
+        if (cudaMalloc(&q, bytes ? bytes : 16) != cudaSuccess) return nullptr;
+        p.push_back(q);
+        return q;
+    }
+    ~TrainBuffers()
+    {
+        for (void *q : p) cudaFree(q);
+    }
+};
+
+}  // namespace wfs
+
+extern "C" {
+
+wf_status wf_mlp_loss_grad(const float *theta, const float *x, const float *y, size_t n, double *loss, float *grad)
+{
+    if (!theta || !x || !y || !n || !loss || !grad || n > (size_t)1 << 30) {
+        set_error("wf_mlp_loss_grad: invalid argument");
+        return WF_ERR_ARG;
+    }
+    const int np = closure_param_count();
+    TrainBuffers b;
+    float *dth = (float *)b.get(sizeof(float) * np), *dx = (float *)b.get(sizeof(float) * 12 * n);
+    float *dy = (float *)b.get(sizeof(float) * n), *dg = (float *)b.get(sizeof(float) * np);
+    double *dl = (double *)b.get(sizeof(double));
+    if (!dth || !dx || !dy || !dg || !dl) { set_error("wf_mlp_loss_grad: device allocation failed"); return WF_ERR_OOM; }
+    WF_TRY_CUDA(cudaMemcpy(dth, theta, sizeof(float) * np, cudaMemcpyHostToDevice));
+    WF_TRY_CUDA(cudaMemcpy(dx, x, sizeof(float) * 12 * n, cudaMemcpyHostToDevice));
+    WF_TRY_CUDA(cudaMemcpy(dy, y, sizeof(float) * n, cudaMemcpyHostToDevice));
+    WF_TRY_CUDA(launch_mlp_grad(dth, dx, dy, nullptr, (int)n, dg, dl, 0));
+    WF_TRY_CUDA(cudaMemcpy(grad, dg, sizeof(float) * (np - 12), cudaMemcpyDeviceToHost));
+    WF_TRY_CUDA(cudaMemcpy(loss, dl, sizeof(double), cudaMemcpyDeviceToHost));
+    for (int q = np - 12; q < np; q++) grad[q] = 0.0f;   // feature scales are not trained
+    return WF_OK;
+}
+
+wf_status wf_mlp_train(float *theta, const float *x, const float *y, size_t n, int steps, int batch, float lr,
+                       unsigned long long seed, double *loss_history)
+{
+    if (!theta || !x || !y || n < 1 || steps < 1 || batch < 1 || n > (size_t)1 << 30) {
+        set_error("wf_mlp_train: invalid argument");
+        return WF_ERR_ARG;
+    }
+    if ((size_t)batch > n) batch = (int)n;
+    const int np = closure_param_count();
+    TrainBuffers b;
+    float *dth = (float *)b.get(sizeof(float) * np), *dm = (float *)b.get(sizeof(float) * np);
+    float *dv = (float *)b.get(sizeof(float) * np), *dg = (float *)b.get(sizeof(float) * np);
+    float *dx = (float *)b.get(sizeof(float) * 12 * n), *dy = (float *)b.get(sizeof(float) * n);
+    int *didx = (int *)b.get(sizeof(int) * (size_t)batch * steps);
+    double *dl = (double *)b.get(sizeof(double) * steps);
+    if (!dth || !dm || !dv || !dg || !dx || !dy || !didx || !dl) {
+        set_error("wf_mlp_train: device allocation failed");
+        return WF_ERR_OOM;
+    }
+    WF_TRY_CUDA(cudaMemcpy(dth, theta, sizeof(float) * np, cudaMemcpyHostToDevice));
+    WF_TRY_CUDA(cudaMemset(dm, 0, sizeof(float) * np));
+    WF_TRY_CUDA(cudaMemset(dv, 0, sizeof(float) * np));
+    WF_TRY_CUDA(cudaMemcpy(dx, x, sizeof(float) * 12 * n, cudaMemcpyHostToDevice));
+    WF_TRY_CUDA(cudaMemcpy(dy, y, sizeof(float) * n, cudaMemcpyHostToDevice));
+    // minibatches: a fresh seeded permutation of the samples per epoch (splitmix64)
+    std::vector<int> idx((size_t)batch * steps), perm(n);
+    unsigned long long s = seed;
+    auto next = [&]() {
+        unsigned long long z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    size_t pos = n;
+    for (size_t q = 0; q < idx.size(); q++) {
+        if (pos == n) {
+            for (size_t i = 0; i < n; i++) perm[i] = (int)i;
+            for (size_t i = n - 1; i > 0; i--) std::swap(perm[i], perm[next() % (i + 1)]);
+            pos = 0;
+        }
+        idx[q] = perm[pos++];
+    }
+    WF_TRY_CUDA(cudaMemcpy(didx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice));
+    for (int t = 0; t < steps; t++) {
+        WF_TRY_CUDA(launch_mlp_grad(dth, dx, dy, didx + (size_t)t * batch, batch, dg, dl + t, 0));
+        WF_TRY_CUDA(launch_adam(dth, dm, dv, dg, t + 1, lr, 0));
+    }
+    WF_TRY_CUDA(cudaMemcpy(theta, dth, sizeof(float) * (np - 12), cudaMemcpyDeviceToHost));
+    if (loss_history) WF_TRY_CUDA(cudaMemcpy(loss_history, dl, sizeof(double) * steps, cudaMemcpyDeviceToHost));
     return WF_OK;
 }
 

@@ -376,7 +376,13 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
                                     : R(0);
             const Thermo<R> th = thermo(p, smu, sk, Tc, pT[(kk + 1) * ZS], Yq, gk, nzy, Tx, Ty, Tz,
                                         Txx + Tyy + Tzz, t.K(kk, RDZ), rho);
-            t.G(0, ii, jj, kk) = rho * t.K(kk, RDEL2) * mod_S;
+            if (a.coef) {
+                // learned closure: the coefficient of this point replaces C_s^2
+                const R cq = a.coef[((size_t)wrap_p(i0 + ii, Nx - 1) * Ny + wrap_p(j0 + jj, Ny - 1)) * Nz + gk];
+                t.G(0, ii, jj, kk) = rho * (t.K(kk, RDD2) * cq) * mod_S;
+            } else {
+                t.G(0, ii, jj, kk) = rho * t.K(kk, RDEL2) * mod_S;
+            }
             t.G(1, ii, jj, kk) = S11;
             t.G(2, ii, jj, kk) = R(0.5) * (uy + vx);
             t.G(3, ii, jj, kk) = R(0.5) * (uz + wx);
@@ -663,6 +669,10 @@ template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t 
 {
     using C = StageCfg<R>;
     const int ncol = a.g.Nx * a.g.Ny;
+    if (a.coef) {
+        cudaError_t e = launch_closure_coef<R>(a.X, a.g, a.ph.dx, a.ph.dy, a.theta, a.coef, s);
+        if (e) return e;
+    }
     k_utau<R><<<(ncol + 127) / 128, 128, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[0], s);
     const int ntk = (a.g.Nz + C::KZ - 1) / C::KZ, ntj = (a.g.Ny + C::TJ - 1) / C::TJ, nti = (a.g.Nx + C::TI - 1) / C::TI;

@@ -68,6 +68,7 @@ enum KRow {
     RDZ = 14,   // dz_k
     RDEL2 = 15, // Smagorinsky length squared
     RZ = 16,    // z_k
+    RDD2 = 17,  // (dx dy dz_k)^(2/3): the filter width squared (learned closure)
     KROW = 20
 };
 
@@ -103,7 +104,19 @@ struct StageArgs {
     double a_prev;   // Euler/RK2 weights (see stage.cu)
     int method;      // 0 Euler, 1 RK2, 2 RK4, 3 = store k_s itself (operator tests)
     int stage;       // 1-based stage index
+    // learned closure (closure.cu): when coef is set, mu_sgs = rho coef Delta^2 |S|
+    R *coef;               // [N] coefficient of the stage input, written before the stage
+    const float *theta;    // closure parameters on the device
 };
+
+// Learned closure (closure.cu).
+int closure_param_count();
+template <class R>
+cudaError_t launch_closure_coef(const R *X, const Geom &g, double dx, double dy, const float *theta, R *coef,
+                                cudaStream_t s);
+cudaError_t launch_mlp_grad(const float *theta, const float *xs, const float *ys, const int *idx, int n, float *grad,
+                            double *loss, cudaStream_t s);
+cudaError_t launch_adam(float *theta, float *m, float *v, const float *g, int step, float lr, cudaStream_t s);
 
 // Launch helpers implemented in the .cu files.
 // ev (optional): one event recorded after each of the 3 kernels, for profiling.
