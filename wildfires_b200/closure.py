@@ -129,7 +129,7 @@ def targets(uf, vf, wf, dxc, dyc, zc):
 
 
 # ---- cases ----------------------------------------------------------------------
-def study_case(Nc=(33, 33, 13), fine=False, seed=0, Nt=200, dt=0.002, L=100.0, H=8.0, gust=1.0, Y_h=0.1):
+def study_case(Nc=(33, 33, 9), fine=False, seed=0, Nt=120, dt=0.002, L=100.0, H=20.0, gust=1.0, Y_h=0.1):
     """The closure study family: flat terrain, log wind with seeded velocity
     fluctuations (`gust` m/s, on the fine grid's scale so that the coarse grid
     does not resolve them), one hot spot; the fine grid has 4x the intervals
@@ -189,8 +189,9 @@ def fine_snapshots(seed, Nc, steps, every, precision="fp32"):
             yield n, P, y
 
 
-def dataset(seeds, Nc=(33, 33, 13), steps=200, every=20):
-    """Features (unnormalised) and targets at interior coarse nodes."""
+def dataset(seeds, Nc=(33, 33, 9), steps=120, every=12):
+    """Features (unnormalised) and targets at interior coarse nodes (samples
+    with a non-finite value are dropped)."""
     from . import configs
     Pc, _, _ = configs.materialize(study_case(Nc, seed=0, Nt=1))
     r = Pc.rec
@@ -203,7 +204,9 @@ def dataset(seeds, Nc=(33, 33, 13), steps=200, every=20):
             c = targets(uf, vf, wf, r.dx, r.dy, zc)
             X.append(F[:-1, :-1, 1:-1].reshape(-1, NIN))
             Yt.append(c[:-1, :-1, 1:-1].reshape(-1))
-    return np.concatenate(X).astype(np.float32), np.concatenate(Yt).astype(np.float32)
+    X, Yt = np.concatenate(X), np.concatenate(Yt)
+    ok = np.isfinite(X).all(axis=1) & np.isfinite(Yt)
+    return X[ok].astype(np.float32), Yt[ok].astype(np.float32)
 
 
 # ---- training -------------------------------------------------------------------
@@ -243,7 +246,7 @@ def burned_fraction(P, y, y0):
     return float(1.0 - y[4 * N:].sum() / y0[4 * N:].sum())
 
 
-def evaluate(th, seed=100, Nc=(33, 33, 13), steps=200, precision="fp32"):
+def evaluate(th, seed=100, Nc=(33, 33, 9), steps=120, precision="fp32"):
     """Coarse runs with Smagorinsky and with the network against the filtered fine run."""
     import ctypes as C
     from . import Solver, configs
