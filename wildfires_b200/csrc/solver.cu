@@ -310,6 +310,9 @@ template <class R> PhysR<R> make_physr(const Parameters &P)
     r.c4 = (R)(4 * kSigmaSB * P.delta);
     r.Pr = (R)P.Pr;
     r.inv_avd = R(1) / R(26.0);
+    r.mu_Trho = (R)(P.mu / (P.T_inf * P.rho_inf));
+    r.inv_Trho_cp = (R)(1.0 / (P.T_inf * P.rho_inf * P.c_p));
+    r.H_C_cp = (R)(P.H_C / P.c_p);
     r.T_min = (R)P.T_min; r.T_max = (R)P.T_max; r.Y_min = (R)P.Y_min; r.Y_max = (R)P.Y_max;
     return r;
 }

@@ -62,6 +62,9 @@ __device__ __forceinline__ float rfabs(float x) { return fabsf(x); }
 // exponential is smaller than half an ulp of 1 and the result is exactly 1.
 __device__ __forceinline__ double van_driest(double x) { return x < -37.5 ? 1.0 : 1.0 - exp(x); }
 __device__ __forceinline__ float van_driest(float x) { return x < -17.5f ? 1.0f : 1.0f - expf(x); }
+template <class R> struct VanDriestCut;
+template <> struct VanDriestCut<double> { static constexpr double v = 37.5; };
+template <> struct VanDriestCut<float> { static constexpr float v = 17.5f; };
 
 // Temperature source terms (pde.cu:664-711).
 template <class R> struct Thermo {
@@ -291,6 +294,26 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
         __syncthreads();
 
         const int smu = a.ph.sutherland_viscosity, sk = a.ph.sutherland_conductivity;
+        // FP32 path without Sutherland laws or convective exchange: the
+        // divergence source nu T_RHS / T reduces to mu/(T_inf rho_inf) T_RHS
+        const bool lean = sizeof(R) == 4 && smu != 1 && sk != 1 && !(p.alpha_s * p.sigma_s != R(0));
+
+        // Lower bound over the tile of z_ibm u_tau / A_vd: when it exceeds
+        // the cut-off times nu, every Van Driest factor of the tile is exactly 1.
+        __shared__ R s_vd_bound;
+        if (threadIdx.x < 32) {
+            const R zlow = (k0 > 0) ? t.K(-1, RZ) : R(0);
+            R hmax = R(-1e30), umin = R(1e30);
+            for (int c = threadIdx.x; c < TL::NCOL; c += 32) {
+                hmax = rmax(hmax, (R)t.ctopo[c]);
+                umin = rmin(umin, t.cut_[c]);
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                hmax = rmax(hmax, __shfl_xor_sync(0xffffffffu, hmax, o));
+                umin = rmin(umin, __shfl_xor_sync(0xffffffffu, umin, o));
+            }
+            if (threadIdx.x == 0) s_vd_bound = rmax(zlow - hmax, R(0)) * rmax(umin, R(0)) * p.inv_avd;
+        }
 
         // ---- 2. SGS inputs on the tile and its halo 1 (pde.cu:632-765).  Needed
         //        set: tile columns on k0-1 .. k0+KZ, side columns on k0 .. k0+KZ-1.
@@ -374,8 +397,19 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
             // fuel fraction of the stage input (used only below the column's fuel top)
             const R Yq = (gk < nzy) ? X[4 * (size_t)N + (size_t)(wrap_p(i0 + ii, Nx - 1) * Ny + wrap_p(j0 + jj, Ny - 1)) * g.NzY + gk]
                                     : R(0);
-            const Thermo<R> th = thermo(p, smu, sk, Tc, pT[(kk + 1) * ZS], Yq, gk, nzy, Tx, Ty, Tz,
-                                        Txx + Tyy + Tzz, t.K(kk, RDZ), rho);
+            R g7;
+            if (lean) {
+                const R K_T = (Tc > p.T_pc) ? p.A * rexp(-fdiv(p.T_act, Tc)) : R(0);
+                const R Yv = (gk < nzy) ? Yq : R(0);
+                const R T2 = Tc * Tc;
+                g7 = p.mu_Trho * ((p.c12 * T2 * (Tx * Tx + Ty * Ty + Tz * Tz) + (p.kT + p.c4 * (T2 * Tc)) * (Txx + Tyy + Tzz)) *
+                                      (Tc * p.inv_Trho_cp) +
+                                  p.H_C_cp * Yv * K_T);
+            } else {
+                const Thermo<R> th = thermo(p, smu, sk, Tc, pT[(kk + 1) * ZS], Yq, gk, nzy, Tx, Ty, Tz,
+                                            Txx + Tyy + Tzz, t.K(kk, RDZ), rho);
+                g7 = fdiv(th.nu * th.T_RHS_tmp, Tc);
+            }
             if (a.coef) {
                 // learned closure: the coefficient of this point replaces C_s^2
                 const R cq = a.coef[((size_t)wrap_p(i0 + ii, Nx - 1) * Ny + wrap_p(j0 + jj, Ny - 1)) * Nz + gk];
@@ -389,7 +423,7 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
             t.G(4, ii, jj, kk) = S22;
             t.G(5, ii, jj, kk) = R(0.5) * (wy + vz);
             t.G(6, ii, jj, kk) = S33;
-            t.G(7, ii, jj, kk) = fdiv(th.nu * th.T_RHS_tmp, Tc);
+            t.G(7, ii, jj, kk) = g7;
         }
         __syncthreads();
 
@@ -484,14 +518,17 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
                     };
                     const int qxp = TL::cq(ii + 1, jj), qxm = TL::cq(ii - 1, jj);
                     const int qyp = TL::cq(ii, jj + 1), qym = TL::cq(ii, jj - 1);
-                    const R ut0 = t.cut_[cc];
-                    const R fc = van_driest(-zibm(cc, zk) * ut0 * inv_avd_nu);
-                    const R fxp_ = van_driest(-zibm(qxp, zk) * t.cut_[qxp] * inv_avd_nu);
-                    const R fxm_ = van_driest(-zibm(qxm, zk) * t.cut_[qxm] * inv_avd_nu);
-                    const R fyp_ = van_driest(-zibm(qyp, zk) * t.cut_[qyp] * inv_avd_nu);
-                    const R fym_ = van_driest(-zibm(qym, zk) * t.cut_[qym] * inv_avd_nu);
-                    const R fkm = van_driest(-zibm(cc, t.K(kk - 1, RZ)) * ut0 * inv_avd_nu);
-                    const R fkp = van_driest(-zibm(cc, t.K(kk + 1, RZ)) * ut0 * inv_avd_nu);
+                    R fc = R(1), fxp_ = R(1), fxm_ = R(1), fyp_ = R(1), fym_ = R(1), fkm = R(1), fkp = R(1);
+                    if (!(s_vd_bound > VanDriestCut<R>::v * R(1.001) * nu)) {
+                        const R ut0 = t.cut_[cc];
+                        fc = van_driest(-zibm(cc, zk) * ut0 * inv_avd_nu);
+                        fxp_ = van_driest(-zibm(qxp, zk) * t.cut_[qxp] * inv_avd_nu);
+                        fxm_ = van_driest(-zibm(qxm, zk) * t.cut_[qxm] * inv_avd_nu);
+                        fyp_ = van_driest(-zibm(qyp, zk) * t.cut_[qyp] * inv_avd_nu);
+                        fym_ = van_driest(-zibm(qym, zk) * t.cut_[qym] * inv_avd_nu);
+                        fkm = van_driest(-zibm(cc, t.K(kk - 1, RZ)) * ut0 * inv_avd_nu);
+                        fkp = van_driest(-zibm(cc, t.K(kk + 1, RZ)) * ut0 * inv_avd_nu);
+                    }
                     const R mu_c = t.G(0, ii, jj, kk) * (fc * fc);
                     const R mu_xp = t.G(0, ii + 1, jj, kk) * (fxp_ * fxp_), mu_xm = t.G(0, ii - 1, jj, kk) * (fxm_ * fxm_);
                     const R mu_yp = t.G(0, ii, jj + 1, kk) * (fyp_ * fyp_), mu_ym = t.G(0, ii, jj - 1, kk) * (fym_ * fym_);

@@ -56,6 +56,7 @@ template <class R> struct PhysR {
     R mu, kT, Y_f, H_C, A, T_act, T_pc, h_c, alpha_s, sigma_s;
     R T_inf, c_p, rho_inf, cd, g, c12, c4, Pr, inv_avd;
     R T_min, T_max, Y_min, Y_max;
+    R mu_Trho, inv_Trho_cp, H_C_cp;     // mu/(T_inf rho_inf), 1/(T_inf rho_inf c_p), H_C/c_p
 };
 
 // Per-k row of z-stencil weights in the stencil precision (branch-free
