@@ -147,11 +147,23 @@ struct wf_ctx {
     double last_err = 0.0;   // max |p_m - p_{m-1}| of the last iteration (variable density)
     int last_ref_iter = 0;   // iteration count as solve_pressure_iterative reports it
     int closure = 0;         // WF_CLOSURE_SMAGORINSKY / WF_CLOSURE_MLP
+    int *d_bcfix = nullptr;  // columns left to k_stage_bc
+    int nbcfix = 0;
     void *coef = nullptr;    // [N] learned coefficient (stencil precision)
     float *d_theta = nullptr;
 };
 
 namespace wfs {
+
+// Kernel launches of one step: per stage the optional closure inference,
+// k_utau, k_stage_fused and, when some column needs it, k_stage_bc; five
+// pressure kernels per solve; the projection.
+int launches_per_step(const wf_ctx *c)
+{
+    const int per_stage = 2 + (c->nbcfix > 0 ? 1 : 0) + (c->closure ? 1 : 0);
+    const int solves = (c->P.variable_density != 0) ? (c->P.pressure_solver_iter > 1 ? c->P.pressure_solver_iter : 1) : 1;
+    return c->nstages * per_stage + 5 * solves + 1;
+}
 
 wf_status dev_alloc(wf_ctx *c, void **out, size_t bytes)
 {
@@ -355,6 +367,8 @@ template <class R> StageArgs<R> stage_args(wf_ctx *c, const void *X, const void 
     a.a_prev = 0.0;
     a.coef = c->closure ? (R *)c->coef : nullptr;
     a.theta = c->d_theta;
+    a.bcfix = c->d_bcfix;
+    a.nbcfix = c->nbcfix;
     const double dt = c->P.dt;
     if (c->method == 0) a.a_next = dt;
     else if (c->method == 1) a.a_next = (stage == 1) ? dt : 0.5 * dt;
@@ -725,9 +739,22 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
     cudaError_t e = (precision == WF_FP64) ? poisson_set_attributes<double>() : poisson_set_attributes<float>();
     if (e == cudaSuccess) e = (precision == WF_FP64) ? stage_set_attributes<double>() : stage_set_attributes<float>();
     if (e != cudaSuccess) { set_error("wf_create: %s", cudaGetErrorString(e)); return fail(WF_ERR_CUDA); }
+    {
+        // columns whose cut node (or, for every column, the top plane) the
+        // fused stage pass cannot complete within one z-tile
+        const int KZ = stage_tile_planes(precision);
+        const bool top_ok = (Nz - 1) / KZ == (Nz - 3) / KZ;
+        std::vector<int> fix;
+        for (int col = 0; col < Nx * Ny; col++) {
+            const int kc = c->hcut[col];
+            if (!top_ok || kc / KZ != (kc + 2) / KZ) fix.push_back(col);
+        }
+        c->nbcfix = (int)fix.size();
+        if (!fix.empty() && (st = upload(c, &c->d_bcfix, fix.data(), fix.size()))) return fail(st);
+    }
     WF_TRY_CUDA(cudaMemsetAsync(c->p, 0, sizeof(double) * c->N, c->stream));
     WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
-    c->launches = c->nstages * 3 + 5 + 1;
+    c->launches = launches_per_step(c);
     *out = c;
     return WF_OK;
 }
@@ -1081,7 +1108,7 @@ wf_status wf_set_closure(wf_ctx *c, int kind, const float *params)
     drop_graphs(c);
     if (kind == WF_CLOSURE_SMAGORINSKY) {
         c->closure = 0;
-        c->launches = c->nstages * 3 + 5 + 1;
+        c->launches = launches_per_step(c);
         return WF_OK;
     }
     wf_status st;
@@ -1093,7 +1120,7 @@ wf_status wf_set_closure(wf_ctx *c, int kind, const float *params)
     }
     WF_TRY_CUDA(cudaMemcpy(c->d_theta, params, sizeof(float) * closure_param_count(), cudaMemcpyHostToDevice));
     c->closure = 1;
-    c->launches = c->nstages * 4 + 5 + 1;
+    c->launches = launches_per_step(c);
     return WF_OK;
 }
 

@@ -135,6 +135,55 @@ __device__ __forceinline__ bool stage_reads_acc(int method, int stage)
     return (method == 1 && stage == 2) || (method == 2 && stage > 1);
 }
 
+// RK update of the value at offset o with k-value kv.
+template <class R>
+__device__ __forceinline__ void rk_cell(const StageArgs<R> &a, size_t o, R kv, bool rd, bool kp, R an)
+{
+    R accv = rd ? a.acc[o] : R(0);
+    a.Xout[o] = rk_update(a.method, a.stage, kv, a.yn[o], accv, an);
+    if (kp) a.acc[o] = accv;
+}
+
+// Whether the cut node kc and the two cells above it share a z-tile of KZ
+// planes (then the fused pass completes the cut node), and the same for the
+// top plane and the two below it.
+__host__ __device__ __forceinline__ bool bc_cut_in_tile(int kc, int KZ) { return kc / KZ == (kc + 2) / KZ; }
+__host__ __device__ __forceinline__ bool bc_top_in_tile(int Nz, int KZ) { return (Nz - 1) / KZ == (Nz - 3) / KZ; }
+
+// Cut node of a column (pde.cu:58-77): no-slip velocity, T and Y extrapolated
+// from the k-values of kc+1 and kc+2 held in the column's boundary slots.
+template <class R>
+__device__ __forceinline__ void bc_cut_node(const StageArgs<R> &a, int col, int kc, int nzy, bool rd, bool kp, R an)
+{
+    const R *bc = a.bc + (size_t)col * kBcSlots;
+    const size_t N = (size_t)a.g.N, cb = (size_t)col * a.g.Nz;
+    const double *z = a.g.z;
+    const R A = (R)(z[kc + 1] - z[kc]), B = (R)(z[kc + 2] - z[kc + 1]);
+    rk_cell(a, cb + kc, R(0), rd, kp, an);
+    rk_cell(a, N + cb + kc, R(0), rd, kp, an);
+    rk_cell(a, 2 * N + cb + kc, R(0), rd, kp, an);
+    rk_cell(a, 3 * N + cb + kc, fdiv((A + B) * (A + B) * bc[0] - A * A * bc[1], B * (R(2) * A + B)), rd, kp, an);
+    if (kc < nzy) {
+        const R Y1 = (kc + 1 < nzy) ? bc[2] : R(0), Y2 = (kc + 2 < nzy) ? bc[3] : R(0);
+        rk_cell(a, 4 * N + (size_t)col * a.g.NzY + kc, fdiv((A + B) * (A + B) * Y1 - A * A * Y2, B * (R(2) * A + B)),
+                rd, kp, an);
+    }
+}
+
+// Top plane of a column (pde.cu:79-86): second-order extrapolation from Nz-2, Nz-3.
+template <class R>
+__device__ __forceinline__ void bc_top(const StageArgs<R> &a, int col, bool rd, bool kp, R an)
+{
+    const R *bc = a.bc + (size_t)col * kBcSlots;
+    const int k = a.g.Nz - 1;
+    const size_t N = (size_t)a.g.N, cb = (size_t)col * a.g.Nz;
+    const double *z = a.g.z;
+    const R a1 = (R)(z[k] - z[k - 1]), a2 = (R)(z[k - 1] - z[k - 2]);
+    const R num = (a2 + a1) * (a2 + a1), den = a2 * (a2 + R(2) * a1), a1s = a1 * a1;
+#pragma unroll
+    for (int f = 0; f < 4; f++) rk_cell(a, (size_t)f * N + cb + k, fdiv(num * bc[4 + f] - a1s * bc[8 + f], den), rd, kp, an);
+}
+
 // ---------------------------------------------------------------------------
 // wall friction velocity of every column from its k = 0 plane
 // (pde.cu:767-772: tau_w = sqrt((mu uz)^2 + (mu vz)^2), u_tau = sqrt(tau_w/rho))
@@ -437,10 +486,19 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
             const int col = gi * Ny + gj;
             const int cc = TL::cq(ii, jj);
             const int kc = t.ccut[cc], nzy = t.cnzy[cc];
+            const size_t cg = (size_t)col * Nz + gk;
+            if (gk < kc) {
+                // dead node below the terrain: the boundary rules fix its k-values (pde.cu:88-97)
+                const double dv[4] = {a.ph.u_dead, a.ph.v_dead, a.ph.w_dead, a.ph.T_dead};
+#pragma unroll
+                for (int f = 0; f < 4; f++) rk_cell(a, (size_t)f * N + cg, (R)dv[f], rd, kp, an);
+                if (gk < g.NzY)
+                    rk_cell(a, 4 * (size_t)N + (size_t)col * g.NzY + gk, (gk < nzy) ? (R)a.ph.Y_dead : R(0), rd, kp, an);
+                continue;
+            }
             const bool live = (gk > kc) && (gk < Nz - 1);                 // not overwritten by the boundary rules
             const bool ylive = (gk < g.NzY) && !(gk <= kc && gk < nzy);   // fuel value this pass updates
             if (!live && !ylive) continue;
-            const size_t cg = (size_t)col * Nz + gk;
             // start the RK operand loads early
             R ynv[4], accv[4];
             if (live) {
@@ -586,6 +644,19 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
                 if (kp) a.acc[oY] = accY;
             }
         }
+        __syncthreads();
+        // ---- 4. cut node and top of the tile's columns, where the two cells
+        //        they extrapolate from are in this tile (their k-values were
+        //        stored to a.bc above); the other columns go to k_stage_bc.
+        for (int q = threadIdx.x; q < TI * TJ; q += NT) {
+            const int ii = q / TJ, jj = q % TJ;
+            const int gi = i0 + ii, gj = j0 + jj;
+            if (gi >= Nx || gj >= Ny) continue;
+            const int col = gi * Ny + gj;
+            const int kc = t.ccut[TL::cq(ii, jj)], nzy = t.cnzy[TL::cq(ii, jj)];
+            if (kc >= k0 && kc < k0 + KZ && bc_cut_in_tile(kc, KZ)) bc_cut_node(a, col, kc, nzy, rd, kp, an);
+            if (Nz - 1 >= k0 && Nz - 1 < k0 + KZ && bc_top_in_tile(Nz, KZ)) bc_top(a, col, rd, kp, an);
+        }
         __syncthreads();         // buffer and SGS inputs free for the next tiles
     }
     cp_async_wait<0>();
@@ -593,84 +664,25 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
 
 
 // ---------------------------------------------------------------------------
-// boundary/IBM k-values per column (pde.cu:14-99) and their RK update
+// Boundary values the fused pass could not complete (pde.cu:14-99): the cut
+// node of the listed columns whose kc+1 / kc+2 lie in the next z-tile, and the
+// top plane when Nz-3 and Nz-1 lie in different z-tiles.  One thread per
+// listed column; the k-values come from the boundary slots.
 template <class R>
-__global__ void __launch_bounds__(256) k_stage_bc(const StageArgs<R> a)
+__global__ void __launch_bounds__(128) k_stage_bc(const StageArgs<R> a, int KZ)
 {
-    // kBcLanes lanes per column; the column's boundary values -- 4 fields (and
-    // Y where stored) on each dead node k < kc, 5 on the cut node, 4 on the
-    // top -- are enumerated field-major so consecutive lanes touch
-    // consecutive k of one field.
-    constexpr int kBcLanes = 16;
-    const Geom &g = a.g;
-    const Phys &ph = a.ph;
-    const int col = (blockIdx.x * blockDim.x + threadIdx.x) / kBcLanes;
-    const int lane = threadIdx.x % kBcLanes;
-    if (col >= g.Nx * g.Ny) return;
-    const int Nz = g.Nz, N = g.N;
-    const int kc = __ldg(g.cut + col), nzy = __ldg(g.nzy + col);
-    const R *bc = a.bc + (size_t)col * kBcSlots;
-    const double *z = g.z;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= a.nbcfix) return;
+    const int col = a.bcfix[q];
+    const int kc = __ldg(a.g.cut + col), nzy = __ldg(a.g.nzy + col);
     const R an = (R)a.a_next;
     const bool rd = stage_reads_acc(a.method, a.stage), kp = stage_keeps_acc(a.method, a.stage);
-    const size_t cb = (size_t)col * Nz;
-    const size_t cy = 4 * (size_t)N + (size_t)col * g.NzY;
-    const int n_dead = 4 * kc + min(kc, nzy);
-    const int n_items = n_dead + 5 + 4;
-    for (int u = lane; u < n_items; u += kBcLanes) {
-        size_t o;
-        R kv;
-        if (u < n_dead) {
-            // dead nodes below the terrain
-            int f, k;
-            if (u < 4 * kc) {
-                f = u / kc;
-                k = u - f * kc;
-            } else {
-                f = 4;
-                k = u - 4 * kc;
-            }
-            o = (f < 4) ? (size_t)f * N + cb + k : cy + k;
-            const double dv = (f == 0) ? ph.u_dead : (f == 1) ? ph.v_dead : (f == 2) ? ph.w_dead
-                            : (f == 3) ? ph.T_dead : ph.Y_dead;
-            kv = (R)dv;
-        } else if (u < n_dead + 5) {
-            // cut node: no-slip velocity, second-order extrapolated T and Y
-            const int f = u - n_dead;
-            if (f == 4 && kc >= nzy) continue;
-            o = (f < 4) ? (size_t)f * N + cb + kc : cy + kc;
-            kv = R(0);
-            if (f >= 3) {
-                const R A = (R)(z[kc + 1] - z[kc]), B = (R)(z[kc + 2] - z[kc + 1]);
-                R v1, v2;
-                if (f == 3) {
-                    v1 = bc[0];
-                    v2 = bc[1];
-                } else {
-                    v1 = (kc + 1 < nzy) ? bc[2] : R(0);
-                    v2 = (kc + 2 < nzy) ? bc[3] : R(0);
-                }
-                kv = fdiv((A + B) * (A + B) * v1 - A * A * v2, B * (R(2) * A + B));
-            }
-        } else {
-            // top: second-order extrapolation from k = Nz-2, Nz-3
-            const int f = u - n_dead - 5;
-            const int k = Nz - 1;
-            const R a1 = (R)(z[k] - z[k - 1]), a2 = (R)(z[k - 1] - z[k - 2]);
-            const R num = (a2 + a1) * (a2 + a1), den = a2 * (a2 + R(2) * a1), a1s = a1 * a1;
-            o = (size_t)f * N + cb + k;
-            kv = fdiv(num * bc[4 + f] - a1s * bc[8 + f], den);
-        }
-        R accv = rd ? a.acc[o] : R(0);
-        a.Xout[o] = rk_update(a.method, a.stage, kv, a.yn[o], accv, an);
-        if (kp) a.acc[o] = accv;
-    }
+    if (!bc_cut_in_tile(kc, KZ)) bc_cut_node(a, col, kc, nzy, rd, kp, an);
+    if (!bc_top_in_tile(a.g.Nz, KZ)) bc_top(a, col, rd, kp, an);
 }
 
 }  // namespace
 
-// Tile shapes: FP32 8 x 16 x 8 cells (two blocks per SM), FP64 8 x 8 x 8 cells
-// (one block per SM).
 template <class R> struct StageCfg;
 template <> struct StageCfg<float> {
     static constexpr int TI = 8, TJ = 16, KZ = 8, NT = 256;
@@ -717,10 +729,12 @@ template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t 
     const int blocks = ntiles;
     k_stage_fused<R, C::TI, C::TJ, C::KZ, C::NT><<<blocks, C::NT, stage_smem_bytes<R>(), s>>>(a, ntk, ntj, nti);
     if (ev) cudaEventRecord(ev[1], s);
-    k_stage_bc<R><<<(ncol + 15) / 16, 256, 0, s>>>(a);
+    if (a.nbcfix > 0) k_stage_bc<R><<<(a.nbcfix + 127) / 128, 128, 0, s>>>(a, C::KZ);
     if (ev) cudaEventRecord(ev[2], s);
     return cudaGetLastError();
 }
+
+int stage_tile_planes(int precision) { return precision == 0 ? StageCfg<double>::KZ : StageCfg<float>::KZ; }
 
 template cudaError_t launch_stage<double>(const StageArgs<double> &, cudaStream_t, cudaEvent_t *);
 template cudaError_t launch_stage<float>(const StageArgs<float> &, cudaStream_t, cudaEvent_t *);

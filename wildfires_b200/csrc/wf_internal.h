@@ -108,6 +108,8 @@ struct StageArgs {
     // learned closure (closure.cu): when coef is set, mu_sgs = rho coef Delta^2 |S|
     R *coef;               // [N] coefficient of the stage input, written before the stage
     const float *theta;    // closure parameters on the device
+    const int *bcfix;      // columns whose cut node or top the fused pass leaves to k_stage_bc
+    int nbcfix;
 };
 
 // Learned closure (closure.cu).
@@ -123,6 +125,7 @@ cudaError_t launch_adam(float *theta, float *m, float *v, const float *g, int st
 // ev (optional): one event recorded after each of the 3 kernels, for profiling.
 template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t s, cudaEvent_t *ev = nullptr);
 template <class R> cudaError_t stage_set_attributes();
+int stage_tile_planes(int precision);   // z planes of a fused-stage tile
 
 template <class R>
 struct ProjectArgs {
