@@ -157,8 +157,22 @@ __device__ __forceinline__ void stage(double2 *buf, int jj, const double2 *__res
         const int j = jj + T * b;
         const int k = j & (Ns - 1);
         if constexpr (Ns > 1) {
+            // twiddles w^r, w = exp(-2 pi i k / (Ns R)): powers of two from the
+            // table, the rest as products of at most three of them
+            constexpr int SH = L - SL - LR;
+            double2 w[R];
+            w[1] = __ldg(tw + (k << SH));
+            if constexpr (R > 2) w[2] = __ldg(tw + ((2 * k) << SH));
+            if constexpr (R > 4) w[4] = __ldg(tw + ((4 * k) << SH));
+            if constexpr (R > 8) w[8] = __ldg(tw + ((8 * k) << SH));
 #pragma unroll
-            for (int r = 1; r < R; r++) v[b][r] = cmul(v[b][r], __ldg(tw + ((r * k) << (L - SL - LR))));
+            for (int r = 3; r < R; r++) {
+                if ((r & (r - 1)) == 0) continue;
+                const int hi = 1 << (31 - __clz(r));     // highest power of two in r
+                w[r] = cmul(w[hi], w[r - hi]);
+            }
+#pragma unroll
+            for (int r = 1; r < R; r++) v[b][r] = cmul(v[b][r], w[r]);
         }
         dft<R>(v[b]);
         const int base = ((j >> SL) << (SL + LR)) + k;
