@@ -47,6 +47,7 @@ def parse_args():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-refgpu", action="store_true", help="skip timing the reference's own GPU build")
     ap.add_argument("--ensemble", type=int, default=0, metavar="M",
                     help="instead: M seeded members of uneven grids (Nx, Ny in 96..256, Nz = 64), "
                          "one graph launch per ensemble step against the members stepped one by one")
@@ -246,6 +247,27 @@ def _sample_kw(name, n, nsteps):
     return kw
 
 
+def reference_gpu_sample(case_name, n_short=2, n_long=6):
+    """The reference's own sm_100a build (oracle/_ref/ref_gpu: its src/cu
+    sources compiled unmodified, FP64) on the same workload and GPU: wall time
+    of its solve_PDE for n_long and n_short steps; the difference divided by
+    the extra steps removes its set-up (allocations, coefficient tables)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner
+    from wildfires_b200 import configs
+    if not ref_runner.available("gpu"):
+        return None
+    secs = {}
+    for n in (n_short, n_long):
+        secs[n] = ref_runner.run(configs.CASES[case_name](Nt=n), "time", flavour="gpu")["seconds"]
+    per = (secs[n_long] - secs[n_short]) / (n_long - n_short)
+    P = build_params_only(case_name)
+    cells = P.rec.Nx * P.rec.Ny * P.rec.Nz
+    return {"value": round(cells / per / 1e6, 2), "unit": METRIC, "ms_per_step": round(per * 1e3, 2),
+            "dtype": "f64", "how": "reference src/cu built for sm_100a, solve_PDE wall time for %d and %d steps, "
+                                   "difference per step (set-up removed)" % (n_short, n_long)}
+
+
 # ---- GPU arm --------------------------------------------------------------------
 def run_ours(args):
     import torch
@@ -407,6 +429,7 @@ def run_ours(args):
             "config": workload_config(args.config, P, args.precision, world),
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roof,
             "kernels": kernels, "cpu_baseline": cpu, "clocks": clk, "fp64": fp64,
+            "reference_gpu": None if (args.no_refgpu or world > 1) else reference_gpu_sample(args.config),
         }
         print(json.dumps(out), flush=True)
     if world > 1:
