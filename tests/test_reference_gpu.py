@@ -1,10 +1,14 @@
 """Full-size parity against the reference's own CUDA solver.
 
 The reference's src/cu sources, built unmodified for sm_100a by oracle/Makefile
-(oracle/_ref/ref_gpu), run the flat 128 x 128 x 64 workload on the same B200
-from the same seeded inputs.  Comparisons use the periodic cell set (the
-duplicate planes i = Nx-1, j = Ny-1 are filled by the reference with a racy
-in-place copy, src/cu/pressure.cu:409-414, and never feed back).
+(oracle/_ref/ref_gpu), run the flat 128 x 128 x 64 workload and the
+512 x 512 x 128 eight-hill workload on the same B200 from the same seeded
+inputs.  Comparisons use the periodic cell set (the duplicate planes
+i = Nx-1, j = Ny-1 are filled by the reference with an in-place copy that races
+with the writes of plane 0, src/cu/pressure.cu:409-414; on these grids each
+reference thread owns 16 or more cells, plane 0 is written long before the
+copy, and the GPU build is reproducible -- on grids with one cell per thread
+it is not, see tests/test_dropin_gpu.py).
 
 The model amplifies rounding differences by about 1e12 between steps 50 and
 100 of this workload (buoyant plume + stiff Arrhenius source): the reference's
@@ -77,3 +81,15 @@ def test_fp64_after_stated_steps_within_model_sensitivity():
     own = _errors(P, yp, y)
     for f in "uvwT":
         assert vs_ref[f][1] <= own[f][1], (f, vs_ref[f], own[f])
+
+
+def test_full_size_eight_hills_fp64_matches_reference_cuda():
+    """The benchmark workload itself (512 x 512 x 128, terrain override), three
+    FP64 steps against the reference's own GPU build at the 1e-10 gate."""
+    from wildfires_b200 import configs
+    res = ref_runner.run(configs.hills8(Nt=3), "step", flavour="gpu", timeout=1800)
+    y, d = _run(res["P"], res["y0"], res["p0"], 3)
+    assert d["nan_count"] == 0
+    errs = _errors(res["P"], y, res["y"])
+    bad = {f: e for f, e in errs.items() if e[0] > 1e-10 or e[1] > 1e-10}
+    assert not bad, bad
