@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_fftx(double2 *__restri
 // zt holds per-k constants: [0..nk) a, [nk..2nk) c, [2nk..3nk) D (b = -(kk + D)),
 // followed by b0, c0base, inv_dz1, half_dz0, cl.  The right-hand sides are
 // fetched eight planes ahead of the recurrence so the loads overlap.
-__global__ void __launch_bounds__(128) k_p_tridiag(double2 *__restrict__ G, const double *__restrict__ kx2,
+__global__ void __launch_bounds__(128, 8) k_p_tridiag(double2 *__restrict__ G, const double *__restrict__ kx2,
                                                    const double *__restrict__ ky2, const double *__restrict__ zt,
                                                    int n0, int h1, int nk)
 {
