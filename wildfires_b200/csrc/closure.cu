@@ -8,10 +8,11 @@
 // scaled by Delta / 1 m/s and temperature gradients by Delta / 100 K, then by
 // per-feature scales learned with the weights; Delta = (dx dy dz_k)^(1/3).
 //
-//   k_closure_coef  inference for every cell of a stage input: BF16 weights
-//                   and activations on the tensor cores (mma.sync m16n8k16,
-//                   FP32 accumulation), 32 cells per warp.  The stage kernel
-//                   reads the coefficient in place of C_s^2.
+//   k_closure_coef_tc  inference for every cell of a stage input on the
+//                   5th-generation tensor cores: tcgen05.mma with BF16 operands
+//                   in shared memory and FP32 accumulators in tensor memory,
+//                   128 cells per CTA.  The stage kernel reads the coefficient
+//                   in place of C_s^2.
 //   k_mlp_grad      training: FP32 forward + backward per sample, gradients
 //                   accumulated in shared memory then in global memory.
 //   k_adam          Adam update of the FP32 master parameters.
@@ -55,31 +56,10 @@ __device__ __forceinline__ int wrap1(int v, int n)
     return v;
 }
 
-// ---- inference ---------------------------------------------------------------
-// Shared memory (bytes): W1 as [64][24] bf16 (k padded 12 -> 16, row stride
-// 24 for conflict-free fragment loads), W2 [64][72] bf16, W3, b1, b2, b3,
-// scales (fp32), and per warp a 32 x 24 bf16 feature tile.
-constexpr int W1S = 24, W2S = 72, XS = 24;
-constexpr int kClosureThreads = 256;
-constexpr size_t kSmemW1 = 0;
-constexpr size_t kSmemW2 = kSmemW1 + sizeof(__nv_bfloat16) * NH * W1S;
-constexpr size_t kSmemF = kSmemW2 + sizeof(__nv_bfloat16) * NH * W2S;
-constexpr size_t kSmemX = kSmemF + sizeof(float) * (NH + NH + NH + 1 + NIN + 3);
-constexpr size_t kSmemClosure = kSmemX + sizeof(__nv_bfloat16) * (kClosureThreads / 32) * 32 * XS;
-
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 {
     const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);   // .x = lo (lower 16 bits)
     return *reinterpret_cast<const uint32_t *>(&v);
-}
-
-__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
-                                         uint32_t b0, uint32_t b1)
-{
-    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-                 "{%0,%1,%2,%3};"
-                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
 // The 12 raw features at cell (i, j, k) of the state X (walls: zero).
@@ -126,42 +106,136 @@ __device__ void cell_features(const R *__restrict__ X, const Geom &g, double dx,
     f[11] = d[3][2] * st;
 }
 
-template <class R>
-__global__ void __launch_bounds__(kClosureThreads) k_closure_coef(const R *__restrict__ X, Geom g, double dx,
-                                                                  double dy, const float *__restrict__ theta,
-                                                                  R *__restrict__ coef)
+// ---- inference on the 5th-generation tensor cores (tcgen05 + TMEM) ---------------
+// One CTA of 128 threads (one warpgroup) per tile of 128 cells, persistent over
+// tiles.  Thread r computes the features of cell r of the tile into the A
+// operand (BF16, K-major, no swizzle: 8-row x 16-byte core matrices); one
+// thread issues tcgen05.mma (M = 128, N = 64, FP32 accumulation in TMEM) for
+// layer 1 (K = 16) and, after the epilogue has written GELU(h1) back as the
+// next A operand, four for layer 2 (K = 64); each warp reads its 32 TMEM lanes
+// (= its 32 cells) with tcgen05.ld.  Every mbarrier wait is bounded: on timeout
+// the kernel raises *err, skips the rest and still frees its TMEM.
+constexpr int kTcThreads = 128, kTcCols = 128;
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr size_t kTcA1 = 0, kTcA2 = kTcA1 + 128 * 16 * 2, kTcB1 = kTcA2 + 128 * 64 * 2, kTcB2 = kTcB1 + 64 * 16 * 2;
+constexpr size_t kTcF = kTcB2 + 64 * 64 * 2;                       // fp32: b1, b2, W3, b3, scales
+constexpr size_t kTcBar = kTcF + sizeof(float) * (64 + 64 + 64 + 4 + 12);
+constexpr size_t kSmemTc = kTcBar + 16;
+
+// byte offset of (row, k) in a K-major no-swizzle operand with K/8 core
+// matrices per 8-row group (core matrix = 8 rows x 8 bf16 = 128 bytes)
+__device__ __forceinline__ uint32_t tc_off(int row, int k, int kchunks)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __nv_bfloat16 *sW1 = reinterpret_cast<__nv_bfloat16 *>(smem + kSmemW1);
-    __nv_bfloat16 *sW2 = reinterpret_cast<__nv_bfloat16 *>(smem + kSmemW2);
-    float *sb1 = reinterpret_cast<float *>(smem + kSmemF), *sb2 = sb1 + NH, *sW3 = sb2 + NH, *sb3 = sW3 + NH;
-    float *sscale = sb3 + 1;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __nv_bfloat16 *sX = reinterpret_cast<__nv_bfloat16 *>(smem + kSmemX) + warp * 32 * XS;
-    for (int t = threadIdx.x; t < NH * W1S; t += blockDim.x) {
-        const int n = t / W1S, kk = t % W1S;
-        sW1[t] = __float2bfloat16(kk < NIN ? theta[OW1 + n * NIN + kk] : 0.0f);
+    return (uint32_t)(((row >> 3) * kchunks + (k >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+{
+    const uint32_t z = 0;
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                 :
+                 : "r"(dtmem), "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity)
+{
+    for (int it = 0; it < (1 << 22); it++) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(done)
+                     : "r"(bar), "r"(parity)
+                     : "memory");
+        if (done) return true;
     }
-    for (int t = threadIdx.x; t < NH * W2S; t += blockDim.x) {
-        const int n = t / W2S, kk = t % W2S;
-        sW2[t] = __float2bfloat16(kk < NH ? theta[OW2 + n * NH + kk] : 0.0f);
+    return false;
+}
+
+// 64 FP32 accumulators of this thread's TMEM lane, columns [col, col + 64)
+__device__ __forceinline__ void tc_ld64(uint32_t taddr, float (&v)[64])
+{
+    uint32_t r[64];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                 "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, "
+                 "%35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, "
+                 "%56, %57, %58, %59, %60, %61, %62, %63}, [%64];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+                   "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+                   "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+                   "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+                   "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+                   "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+                   "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 64; q++) v[q] = __uint_as_float(r[q]);
+}
+
+template <class R>
+__global__ void __launch_bounds__(kTcThreads, 1) k_closure_coef_tc(const R *__restrict__ X, Geom g, double dx,
+                                                                   double dy, const float *__restrict__ theta,
+                                                                   R *__restrict__ coef, int *err)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint32_t s_taddr;
+    float *sb1 = reinterpret_cast<float *>(smem + kTcF), *sb2 = sb1 + 64, *sW3 = sb2 + 64, *sb3 = sW3 + 64;
+    float *sscale = sb3 + 4;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
+    const uint32_t bar = sbase + (uint32_t)kTcBar;
+    // weights -> B operands (rows = output neurons, K-major)
+    for (int t = tid; t < 64 * 16; t += kTcThreads) {
+        const int n = t >> 4, k = t & 15;
+        *reinterpret_cast<__nv_bfloat16 *>(smem + kTcB1 + tc_off(n, k, 2)) =
+            __float2bfloat16(k < NIN ? theta[OW1 + n * NIN + k] : 0.0f);
     }
-    for (int t = threadIdx.x; t < NH; t += blockDim.x) {
+    for (int t = tid; t < 64 * 64; t += kTcThreads) {
+        const int n = t >> 6, k = t & 63;
+        *reinterpret_cast<__nv_bfloat16 *>(smem + kTcB2 + tc_off(n, k, 8)) = __float2bfloat16(theta[OW2 + n * NH + k]);
+    }
+    for (int t = tid; t < 64; t += kTcThreads) {
         sb1[t] = theta[OB1 + t];
         sb2[t] = theta[OB2 + t];
         sW3[t] = theta[OW3 + t];
     }
-    if (threadIdx.x == 0) sb3[0] = theta[OB3];
-    if (threadIdx.x < NIN) sscale[threadIdx.x] = theta[NPARAM + threadIdx.x];
+    if (tid == 0) sb3[0] = theta[OB3];
+    if (tid < NIN) sscale[tid] = theta[NPARAM + tid];
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&s_taddr);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(kTcCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-
-    const int gid = lane >> 2, tig = lane & 3;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t taddr = s_taddr;
+    const uint32_t lane_base = taddr + ((uint32_t)(32 * warp) << 16);
+    const uint64_t dB1 = tc_desc(sbase + (uint32_t)kTcB1, 128, 256);
     const size_t N = (size_t)g.N;
-    const size_t ngroups = (N + 31) / 32;
-    for (size_t grp = blockIdx.x * (size_t)(blockDim.x / 32) + warp; grp < ngroups;
-         grp += (size_t)gridDim.x * (blockDim.x / 32)) {
-        // features of cell grp*32 + lane -> row `lane` of the warp's tile
-        const size_t cell = grp * 32 + lane;
+    const size_t ntiles = (N + 127) / 128;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (size_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const size_t cell = tile * 128 + tid;
         float f[NIN];
         if (cell < N) {
             const int k = (int)(cell % g.Nz), j = (int)((cell / g.Nz) % g.Ny), i = (int)(cell / ((size_t)g.Nz * g.Ny));
@@ -170,69 +244,75 @@ __global__ void __launch_bounds__(kClosureThreads) k_closure_coef(const R *__res
 #pragma unroll
             for (int q = 0; q < NIN; q++) f[q] = 0.0f;
         }
-#pragma unroll
-        for (int q = 0; q < NIN; q += 2)
-            *reinterpret_cast<uint32_t *>(&sX[lane * XS + q]) = pack_bf16(f[q] * sscale[q], f[q + 1] * sscale[q + 1]);
-        *reinterpret_cast<uint32_t *>(&sX[lane * XS + 12]) = 0u;
-        *reinterpret_cast<uint32_t *>(&sX[lane * XS + 14]) = 0u;
-        __syncwarp();
-#pragma unroll
-        for (int half = 0; half < 2; half++) {
-            const __nv_bfloat16 *A = sX + half * 16 * XS;
-            const uint32_t a0 = *reinterpret_cast<const uint32_t *>(&A[gid * XS + 2 * tig]);
-            const uint32_t a1 = *reinterpret_cast<const uint32_t *>(&A[(gid + 8) * XS + 2 * tig]);
-            const uint32_t a2 = *reinterpret_cast<const uint32_t *>(&A[gid * XS + 2 * tig + 8]);
-            const uint32_t a3 = *reinterpret_cast<const uint32_t *>(&A[(gid + 8) * XS + 2 * tig + 8]);
-            // layer 1: 16 x 64 = A (16 x 16) W1^T
-            float h[8][4];
-#pragma unroll
-            for (int nt = 0; nt < 8; nt++) {
-                h[nt][0] = h[nt][1] = h[nt][2] = h[nt][3] = 0.0f;
-                const __nv_bfloat16 *Brow = sW1 + (8 * nt + gid) * W1S;
-                mma_bf16(h[nt], a0, a1, a2, a3, *reinterpret_cast<const uint32_t *>(&Brow[2 * tig]),
-                         *reinterpret_cast<const uint32_t *>(&Brow[2 * tig + 8]));
-                const int n0 = 8 * nt + 2 * tig;
-                h[nt][0] = gelu(h[nt][0] + sb1[n0]);
-                h[nt][1] = gelu(h[nt][1] + sb1[n0 + 1]);
-                h[nt][2] = gelu(h[nt][2] + sb1[n0]);
-                h[nt][3] = gelu(h[nt][3] + sb1[n0 + 1]);
-            }
-            // layer 2: the layer-1 accumulators are the A fragments (k-step s = n-tiles 2s, 2s+1)
-            float o[8][4];
-#pragma unroll
-            for (int nt = 0; nt < 8; nt++) o[nt][0] = o[nt][1] = o[nt][2] = o[nt][3] = 0.0f;
-#pragma unroll
-            for (int s = 0; s < 4; s++) {
-                const uint32_t b0 = pack_bf16(h[2 * s][0], h[2 * s][1]), b1 = pack_bf16(h[2 * s][2], h[2 * s][3]);
-                const uint32_t b2 = pack_bf16(h[2 * s + 1][0], h[2 * s + 1][1]);
-                const uint32_t b3 = pack_bf16(h[2 * s + 1][2], h[2 * s + 1][3]);
-#pragma unroll
-                for (int nt = 0; nt < 8; nt++) {
-                    const __nv_bfloat16 *Brow = sW2 + (8 * nt + gid) * W2S + 16 * s;
-                    mma_bf16(o[nt], b0, b1, b2, b3, *reinterpret_cast<const uint32_t *>(&Brow[2 * tig]),
-                             *reinterpret_cast<const uint32_t *>(&Brow[2 * tig + 8]));
-                }
-            }
-            // layer 3: per-row dot with W3 over this thread's 16 columns, then the 4 threads of the row
-            float r0 = 0.0f, r1 = 0.0f;
-#pragma unroll
-            for (int nt = 0; nt < 8; nt++) {
-                const int n0 = 8 * nt + 2 * tig;
-                r0 += gelu(o[nt][0] + sb2[n0]) * sW3[n0] + gelu(o[nt][1] + sb2[n0 + 1]) * sW3[n0 + 1];
-                r1 += gelu(o[nt][2] + sb2[n0]) * sW3[n0] + gelu(o[nt][3] + sb2[n0 + 1]) * sW3[n0 + 1];
-            }
-            r0 += __shfl_xor_sync(0xffffffffu, r0, 1);
-            r0 += __shfl_xor_sync(0xffffffffu, r0, 2);
-            r1 += __shfl_xor_sync(0xffffffffu, r1, 1);
-            r1 += __shfl_xor_sync(0xffffffffu, r1, 2);
-            if (tig == 0) {
-                const size_t c0 = grp * 32 + half * 16 + gid, c1 = c0 + 8;
-                if (c0 < N) coef[c0] = (R)softplus(r0 + sb3[0]);
-                if (c1 < N) coef[c1] = (R)softplus(r1 + sb3[0]);
-            }
+        {
+            uint4 lo, hi;
+            lo.x = pack_bf16(f[0] * sscale[0], f[1] * sscale[1]);
+            lo.y = pack_bf16(f[2] * sscale[2], f[3] * sscale[3]);
+            lo.z = pack_bf16(f[4] * sscale[4], f[5] * sscale[5]);
+            lo.w = pack_bf16(f[6] * sscale[6], f[7] * sscale[7]);
+            hi.x = pack_bf16(f[8] * sscale[8], f[9] * sscale[9]);
+            hi.y = pack_bf16(f[10] * sscale[10], f[11] * sscale[11]);
+            hi.z = 0u;
+            hi.w = 0u;
+            *reinterpret_cast<uint4 *>(smem + kTcA1 + tc_off(tid, 0, 2)) = lo;
+            *reinterpret_cast<uint4 *>(smem + kTcA1 + tc_off(tid, 8, 2)) = hi;
         }
-        __syncwarp();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) {
+            tc_mma(taddr, tc_desc(sbase + (uint32_t)kTcA1, 128, 256), dB1, 0u);
+            tc_commit(bar);
+        }
+        ok = __syncthreads_and(tc_wait(bar, phase) ? 1 : 0);
+        phase ^= 1u;
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        float acc[64];
+        tc_ld64(lane_base, acc);
+        // layer-1 epilogue: GELU(h + b1) -> A operand of layer 2 (row tid)
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            uint4 w;
+            w.x = pack_bf16(gelu(acc[8 * c + 0] + sb1[8 * c + 0]), gelu(acc[8 * c + 1] + sb1[8 * c + 1]));
+            w.y = pack_bf16(gelu(acc[8 * c + 2] + sb1[8 * c + 2]), gelu(acc[8 * c + 3] + sb1[8 * c + 3]));
+            w.z = pack_bf16(gelu(acc[8 * c + 4] + sb1[8 * c + 4]), gelu(acc[8 * c + 5] + sb1[8 * c + 5]));
+            w.w = pack_bf16(gelu(acc[8 * c + 6] + sb1[8 * c + 6]), gelu(acc[8 * c + 7] + sb1[8 * c + 7]));
+            *reinterpret_cast<uint4 *>(smem + kTcA2 + tc_off(tid, 8 * c, 8)) = w;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) {
+#pragma unroll
+            for (int s = 0; s < 4; s++)
+                tc_mma(taddr + 64, tc_desc(sbase + (uint32_t)kTcA2 + 256u * s, 128, 1024),
+                       tc_desc(sbase + (uint32_t)kTcB2 + 256u * s, 128, 1024), s > 0 ? 1u : 0u);
+            tc_commit(bar);
+        }
+        ok = __syncthreads_and(tc_wait(bar, phase) ? 1 : 0);
+        phase ^= 1u;
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        tc_ld64(lane_base + 64, acc);
+        float o = sb3[0];
+#pragma unroll
+        for (int q = 0; q < 64; q++) o += gelu(acc[q] + sb2[q]) * sW3[q];
+        if (cell < N) coef[cell] = (R)softplus(o);
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();   // TMEM and operands free for the next tile
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     }
+    if (!ok) {
+        // give the MMA group in flight a bounded chance to finish before TMEM is freed
+        tc_wait(bar, phase ^ 1u);
+        if (tid == 0 && err) atomicExch(err, 1);
+    }
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(kTcCols) : "memory");
 }
 
 // ---- training ------------------------------------------------------------------
@@ -327,26 +407,25 @@ __global__ void k_adam(float *theta, float *m, float *v, const float *g, int np,
 int closure_param_count() { return NTOTAL; }
 
 template <class R>
-cudaError_t launch_closure_coef(const R *X, const Geom &g, double dx, double dy, const float *theta, R *coef,
-                                cudaStream_t s)
+cudaError_t launch_closure_coef_tc(const R *X, const Geom &g, double dx, double dy, const float *theta, R *coef,
+                                   int *err, cudaStream_t s)
 {
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_closure_coef<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)kSmemClosure);
+        cudaError_t e = cudaFuncSetAttribute(k_closure_coef_tc<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kSmemTc);
         if (e) return e;
         attr = true;
     }
-    const size_t groups = ((size_t)g.N + 31) / 32;
-    size_t blocks = (groups + (kClosureThreads / 32) - 1) / (kClosureThreads / 32);
-    if (blocks > 148 * 8) blocks = 148 * 8;
-    k_closure_coef<R><<<(unsigned)blocks, kClosureThreads, kSmemClosure, s>>>(X, g, dx, dy, theta, coef);
+    const size_t tiles = ((size_t)g.N + 127) / 128;
+    const size_t blocks = tiles < 148 * 4 ? tiles : 148 * 4;
+    k_closure_coef_tc<R><<<(unsigned)blocks, kTcThreads, kSmemTc, s>>>(X, g, dx, dy, theta, coef, err);
     return cudaGetLastError();
 }
-template cudaError_t launch_closure_coef<float>(const float *, const Geom &, double, double, const float *, float *,
-                                                cudaStream_t);
-template cudaError_t launch_closure_coef<double>(const double *, const Geom &, double, double, const float *,
-                                                 double *, cudaStream_t);
+template cudaError_t launch_closure_coef_tc<float>(const float *, const Geom &, double, double, const float *, float *,
+                                                   int *, cudaStream_t);
+template cudaError_t launch_closure_coef_tc<double>(const double *, const Geom &, double, double, const float *,
+                                                    double *, int *, cudaStream_t);
 
 cudaError_t launch_mlp_grad(const float *theta, const float *xs, const float *ys, const int *idx, int n, float *grad,
                             double *loss, cudaStream_t s)

@@ -151,6 +151,7 @@ struct wf_ctx {
     int nbcfix = 0;
     void *coef = nullptr;    // [N] learned coefficient (stencil precision)
     float *d_theta = nullptr;
+    int *d_closure_err = nullptr;   // raised by the closure kernel on a timed-out tensor-core wait
 };
 
 namespace wfs {
@@ -367,6 +368,7 @@ template <class R> StageArgs<R> stage_args(wf_ctx *c, const void *X, const void 
     a.a_prev = 0.0;
     a.coef = c->closure ? (R *)c->coef : nullptr;
     a.theta = c->d_theta;
+    a.closure_err = c->d_closure_err;
     a.bcfix = c->d_bcfix;
     a.nbcfix = c->nbcfix;
     const double dt = c->P.dt;
@@ -833,6 +835,11 @@ wf_status wf_synchronize(wf_ctx *c)
 {
     if (!c) return WF_ERR_ARG;
     WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->closure && c->d_closure_err) {
+        int herr = 0;
+        WF_TRY_CUDA(cudaMemcpy(&herr, c->d_closure_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (herr) { set_error("wf_synchronize: a closure tensor-core completion wait timed out"); return WF_ERR_CUDA; }
+    }
     return WF_OK;
 }
 
@@ -1117,6 +1124,9 @@ wf_status wf_set_closure(wf_ctx *c, int kind, const float *params)
         if ((st = dev_alloc(c, &p, sizeof(float) * closure_param_count()))) return st;
         c->d_theta = (float *)p;
         if ((st = dev_alloc(c, &c->coef, c->esz * (size_t)c->N))) return st;
+        if ((st = dev_alloc(c, &p, sizeof(int)))) return st;
+        c->d_closure_err = (int *)p;
+        WF_TRY_CUDA(cudaMemset(c->d_closure_err, 0, sizeof(int)));
     }
     WF_TRY_CUDA(cudaMemcpy(c->d_theta, params, sizeof(float) * closure_param_count(), cudaMemcpyHostToDevice));
     c->closure = 1;
@@ -1132,11 +1142,15 @@ wf_status wf_closure_coefficients(wf_ctx *c, const double *y, double *coef)
     wf_status st = put_state(c, in, y);
     if (st) return st;
     cudaError_t e = (c->prec == WF_FP64)
-                        ? launch_closure_coef<double>((const double *)in, c->geom, c->ph.dx, c->ph.dy, c->d_theta,
-                                                      (double *)c->coef, c->stream)
-                        : launch_closure_coef<float>((const float *)in, c->geom, c->ph.dx, c->ph.dy, c->d_theta,
-                                                     (float *)c->coef, c->stream);
+                        ? launch_closure_coef_tc<double>((const double *)in, c->geom, c->ph.dx, c->ph.dy, c->d_theta,
+                                                         (double *)c->coef, c->d_closure_err, c->stream)
+                        : launch_closure_coef_tc<float>((const float *)in, c->geom, c->ph.dx, c->ph.dy, c->d_theta,
+                                                        (float *)c->coef, c->d_closure_err, c->stream);
     if (e) { set_error("wf_closure_coefficients: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
+    int herr = 0;
+    WF_TRY_CUDA(cudaMemcpyAsync(&herr, c->d_closure_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+    if (herr) { set_error("wf_closure_coefficients: a tensor-core completion wait timed out"); return WF_ERR_CUDA; }
     if (c->prec == WF_FP64) {
         WF_TRY_CUDA(cudaMemcpyAsync(coef, c->coef, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
         WF_TRY_CUDA(cudaStreamSynchronize(c->stream));

@@ -108,6 +108,7 @@ struct StageArgs {
     // learned closure (closure.cu): when coef is set, mu_sgs = rho coef Delta^2 |S|
     R *coef;               // [N] coefficient of the stage input, written before the stage
     const float *theta;    // closure parameters on the device
+    int *closure_err;      // set by the closure kernel when a tensor-core wait times out
     const int *bcfix;      // columns whose cut node or top the fused pass leaves to k_stage_bc
     int nbcfix;
 };
@@ -115,8 +116,8 @@ struct StageArgs {
 // Learned closure (closure.cu).
 int closure_param_count();
 template <class R>
-cudaError_t launch_closure_coef(const R *X, const Geom &g, double dx, double dy, const float *theta, R *coef,
-                                cudaStream_t s);
+cudaError_t launch_closure_coef_tc(const R *X, const Geom &g, double dx, double dy, const float *theta, R *coef,
+                                   int *err, cudaStream_t s);
 cudaError_t launch_mlp_grad(const float *theta, const float *xs, const float *ys, const int *idx, int n, float *grad,
                             double *loss, cudaStream_t s);
 cudaError_t launch_adam(float *theta, float *m, float *v, const float *g, int step, float lr, cudaStream_t s);
