@@ -146,10 +146,13 @@ def test_full_size_flat_one_step_matches_oracle():
         assert np.max(np.abs(p - po)) <= 1e-10 * max(np.max(np.abs(po)), 1e-30)
 
 
-@pytest.mark.parametrize("nx,ny", [(512, 9), (9, 512), (96, 160), (192, 256), (128, 65), (33, 17)])
+@pytest.mark.parametrize("nx,ny", [(512, 9), (9, 512), (96, 160), (192, 256), (128, 65), (33, 17),
+                                   (1025, 5), (5, 1001), (1701, 5), (5, 2049), (4, 7)])
 def test_pressure_fft_lengths_match_oracle(nx, ny, params_from_text):
     """Transform lengths Nx-1, Ny-1 of every workload (511, 95, 159, 191, 255,
-    127, 64, 32, 16) through the pressure solve, against the oracle."""
+    127, 64, 32, 16) and the extremes of the FFT engine (1024 direct, 1000 and
+    1700 by Bluestein with inner lengths 2048 and 4096, 2048 direct, 3 and 6)
+    through the pressure solve, against the oracle."""
     from wildfires_b200 import configs
     case = configs.flat(Nx=nx, Ny=ny, Nz=8, Nt=1, jitter=0.3, seed=nx + ny)
     P = params_from_text(configs.param_text(case.params))
