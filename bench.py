@@ -328,7 +328,7 @@ def run_ours(args):
     ms = max_over_ranks(ms)
     ms_step = ms / K
     value = cells * K * world / (ms * 1e-3) / 1e6
-    launches = sol.launches_per_step() * K
+    launches = sol.launches_per_step() * K * world   # all ranks' kernels in the timed region
 
     # per-kernel device times (eager launches with events on the solver stream)
     prof = sol.profile(2)
@@ -417,8 +417,9 @@ def run_ours(args):
 
     out = None
     if rank == 0:
-        cpu = None if args.no_cpu else cpu_reference_sample(args.config)
-        if cpu is None and not args.no_cpu:
+        # the CPU baseline is a single-GPU figure: sampled on rank 0 of a 1-GPU run only
+        cpu = None if (args.no_cpu or world > 1) else cpu_reference_sample(args.config)
+        if cpu is None and not args.no_cpu and world == 1:
             cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "reference",
                    "sample": "reference host build not available on this machine"}
         out = {
