@@ -1,14 +1,15 @@
 // fft.cuh -- batched FP64 complex FFT lines in shared memory for sm_100a.
 //
-// A block of 256 threads transforms LB lines of length M = 2^L at once.  Each
-// line belongs to T = M/16 threads (T = 1 for M < 16); thread (q, jj) with
-// q = tid % LB (the line) and jj = tid / LB holds 16 complex values in
-// registers per stage.  The transform is a Stockham auto-sort FFT with radix-16
-// stages and one final radix-2/4/8 stage when L is not a multiple of 4, so a
-// 1024-point line takes three passes through shared memory instead of five.
+// A block of 256 threads transforms LB lines of length M = 2^L at once.  With
+// largest radix RM (8 or 16), each line belongs to T = M/RM threads (T = 1 for
+// M < RM); thread (q, jj) with q = tid % LB (the line) and jj = tid / LB holds
+// RM complex values in registers per stage.  The transform is a Stockham
+// auto-sort FFT with radix-RM stages and one final smaller power-of-two stage
+// when L is not a multiple of log2(RM): a 1024-point line takes three passes
+// through shared memory at radix 16, four at radix 8 (with half the registers).
 //
 // Shared-memory layout: element i of line q sits at q*LS + pad(i) with
-// pad(i) = i + i/16 (one spare slot per 16).  The padding makes the stride-16
+// pad(i) = i + i/RM (one spare slot per RM).  The padding makes the stride-RM
 // Stockham writes of the first stage conflict-free; the line stride LS is
 // chosen so that the 8 lanes of one 128-byte shared-memory phase (8 lines at
 // the same position when LB >= 8, otherwise LB lines x 8/LB positions) fall in
@@ -27,18 +28,20 @@
 namespace wf {
 namespace fft {
 
-template <int L>
+// RM: the largest radix (8 or 16); each thread holds RM complex values per stage.
+template <int L, int RM = 16>
 struct Shape {
     static constexpr int M = 1 << L;
-    static constexpr int T = (M >= 16) ? M / 16 : 1;       // threads per line
+    static constexpr int T = (M >= RM) ? M / RM : 1;       // threads per line
     static constexpr int LB = 256 / T;                     // lines per block
-    static constexpr int MP = M + M / 16;                  // padded line length
+    static constexpr int MP = M + M / RM;                  // padded line length
     static constexpr int C = (LB >= 8) ? 1 : 8 / LB;       // wanted LS mod 8
     static constexpr int LS = MP + (((C % 8) - (MP % 8)) + 8) % 8;
     static constexpr size_t smem_bytes = (size_t)LB * LS * 16;
 };
 
-__device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
+// padded position of element i: one spare slot after every RM elements
+template <int RM = 16> __device__ __forceinline__ int pad(int i) { return i + (RM == 16 ? (i >> 4) : (i >> 3)); }
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b)
 {
@@ -129,15 +132,16 @@ __device__ __forceinline__ void dft(double2 (&v)[R])
 }
 
 // One Stockham stage with Ns = 2^SL, followed by the remaining stages.
-template <int L, int SL, bool FIRST, class Pre, class Post>
+template <int L, int RM, int SL, bool FIRST, class Pre, class Post>
 __device__ __forceinline__ void stage(double2 *buf, int jj, const double2 *__restrict__ tw, Pre &pre, Post &post)
 {
     constexpr int M = 1 << L;
     constexpr int REM = L - SL;
-    constexpr int LR = (REM >= 4) ? 4 : REM;
+    constexpr int LRM = (RM == 16) ? 4 : 3;
+    constexpr int LR = (REM >= LRM) ? LRM : REM;
     constexpr int R = 1 << LR;
     constexpr bool LAST = (REM == LR);
-    constexpr int T = Shape<L>::T;
+    constexpr int T = Shape<L, RM>::T;
     constexpr int NB = (M / R) / T;
     constexpr int Ns = 1 << SL;
     double2 v[NB][R];
@@ -148,7 +152,7 @@ __device__ __forceinline__ void stage(double2 *buf, int jj, const double2 *__res
         for (int r = 0; r < R; r++) {
             const int idx = j + r * (M / R);
             if constexpr (FIRST) v[b][r] = pre(idx);
-            else v[b][r] = buf[pad(idx)];
+            else v[b][r] = buf[pad<RM>(idx)];
         }
     }
     __syncthreads();
@@ -180,12 +184,12 @@ __device__ __forceinline__ void stage(double2 *buf, int jj, const double2 *__res
         for (int r = 0; r < R; r++) {
             const int o = base + (r << SL);
             if constexpr (LAST) post(o, v[b][out_slot<R>(r)]);
-            else buf[pad(o)] = v[b][out_slot<R>(r)];
+            else buf[pad<RM>(o)] = v[b][out_slot<R>(r)];
         }
     }
     if constexpr (!LAST) {
         __syncthreads();
-        stage<L, SL + LR, false>(buf, jj, tw, pre, post);
+        stage<L, RM, SL + LR, false>(buf, jj, tw, pre, post);
     }
 }
 
@@ -193,10 +197,10 @@ __device__ __forceinline__ void stage(double2 *buf, int jj, const double2 *__res
 // call it (it synchronises the block).  pre is read once per element in the
 // first stage after which a block barrier follows, so pre may read buf; post is
 // called once per element after the last barrier, so it may write buf.
-template <int L, class Pre, class Post>
+template <int L, int RM, class Pre, class Post>
 __device__ __forceinline__ void run(double2 *buf, int jj, const double2 *__restrict__ tw, Pre pre, Post post)
 {
-    stage<L, 0, true>(buf, jj, tw, pre, post);
+    stage<L, RM, 0, true>(buf, jj, tw, pre, post);
 }
 
 }  // namespace fft

@@ -39,7 +39,15 @@ using fft::cadd;
 using fft::cconj;
 using fft::cmul;
 using fft::csub;
-using fft::pad;
+// Largest FFT radix per kernel: each thread of a line holds this many complex
+// values per stage.  Radix 8 (no spills at 128 registers) measured faster for
+// the x transforms and the inverse y transform; the source kernel, which holds
+// more live values while it fills the lines, keeps radix 16.  Radix 8 needs
+// M/8 threads per line, so lines of 4096 keep radix 16 (256 threads).
+constexpr int kRadixRhs = 16;
+constexpr int kRadixFft = 8;
+template <int L, int RB> constexpr int kRad = (L >= 12) ? 16 : RB;
+template <int L, int RB> __device__ __forceinline__ int padl(int i) { return fft::pad<kRad<L, RB>>(i); }
 
 // Poisson source at (i, j, k), k < Nz-1 (pressure.cu:37-95 and 150-321).
 template <class R>
@@ -142,11 +150,11 @@ __device__ double poisson_source(const PoissonArgs<R> &a, int i, int j, int k)
 // the inverse FFT taken as conj(FFT(conj(.))).  pre(idx) supplies x[idx] for
 // idx < n and post(idx, X) receives X[idx] for idx < n.  INV selects
 // exp(+2 pi i jk/n), unnormalised.  pre may read buf and post may write it.
-template <int L, bool INV, class Pre, class Post>
+template <int L, bool INV, int RB, class Pre, class Post>
 __device__ __forceinline__ void line_dft(const FftDesc &d, double2 *buf, int jj, Pre pre, Post post)
 {
     if (!d.bluestein) {
-        fft::run<L>(
+        fft::run<L, kRad<L, RB>>(
             buf, jj, d.tw,
             [&](int idx) {
                 const double2 v = pre(idx);
@@ -158,7 +166,7 @@ __device__ __forceinline__ void line_dft(const FftDesc &d, double2 *buf, int jj,
     const int n = d.n;
     const double2 *__restrict__ chirp = d.chirp;
     const double2 *__restrict__ filt = d.filt;
-    fft::run<L>(
+    fft::run<L, kRad<L, RB>>(
         buf, jj, d.tw,
         [&](int idx) {
             double2 v = make_double2(0.0, 0.0);
@@ -169,11 +177,11 @@ __device__ __forceinline__ void line_dft(const FftDesc &d, double2 *buf, int jj,
             }
             return v;
         },
-        [&](int idx, double2 v) { buf[pad(idx)] = cconj(cmul(v, __ldg(filt + idx))); });
+        [&](int idx, double2 v) { buf[padl<L, RB>(idx)] = cconj(cmul(v, __ldg(filt + idx))); });
     __syncthreads();
     constexpr double inv_m = 1.0 / (double)(1 << L);
-    fft::run<L>(
-        buf, jj, d.tw, [&](int idx) { return buf[pad(idx)]; },
+    fft::run<L, kRad<L, RB>>(
+        buf, jj, d.tw, [&](int idx) { return buf[padl<L, RB>(idx)]; },
         [&](int idx, double2 v) {
             if (idx < n) {
                 v = cmul(make_double2(v.x * inv_m, -v.y * inv_m), __ldg(chirp + idx));
@@ -188,7 +196,7 @@ __device__ __forceinline__ void line_dft(const FftDesc &d, double2 *buf, int jj,
 template <int L, class R>
 __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_rhs_ffty(const PoissonArgs<R> a)
 {
-    using SH = fft::Shape<L>;
+    using SH = fft::Shape<L, kRad<L, kRadixRhs>>;
     constexpr int LB = SH::LB, LS = SH::LS;
     extern __shared__ double2 smem[];
     const Geom &g = a.g;
@@ -203,14 +211,14 @@ __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_rhs_ffty(const Poisson
         double val = 0.0;
         if (kk < nk) val = poisson_source(a, i, jj, kk);
         else if (kk == nk) val = a.p[((size_t)i * g.Ny + jj) * g.Nz + (g.Nz - 1)];
-        Ad[2 * ((q >> 1) * LS + pad(jj)) + (q & 1)] = val;
+        Ad[2 * ((q >> 1) * LS + padl<L, kRadixRhs>(jj)) + (q & 1)] = val;
     }
     __syncthreads();
     {
         const int q = threadIdx.x % LB, jj = threadIdx.x / LB;
         double2 *buf = smem + q * LS;
-        line_dft<L, false>(
-            a.fy, buf, jj, [&](int idx) { return buf[pad(idx)]; }, [&](int idx, double2 v) { buf[pad(idx)] = v; });
+        line_dft<L, false, kRadixRhs>(
+            a.fy, buf, jj, [&](int idx) { return buf[padl<L, kRadixRhs>(idx)]; }, [&](int idx, double2 v) { buf[padl<L, kRadixRhs>(idx)] = v; });
     }
     __syncthreads();
     // split each packed transform into the two half spectra
@@ -218,8 +226,8 @@ __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_rhs_ffty(const Poisson
     for (int t = threadIdx.x; t < kp * h1; t += 256) {
         const int line = t / h1, s = t - line * h1;
         const double2 *Rb = smem + line * LS;
-        const double2 Zs = Rb[pad(s)];
-        const double2 Zc = cconj(Rb[pad(s == 0 ? 0 : n1 - s)]);
+        const double2 Zs = Rb[padl<L, kRadixRhs>(s)];
+        const double2 Zc = cconj(Rb[padl<L, kRadixRhs>(s == 0 ? 0 : n1 - s)]);
         const double2 Fa = make_double2(0.5 * (Zs.x + Zc.x), 0.5 * (Zs.y + Zc.y));
         const double2 Fb = make_double2(0.5 * (Zs.y - Zc.y), -0.5 * (Zs.x - Zc.x));
         const int kk0 = 2 * (pair0 + line);
@@ -233,14 +241,14 @@ __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_rhs_ffty(const Poisson
 template <int L, bool INV>
 __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_fftx(double2 *__restrict__ G, const FftDesc fx, int n0, int h1)
 {
-    using SH = fft::Shape<L>;
+    using SH = fft::Shape<L, kRad<L, kRadixFft>>;
     extern __shared__ double2 smem[];
     const int q = threadIdx.x % SH::LB, jj = threadIdx.x / SH::LB;
     const int s = blockIdx.y * SH::LB + q;
     const bool act = s < h1;
     double2 *buf = smem + q * SH::LS;
     double2 *g = G + (size_t)blockIdx.x * n0 * h1 + (act ? s : 0);
-    line_dft<L, INV>(
+    line_dft<L, INV, kRadixFft>(
         fx, buf, jj, [&](int idx) { return act ? g[(size_t)idx * h1] : make_double2(0.0, 0.0); },
         [&](int idx, double2 v) {
             if (act) g[(size_t)idx * h1] = v;
@@ -321,7 +329,7 @@ __global__ void __launch_bounds__(128, 8) k_p_tridiag(double2 *__restrict__ G, c
 template <int L, class R>
 __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_iffty_out(const PoissonArgs<R> a)
 {
-    using SH = fft::Shape<L>;
+    using SH = fft::Shape<L, kRad<L, kRadixFft>>;
     constexpr int LB = SH::LB, LS = SH::LS;
     extern __shared__ double2 smem[];
     const Geom &g = a.g;
@@ -350,14 +358,14 @@ __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_iffty_out(const Poisso
             }
             val = make_double2(Fa.x - Fb.y, Fa.y + Fb.x);
         }
-        smem[line * LS + pad(s)] = val;
+        smem[line * LS + padl<L, kRadixFft>(s)] = val;
     }
     __syncthreads();
     {
         const int q = threadIdx.x % LB, jj = threadIdx.x / LB;
         double2 *buf = smem + q * LS;
-        line_dft<L, true>(
-            a.fy, buf, jj, [&](int idx) { return buf[pad(idx)]; }, [&](int idx, double2 v) { buf[pad(idx)] = v; });
+        line_dft<L, true, kRadixFft>(
+            a.fy, buf, jj, [&](int idx) { return buf[padl<L, kRadixFft>(idx)]; }, [&](int idx, double2 v) { buf[padl<L, kRadixFft>(idx)] = v; });
     }
     __syncthreads();
     const double norm = (double)n0 * (double)n1;
@@ -367,7 +375,7 @@ __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_iffty_out(const Poisso
         const int jj = t / ns, q = t - jj * ns;
         const int kk = 2 * pair0 + q;
         if (kk >= nk) continue;
-        const double2 zv = smem[(q >> 1) * LS + pad(jj)];
+        const double2 zv = smem[(q >> 1) * LS + padl<L, kRadixFft>(jj)];
         const double val = ((q & 1) ? zv.y : zv.x) / norm;
         p[((size_t)i * Ny + jj) * Nz + kk] = val;
         if (jj == 0) p[((size_t)i * Ny + (Ny - 1)) * Nz + kk] = val;
@@ -412,7 +420,7 @@ template <class R>
 struct LaunchP1 {
     template <int L> static cudaError_t go(const PoissonArgs<R> &a, cudaStream_t &s)
     {
-        using SH = fft::Shape<L>;
+        using SH = fft::Shape<L, kRad<L, kRadixRhs>>;
         const int np = (a.g.Nz - 1 + 2) / 2;
         k_p_rhs_ffty<L, R><<<dim3(a.g.Nx - 1, (np + SH::LB - 1) / SH::LB), 256, SH::smem_bytes, s>>>(a);
         return cudaSuccess;
@@ -422,7 +430,7 @@ template <class R>
 struct LaunchP5 {
     template <int L> static cudaError_t go(const PoissonArgs<R> &a, cudaStream_t &s)
     {
-        using SH = fft::Shape<L>;
+        using SH = fft::Shape<L, kRad<L, kRadixFft>>;
         const int np = (a.g.Nz - 1 + 1) / 2;
         k_p_iffty_out<L, R><<<dim3(a.g.Nx - 1, (np + SH::LB - 1) / SH::LB), 256, SH::smem_bytes, s>>>(a);
         return cudaSuccess;
@@ -433,7 +441,7 @@ struct LaunchFx {
     template <int L> static cudaError_t go(double2 *const &G, const FftDesc &fx, const int &nslices, const int &n0,
                                            const int &h1, cudaStream_t &s)
     {
-        using SH = fft::Shape<L>;
+        using SH = fft::Shape<L, kRad<L, kRadixFft>>;
         k_p_fftx<L, INV><<<dim3(nslices, (h1 + SH::LB - 1) / SH::LB), 256, SH::smem_bytes, s>>>(G, fx, n0, h1);
         return cudaSuccess;
     }
@@ -442,9 +450,10 @@ struct LaunchFx {
 template <class R, int L>
 cudaError_t set_attributes_for()
 {
-    const int b = (int)fft::Shape<L>::smem_bytes;
+    const int b1 = (int)fft::Shape<L, kRad<L, kRadixRhs>>::smem_bytes;
+    const int b = (int)fft::Shape<L, kRad<L, kRadixFft>>::smem_bytes;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_p_rhs_ffty<L, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_p_rhs_ffty<L, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, b1))) return e;
     if ((e = cudaFuncSetAttribute(k_p_iffty_out<L, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
     if ((e = cudaFuncSetAttribute(k_p_fftx<L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
     if ((e = cudaFuncSetAttribute(k_p_fftx<L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
