@@ -58,6 +58,14 @@ __device__ __forceinline__ float rpow(float x, float y) { return powf(x, y); }
 __device__ __forceinline__ double rfabs(double x) { return fabs(x); }
 __device__ __forceinline__ float rfabs(float x) { return fabsf(x); }
 
+// Packed FP32 pairs (sm_100 FFMA2 / FMUL2 / FADD2): the stencil arithmetic of
+// two fields in one instruction.  Each lane is rounded like the scalar form.
+__device__ __forceinline__ float2 bcast(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+
 // Van Driest damping f_w = 1 - exp(-z+ / A_VD).  Below the cut-off the
 // exponential is smaller than half an ulp of 1 and the result is exactly 1.
 __device__ __forceinline__ double van_driest(double x) { return x < -37.5 ? 1.0 : 1.0 - exp(x); }
@@ -213,11 +221,15 @@ __global__ void __launch_bounds__(128) k_utau(const StageArgs<R> a)
 // (ii, jj, kk) in [-2, T+1] for the state and [-1, T] for the rest.  Both
 // arrays are stored j-fastest with a row stride of TJ+4: a warp covering
 // 8 consecutive k x 4 consecutive j then touches 32 distinct banks (FP32).
+// In FP32 the state is stored as two arrays of pairs, (u, v) and (w, T), so
+// one 8-byte load brings two fields and the pair arithmetic runs on FFMA2;
+// each half-warp (4 k x 4 j) of an 8-byte load then covers the 16 bank pairs.
 // The fuel fraction is read from global memory where a column has fuel.
 template <class R, int TI, int TJ, int KZ> struct Tile {
     static constexpr int SI = TI + 4, SJ = TJ + 4, SK = KZ + 4, SR = SI * SJ * SK;
     static constexpr int GI = TI + 2, GJ = TJ + 2, GK = KZ + 2, GJP = SJ, GR = GI * GK * GJP;
     static constexpr int ZS = SJ;   // z stride of the state tile
+    static constexpr bool PAIRED = sizeof(R) == 4;
     static constexpr int NCOL = GI * GJ, CELLS = TI * TJ * KZ;
     static constexpr size_t up16(size_t b) { return (b + 15) / 16 * 16; }
     static constexpr size_t O_KR = up16(sizeof(R) * 4 * (size_t)SR);
@@ -246,7 +258,14 @@ template <class R, int TI, int TJ, int KZ> struct Tile {
     __device__ static int s(int ii, int jj, int kk) { return ((ii + 2) * SK + (kk + 2)) * SJ + (jj + 2); }
     __device__ static int q(int ii, int jj, int kk) { return ((ii + 1) * GK + (kk + 1)) * GJP + (jj + 1); }
     __device__ static int cq(int ii, int jj) { return (ii + 1) * GJ + (jj + 1); }
-    __device__ R &S(int f, int ii, int jj, int kk) { return st[f * SR + s(ii, jj, kk)]; }
+    // position of field f at tile offset sidx: pairs (u, v), (w, T) in FP32, planar in FP64
+    __device__ static int so(int f, int sidx) { return PAIRED ? (f >> 1) * 2 * SR + 2 * sidx + (f & 1) : f * SR + sidx; }
+    __device__ R &S(int f, int ii, int jj, int kk) { return st[so(f, s(ii, jj, kk))]; }
+    // pair pr (0: u, v; 1: w, T), FP32 only
+    __device__ float2 P(int pr, int ii, int jj, int kk) const
+    {
+        return reinterpret_cast<const float2 *>(st)[pr * SR + s(ii, jj, kk)];
+    }
     __device__ R &G(int f, int ii, int jj, int kk) { return gs[f * GR + q(ii, jj, kk)]; }
     __device__ R K(int kk, int e) const { return kr[(kk + 1) * KROW + e]; }
 };
@@ -292,7 +311,7 @@ __device__ __forceinline__ void issue_tile(const StageArgs<R> &a, TL &t, int i0,
         const bool ok = gk >= 0 && gk < Nz && i0 + ii <= Nx + 1 && j0 + jj <= Ny + 1;
         const size_t o = ok ? ((size_t)wrap_p(i0 + ii, Nx - 1) * Ny + wrap_p(j0 + jj, Ny - 1)) * Nz + gk : 0;
 #pragma unroll
-        for (int f = 0; f < 4; f++) cp_async<sizeof(R)>(t.st + f * TL::SR + TL::s(ii, jj, kk), X + (size_t)f * N + o, ok);
+        for (int f = 0; f < 4; f++) cp_async<sizeof(R)>(t.st + TL::so(f, TL::s(ii, jj, kk)), X + (size_t)f * N + o, ok);
     }
     cp_async_commit();
 }
@@ -369,24 +388,26 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
         //        Enumerated so that each warp covers 8 consecutive k x 4 j where
         //        it can: tile columns k0-1..k0+6, tile columns k0+7..k0+8,
         //        x-side columns, y-side columns.
-        static_assert(KZ == 8, "phase-2 enumeration assumes 8 planes per tile");
+        //        In the 8-plane groups the lanes of a warp are 4 j (fastest) x 8 k.
+        static_assert(KZ == 8 && TJ % 4 == 0 && NT % 32 == 0, "phase-2/3 enumeration: 8 planes, 4-column lane groups");
         constexpr int NA1 = TI * TJ * 8, NA2 = TI * TJ * 2, NB = 2 * TJ * KZ, NC = TI * 2 * KZ;
+        static_assert(NA1 % 32 == 0 && NA2 % 32 == 0, "warp-aligned groups");
         for (int c = threadIdx.x; c < NA1 + NA2 + NB + NC; c += NT) {
             int ii, jj, kk;
             if (c < NA1) {
-                kk = c % 8 - 1;
-                jj = (c / 8) % TJ;
-                ii = c / (8 * TJ);
+                kk = ((c & 31) >> 2) - 1;
+                jj = ((c >> 5) % (TJ / 4)) * 4 + (c & 3);
+                ii = (c >> 5) / (TJ / 4);
             } else if (c < NA1 + NA2) {
                 const int d = c - NA1;
-                kk = 7 + d % 2;
-                jj = (d / 2) % TJ;
+                jj = d % TJ;
+                kk = 7 + (d / TJ) % 2;
                 ii = d / (2 * TJ);
             } else if (c < NA1 + NA2 + NB) {
                 const int d = c - NA1 - NA2;
-                kk = d % KZ;
-                jj = (d / KZ) % TJ;
-                ii = (d / (KZ * TJ)) ? TI : -1;
+                kk = (d & 31) >> 2;
+                jj = ((d >> 5) % (TJ / 4)) * 4 + (d & 3);
+                ii = ((d >> 5) / (TJ / 4)) ? TI : -1;
             } else {
                 const int d = c - NA1 - NA2 - NB;
                 kk = d % KZ;
@@ -395,46 +416,76 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
             }
             const int gk = k0 + kk;
             if (gk < 0 || gk >= Nz || i0 + ii > Nx || j0 + jj > Ny) continue;
-            const R *pu = &t.S(0, ii, jj, 0), *pv = &t.S(1, ii, jj, 0), *pw = &t.S(2, ii, jj, 0), *pT = &t.S(3, ii, jj, 0);
-            const R ux = (t.S(0, ii + 1, jj, kk) - t.S(0, ii - 1, jj, kk)) * p.inv2dx;
-            const R uy = (t.S(0, ii, jj + 1, kk) - t.S(0, ii, jj - 1, kk)) * p.inv2dy;
-            const R vx = (t.S(1, ii + 1, jj, kk) - t.S(1, ii - 1, jj, kk)) * p.inv2dx;
-            const R vy = (t.S(1, ii, jj + 1, kk) - t.S(1, ii, jj - 1, kk)) * p.inv2dy;
-            const R wx = (t.S(2, ii + 1, jj, kk) - t.S(2, ii - 1, jj, kk)) * p.inv2dx;
-            const R wy = (t.S(2, ii, jj + 1, kk) - t.S(2, ii, jj - 1, kk)) * p.inv2dy;
-            constexpr int ZS = TL::ZS;
-            const R Tc = pT[kk * ZS];
-            const R Txp = t.S(3, ii + 1, jj, kk), Txm = t.S(3, ii - 1, jj, kk);
-            const R Typ = t.S(3, ii, jj + 1, kk), Tym = t.S(3, ii, jj - 1, kk);
-            const R Tx = (Txp - Txm) * p.inv2dx, Ty = (Typ - Tym) * p.inv2dy;
-            const R Txx = (Txp - R(2) * Tc + Txm) * p.invdx2, Tyy = (Typ - R(2) * Tc + Tym) * p.invdy2;
-            R uz, vz, wz, Tz, Tzz;
-            if (gk > 0 && gk < Nz - 1) {
-                const R wc = t.K(kk, RD1);
-                uz = (pu[(kk + 1) * ZS] - pu[(kk - 1) * ZS]) * wc;
-                vz = (pv[(kk + 1) * ZS] - pv[(kk - 1) * ZS]) * wc;
-                wz = (pw[(kk + 1) * ZS] - pw[(kk - 1) * ZS]) * wc;
-                Tz = (pT[(kk + 1) * ZS] - pT[(kk - 1) * ZS]) * wc;
-                Tzz = t.K(kk, RD2) * pT[(kk - 1) * ZS] + t.K(kk, RD2 + 1) * Tc + t.K(kk, RD2 + 2) * pT[(kk + 1) * ZS];
+            R ux, uy, uz, vx, vy, vz, wx, wy, wz, Tc, Tx, Ty, Tz, Txx, Tyy, Tzz;
+            bool zdone = false;
+            if constexpr (TL::PAIRED) {
+                const float2 UVxp = t.P(0, ii + 1, jj, kk), UVxm = t.P(0, ii - 1, jj, kk);
+                const float2 UVyp = t.P(0, ii, jj + 1, kk), UVym = t.P(0, ii, jj - 1, kk);
+                const float2 WTxp = t.P(1, ii + 1, jj, kk), WTxm = t.P(1, ii - 1, jj, kk);
+                const float2 WTyp = t.P(1, ii, jj + 1, kk), WTym = t.P(1, ii, jj - 1, kk);
+                const float2 i2x = bcast(p.inv2dx), i2y = bcast(p.inv2dy);
+                const float2 dUVx = mul2(sub2(UVxp, UVxm), i2x), dUVy = mul2(sub2(UVyp, UVym), i2y);
+                const float2 dWTx = mul2(sub2(WTxp, WTxm), i2x), dWTy = mul2(sub2(WTyp, WTym), i2y);
+                ux = dUVx.x; vx = dUVx.y; wx = dWTx.x; Tx = dWTx.y;
+                uy = dUVy.x; vy = dUVy.y; wy = dWTy.x; Ty = dWTy.y;
+                Tc = t.P(1, ii, jj, kk).y;
+                Txx = (WTxp.y - R(2) * Tc + WTxm.y) * p.invdx2;
+                Tyy = (WTyp.y - R(2) * Tc + WTym.y) * p.invdy2;
+                if (gk > 0 && gk < Nz - 1) {
+                    const float2 UVzp = t.P(0, ii, jj, kk + 1), UVzm = t.P(0, ii, jj, kk - 1);
+                    const float2 WTzp = t.P(1, ii, jj, kk + 1), WTzm = t.P(1, ii, jj, kk - 1);
+                    const float2 wc = bcast(t.K(kk, RD1));
+                    const float2 dUVz = mul2(sub2(UVzp, UVzm), wc), dWTz = mul2(sub2(WTzp, WTzm), wc);
+                    uz = dUVz.x; vz = dUVz.y; wz = dWTz.x; Tz = dWTz.y;
+                    Tzz = t.K(kk, RD2) * WTzm.y + t.K(kk, RD2 + 1) * Tc + t.K(kk, RD2 + 2) * WTzp.y;
+                    zdone = true;
+                }
             } else {
+                Tc = t.S(3, ii, jj, kk);
+                ux = (t.S(0, ii + 1, jj, kk) - t.S(0, ii - 1, jj, kk)) * p.inv2dx;
+                uy = (t.S(0, ii, jj + 1, kk) - t.S(0, ii, jj - 1, kk)) * p.inv2dy;
+                vx = (t.S(1, ii + 1, jj, kk) - t.S(1, ii - 1, jj, kk)) * p.inv2dx;
+                vy = (t.S(1, ii, jj + 1, kk) - t.S(1, ii, jj - 1, kk)) * p.inv2dy;
+                wx = (t.S(2, ii + 1, jj, kk) - t.S(2, ii - 1, jj, kk)) * p.inv2dx;
+                wy = (t.S(2, ii, jj + 1, kk) - t.S(2, ii, jj - 1, kk)) * p.inv2dy;
+                const R Txp = t.S(3, ii + 1, jj, kk), Txm = t.S(3, ii - 1, jj, kk);
+                const R Typ = t.S(3, ii, jj + 1, kk), Tym = t.S(3, ii, jj - 1, kk);
+                Tx = (Txp - Txm) * p.inv2dx;
+                Ty = (Typ - Tym) * p.inv2dy;
+                Txx = (Txp - R(2) * Tc + Txm) * p.invdx2;
+                Tyy = (Typ - R(2) * Tc + Tym) * p.invdy2;
+                if (gk > 0 && gk < Nz - 1) {
+                    const R wc = t.K(kk, RD1);
+                    uz = (t.S(0, ii, jj, kk + 1) - t.S(0, ii, jj, kk - 1)) * wc;
+                    vz = (t.S(1, ii, jj, kk + 1) - t.S(1, ii, jj, kk - 1)) * wc;
+                    wz = (t.S(2, ii, jj, kk + 1) - t.S(2, ii, jj, kk - 1)) * wc;
+                    Tz = (t.S(3, ii, jj, kk + 1) - t.S(3, ii, jj, kk - 1)) * wc;
+                    Tzz = t.K(kk, RD2) * t.S(3, ii, jj, kk - 1) + t.K(kk, RD2 + 1) * Tc + t.K(kk, RD2 + 2) * t.S(3, ii, jj, kk + 1);
+                    zdone = true;
+                }
+            }
+            if (!zdone) {
                 // walls: one-sided stencils from the double table (planes k = 0 and Nz-1 only)
                 const double *zc = g.zc;
                 const bool bot = (gk == 0);
-                auto d1 = [&](const R *f) -> R {
-                    if (bot) return (R)zc[ZF0 * Nz] * f[kk * ZS] + (R)zc[ZF1 * Nz] * f[(kk + 1) * ZS] + (R)zc[ZF2 * Nz] * f[(kk + 2) * ZS];
-                    return (R)zc[ZB0 * Nz + gk] * f[(kk - 2) * ZS] + (R)zc[ZB1 * Nz + gk] * f[(kk - 1) * ZS] + (R)zc[ZB2 * Nz + gk] * f[kk * ZS];
+                auto d1 = [&](int f) -> R {
+                    if (bot)
+                        return (R)zc[ZF0 * Nz] * t.S(f, ii, jj, kk) + (R)zc[ZF1 * Nz] * t.S(f, ii, jj, kk + 1) +
+                               (R)zc[ZF2 * Nz] * t.S(f, ii, jj, kk + 2);
+                    return (R)zc[ZB0 * Nz + gk] * t.S(f, ii, jj, kk - 2) + (R)zc[ZB1 * Nz + gk] * t.S(f, ii, jj, kk - 1) +
+                           (R)zc[ZB2 * Nz + gk] * t.S(f, ii, jj, kk);
                 };
-                uz = d1(pu);
-                vz = d1(pv);
-                wz = d1(pw);
-                Tz = d1(pT);
+                uz = d1(0);
+                vz = d1(1);
+                wz = d1(2);
+                Tz = d1(3);
                 // the backward 4-point form needs k-3, inside the tile unless the
                 // top plane is alone in its tile (then no cell of this tile needs it)
-                const R m3 = (kk >= 1) ? pT[(kk - 3) * ZS] : R(0), p3 = (kk <= KZ - 2) ? pT[(kk + 3) * ZS] : R(0);
-                Tzz = bot ? (R)zc[ZFF0 * Nz] * Tc + (R)zc[ZFF1 * Nz] * pT[(kk + 1) * ZS] + (R)zc[ZFF2 * Nz] * pT[(kk + 2) * ZS] +
-                                (R)zc[ZFF3 * Nz] * p3
-                          : (R)zc[ZBB0 * Nz + gk] * m3 + (R)zc[ZBB1 * Nz + gk] * pT[(kk - 2) * ZS] +
-                                (R)zc[ZBB2 * Nz + gk] * pT[(kk - 1) * ZS] + (R)zc[ZBB3 * Nz + gk] * Tc;
+                const R m3 = (kk >= 1) ? t.S(3, ii, jj, kk - 3) : R(0), p3 = (kk <= KZ - 2) ? t.S(3, ii, jj, kk + 3) : R(0);
+                Tzz = bot ? (R)zc[ZFF0 * Nz] * Tc + (R)zc[ZFF1 * Nz] * t.S(3, ii, jj, kk + 1) +
+                                (R)zc[ZFF2 * Nz] * t.S(3, ii, jj, kk + 2) + (R)zc[ZFF3 * Nz] * p3
+                          : (R)zc[ZBB0 * Nz + gk] * m3 + (R)zc[ZBB1 * Nz + gk] * t.S(3, ii, jj, kk - 2) +
+                                (R)zc[ZBB2 * Nz + gk] * t.S(3, ii, jj, kk - 1) + (R)zc[ZBB3 * Nz + gk] * Tc;
             }
             const R rho = fdiv(p.Trho, Tc);
             const R S11 = third(R(2) * ux) - third(vy + wz);
@@ -455,7 +506,7 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
                                       (Tc * p.inv_Trho_cp) +
                                   p.H_C_cp * Yv * K_T);
             } else {
-                const Thermo<R> th = thermo(p, smu, sk, Tc, pT[(kk + 1) * ZS], Yq, gk, nzy, Tx, Ty, Tz,
+                const Thermo<R> th = thermo(p, smu, sk, Tc, t.S(3, ii, jj, kk + 1), Yq, gk, nzy, Tx, Ty, Tz,
                                             Txx + Tyy + Tzz, t.K(kk, RDZ), rho);
                 g7 = fdiv(th.nu * th.T_RHS_tmp, Tc);
             }
@@ -480,7 +531,8 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
         const R an = (R)a.a_next;
         const bool rd = stage_reads_acc(a.method, a.stage), kp = stage_keeps_acc(a.method, a.stage);
         for (int c = threadIdx.x; c < TL::CELLS; c += NT) {
-            const int kk = c % KZ, jj = (c / KZ) % TJ, ii = c / (KZ * TJ);
+            // lanes: 4 j (fastest) x 8 k, as in phase 2
+            const int kk = (c & 31) >> 2, jj = ((c >> 5) % (TJ / 4)) * 4 + (c & 3), ii = (c >> 5) / (TJ / 4);
             const int gi = i0 + ii, gj = j0 + jj, gk = k0 + kk;
             if (gi >= Nx || gj >= Ny || gk >= Nz) continue;
             const int col = gi * Ny + gj;
@@ -520,51 +572,106 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
             if (live) {
                 const R *kmw = &t.kr[(kk + 1) * KROW + RKM], *kpw = &t.kr[(kk + 1) * KROW + RKP];
                 const R d2m = t.K(kk, RD2), d20 = t.K(kk, RD2 + 1), d2p = t.K(kk, RD2 + 2);
-                const R u = t.S(0, ii, jj, kk), v = t.S(1, ii, jj, kk), w = t.S(2, ii, jj, kk), T = t.S(3, ii, jj, kk);
-                const R u_plu = rmax(u, R(0)), u_min = rmin(u, R(0));
-                const R v_plu = rmax(v, R(0)), v_min = rmin(v, R(0));
-                const R w_plu = rmax(w, R(0)), w_min = rmin(w, R(0));
-                // advection (upwind) and Laplacian of one field from the shared tile
-                auto adv_lap = [&](int f, R f0, R &adv, R &fxx, R &fyy, R &fzz, R &fx, R &fy, R &fz) {
-                    const R *pc = &t.S(f, ii, jj, 0);
-                    const R xm = t.S(f, ii - 1, jj, kk), xp = t.S(f, ii + 1, jj, kk);
-                    const R xm2 = t.S(f, ii - 2, jj, kk), xp2 = t.S(f, ii + 2, jj, kk);
-                    const R ym = t.S(f, ii, jj - 1, kk), yp = t.S(f, ii, jj + 1, kk);
-                    const R ym2 = t.S(f, ii, jj - 2, kk), yp2 = t.S(f, ii, jj + 2, kk);
-                    constexpr int ZS = TL::ZS;
-                    const R zm2 = pc[(kk - 2) * ZS], zm = pc[(kk - 1) * ZS], zp = pc[(kk + 1) * ZS], zp2 = pc[(kk + 2) * ZS];
-                    const R im = (R(3) * f0 - R(4) * xm + xm2) * p.inv2dx;
-                    const R ip = (R(-3) * f0 + R(4) * xp - xp2) * p.inv2dx;
-                    const R jm = (R(3) * f0 - R(4) * ym + ym2) * p.inv2dy;
-                    const R jp = (R(-3) * f0 + R(4) * yp - yp2) * p.inv2dy;
-                    const R km = dz5(kmw, zm2, zm, f0, zp, zp2), kpv = dz5(kpw, zm2, zm, f0, zp, zp2);
-                    adv = (u_plu * im + u_min * ip) + (v_plu * jm + v_min * jp) + (w_plu * km + w_min * kpv);
-                    fxx = (xp - R(2) * f0 + xm) * p.invdx2;
-                    fyy = (yp - R(2) * f0 + ym) * p.invdy2;
-                    fzz = d2m * zm + d20 * f0 + d2p * zp;
-                    fx = (xp - xm) * p.inv2dx;
-                    fy = (yp - ym) * p.inv2dy;
-                    fz = (zp - zm) * t.K(kk, RD1);
-                };
-                R advT, Txx, Tyy, Tzz, Tx, Ty, Tz;
-                adv_lap(3, T, advT, Txx, Tyy, Tzz, Tx, Ty, Tz);
+                R u, v, w, T;
+                R advU, advV, advW, advT, lapU, lapV, lapW, lapT, Tx, Ty, Tz;
+                if constexpr (TL::PAIRED) {
+                    const float2 UV = t.P(0, ii, jj, kk), WT = t.P(1, ii, jj, kk);
+                    u = UV.x; v = UV.y; w = WT.x; T = WT.y;
+                    // The upwind advection of a field is a weighted sum of its 13
+                    // stencil values and the Laplacian one of 7: with a = max(u,0)/(2dx)
+                    // and b = min(u,0)/(2dx), u+ (3f - 4f_{i-1} + f_{i-2})/(2dx) +
+                    // u- (-3f + 4f_{i+1} - f_{i+2})/(2dx) has weights 3(a-b), -4a, a, 4b, -b;
+                    // in z the two 5-point rows combine as w+ kmw + w- kpw.
+                    const R ax = rmax(u, R(0)) * p.inv2dx, bx = rmin(u, R(0)) * p.inv2dx;
+                    const R ay = rmax(v, R(0)) * p.inv2dy, by = rmin(v, R(0)) * p.inv2dy;
+                    const R wp = rmax(w, R(0)), wm = rmin(w, R(0));
+                    const float2 Cxm = bcast(R(-4) * ax), Cxm2 = bcast(ax), Cxp = bcast(R(4) * bx), Cxp2 = bcast(-bx);
+                    const float2 Cym = bcast(R(-4) * ay), Cym2 = bcast(ay), Cyp = bcast(R(4) * by), Cyp2 = bcast(-by);
+                    const float2 Cz0 = bcast(wp * kmw[0] + wm * kpw[0]), Cz1 = bcast(wp * kmw[1] + wm * kpw[1]);
+                    const float2 Cz3 = bcast(wp * kmw[3] + wm * kpw[3]), Cz4 = bcast(wp * kmw[4] + wm * kpw[4]);
+                    const float2 C0 = bcast(R(3) * (ax - bx) + R(3) * (ay - by) + (wp * kmw[2] + wm * kpw[2]));
+                    const float2 Lx = bcast(p.invdx2), Ly = bcast(p.invdy2), Lzm = bcast(d2m), Lzp = bcast(d2p);
+                    const float2 L0 = bcast(d20 - R(2) * p.invdx2 - R(2) * p.invdy2);
+                    const float2 i2x = bcast(p.inv2dx), i2y = bcast(p.inv2dy), i2z = bcast(t.K(kk, RD1));
+                    auto adv_lap2 = [&](int pr, float2 f0, float2 &adv, float2 &lap, float2 &gx, float2 &gy, float2 &gz) {
+                        const float2 xm = t.P(pr, ii - 1, jj, kk), xp = t.P(pr, ii + 1, jj, kk);
+                        const float2 xm2 = t.P(pr, ii - 2, jj, kk), xp2 = t.P(pr, ii + 2, jj, kk);
+                        const float2 ym = t.P(pr, ii, jj - 1, kk), yp = t.P(pr, ii, jj + 1, kk);
+                        const float2 ym2 = t.P(pr, ii, jj - 2, kk), yp2 = t.P(pr, ii, jj + 2, kk);
+                        const float2 zm2 = t.P(pr, ii, jj, kk - 2), zm = t.P(pr, ii, jj, kk - 1);
+                        const float2 zp = t.P(pr, ii, jj, kk + 1), zp2 = t.P(pr, ii, jj, kk + 2);
+                        float2 s0 = mul2(C0, f0);
+                        s0 = fma2(Cxm, xm, s0);
+                        s0 = fma2(Cxm2, xm2, s0);
+                        s0 = fma2(Cxp, xp, s0);
+                        s0 = fma2(Cxp2, xp2, s0);
+                        s0 = fma2(Cym, ym, s0);
+                        s0 = fma2(Cym2, ym2, s0);
+                        s0 = fma2(Cyp, yp, s0);
+                        s0 = fma2(Cyp2, yp2, s0);
+                        s0 = fma2(Cz0, zm2, s0);
+                        s0 = fma2(Cz1, zm, s0);
+                        s0 = fma2(Cz3, zp, s0);
+                        adv = fma2(Cz4, zp2, s0);
+                        float2 l0 = mul2(L0, f0);
+                        l0 = fma2(Lx, add2(xp, xm), l0);
+                        l0 = fma2(Ly, add2(yp, ym), l0);
+                        l0 = fma2(Lzm, zm, l0);
+                        lap = fma2(Lzp, zp, l0);
+                        gx = mul2(sub2(xp, xm), i2x);
+                        gy = mul2(sub2(yp, ym), i2y);
+                        gz = mul2(sub2(zp, zm), i2z);
+                    };
+                    float2 aUV, lUV, aWT, lWT, gx, gy, gz;
+                    adv_lap2(0, UV, aUV, lUV, gx, gy, gz);
+                    adv_lap2(1, WT, aWT, lWT, gx, gy, gz);
+                    advU = aUV.x; advV = aUV.y; advW = aWT.x; advT = aWT.y;
+                    lapU = lUV.x; lapV = lUV.y; lapW = lWT.x; lapT = lWT.y;
+                    Tx = gx.y; Ty = gy.y; Tz = gz.y;
+                } else {
+                    u = t.S(0, ii, jj, kk); v = t.S(1, ii, jj, kk); w = t.S(2, ii, jj, kk); T = t.S(3, ii, jj, kk);
+                    const R u_plu = rmax(u, R(0)), u_min = rmin(u, R(0));
+                    const R v_plu = rmax(v, R(0)), v_min = rmin(v, R(0));
+                    const R w_plu = rmax(w, R(0)), w_min = rmin(w, R(0));
+                    // advection (upwind) and Laplacian of one field from the shared tile
+                    auto adv_lap = [&](int f, R f0, R &adv, R &lap, R &fx, R &fy, R &fz) {
+                        const R xm = t.S(f, ii - 1, jj, kk), xp = t.S(f, ii + 1, jj, kk);
+                        const R xm2 = t.S(f, ii - 2, jj, kk), xp2 = t.S(f, ii + 2, jj, kk);
+                        const R ym = t.S(f, ii, jj - 1, kk), yp = t.S(f, ii, jj + 1, kk);
+                        const R ym2 = t.S(f, ii, jj - 2, kk), yp2 = t.S(f, ii, jj + 2, kk);
+                        const R zm2 = t.S(f, ii, jj, kk - 2), zm = t.S(f, ii, jj, kk - 1);
+                        const R zp = t.S(f, ii, jj, kk + 1), zp2 = t.S(f, ii, jj, kk + 2);
+                        const R im = (R(3) * f0 - R(4) * xm + xm2) * p.inv2dx;
+                        const R ip = (R(-3) * f0 + R(4) * xp - xp2) * p.inv2dx;
+                        const R jm = (R(3) * f0 - R(4) * ym + ym2) * p.inv2dy;
+                        const R jp = (R(-3) * f0 + R(4) * yp - yp2) * p.inv2dy;
+                        const R km = dz5(kmw, zm2, zm, f0, zp, zp2), kpv = dz5(kpw, zm2, zm, f0, zp, zp2);
+                        adv = (u_plu * im + u_min * ip) + (v_plu * jm + v_min * jp) + (w_plu * km + w_min * kpv);
+                        const R fxx = (xp - R(2) * f0 + xm) * p.invdx2;
+                        const R fyy = (yp - R(2) * f0 + ym) * p.invdy2;
+                        const R fzz = d2m * zm + d20 * f0 + d2p * zp;
+                        lap = fxx + fyy + fzz;
+                        fx = (xp - xm) * p.inv2dx;
+                        fy = (yp - ym) * p.inv2dy;
+                        fz = (zp - zm) * t.K(kk, RD1);
+                    };
+                    R fx, fy, fz;
+                    adv_lap(3, T, advT, lapT, Tx, Ty, Tz);
+                    adv_lap(0, u, advU, lapU, fx, fy, fz);
+                    adv_lap(1, v, advV, lapV, fx, fy, fz);
+                    adv_lap(2, w, advW, lapW, fx, fy, fz);
+                }
                 const R rho = fdiv(p.Trho, T);
                 const Thermo<R> th = thermo(p, smu, sk, T, t.S(3, ii, jj, kk + 1), Yx, gk, nzy, Tx,
-                                            Ty, Tz, Txx + Tyy + Tzz, t.K(kk, RDZ), rho);
+                                            Ty, Tz, lapT, t.K(kk, RDZ), rho);
                 kY = -p.Y_f * th.K_T * th.Y;
                 R kval[4];
                 kval[3] = (a.ph.temperature_convection == 0) ? th.T_RHS_tmp - (u * Tx + v * Ty + w * Tz)
                                                              : th.T_RHS_tmp - advT;
                 const R mod_U = rsqrt_(u * u + v * v + w * w);
-                {
-                    R adv, fxx, fyy, fzz, fx, fy, fz;
-                    adv_lap(0, u, adv, fxx, fyy, fzz, fx, fy, fz);
-                    kval[0] = th.nu * (fxx + fyy + fzz) - adv + (-p.cd * th.Y * mod_U * u);
-                    adv_lap(1, v, adv, fxx, fyy, fzz, fx, fy, fz);
-                    kval[1] = th.nu * (fxx + fyy + fzz) - adv + (-p.cd * th.Y * mod_U * v);
-                    adv_lap(2, w, adv, fxx, fyy, fzz, fx, fy, fz);
-                    kval[2] = th.nu * (fxx + fyy + fzz) - adv + (fdiv(p.g * (rho - p.rho_inf), rho) - p.cd * th.Y * mod_U * w);
-                }
+                kval[0] = th.nu * lapU - advU + (-p.cd * th.Y * mod_U * u);
+                kval[1] = th.nu * lapV - advV + (-p.cd * th.Y * mod_U * v);
+                kval[2] = th.nu * lapW - advW + (fdiv(p.g * (rho - p.rho_inf), rho) - p.cd * th.Y * mod_U * w);
                 // ---- SGS divergence with Van Driest damping (turbulence.cu:255-454)
                 {
                     const R nu = fdiv(p.mu, rho);
@@ -614,7 +721,7 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
                     const R sgs_x = R(-2) * (mu_x * S11 + mu_y * S12 + mu_z * S13 + mu_c * div_S_x) * inv_rho;
                     const R sgs_y = R(-2) * (mu_x * S12 + mu_y * S22 + mu_z * S23 + mu_c * div_S_y) * inv_rho;
                     const R sgs_z = R(-2) * (mu_x * S13 + mu_y * S23 + mu_z * S33 + mu_c * div_S_z) * inv_rho;
-                    const R sgs_q = -fdiv(mu_x * Tx + mu_y * Ty + mu_z * Tz + mu_c * (Txx + Tyy + Tzz), rho * p.Pr);
+                    const R sgs_q = -fdiv(mu_x * Tx + mu_y * Ty + mu_z * Tz + mu_c * lapT, rho * p.Pr);
                     kval[0] += -sgs_x + third(dU_x);
                     kval[1] += -sgs_y + third(dU_y);
                     kval[2] += -sgs_z + third(dU_z);
