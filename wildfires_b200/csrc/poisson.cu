@@ -191,8 +191,10 @@ __device__ __forceinline__ void line_dft(const FftDesc &d, double2 *buf, int jj,
 }
 
 // P1: source + top plane, forward FFT in y of packed slice pairs.  Block
-// (i, pair group): LB complex lines, line q packs slices 2(pair0+q) (real
+// (pair group, i): LB complex lines, line q packs slices 2(pair0+q) (real
 // part) and 2(pair0+q)+1 (imaginary part); slice nk is the top-plane pressure.
+// The pair group is the fast grid index, so the blocks resident at one time
+// read whole z-columns of the same x-plane of the state.
 template <int L, class R>
 __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_rhs_ffty(const PoissonArgs<R> a)
 {
@@ -201,8 +203,8 @@ __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_rhs_ffty(const Poisson
     extern __shared__ double2 smem[];
     const Geom &g = a.g;
     const int n0 = g.Nx - 1, n1 = g.Ny - 1, nk = g.Nz - 1, h1 = a.h1;
-    const int i = blockIdx.x;
-    const int pair0 = blockIdx.y * LB;
+    const int i = blockIdx.y;
+    const int pair0 = blockIdx.x * LB;
     const int nslices = nk + 1;                      // f slices + top-plane pressure
     double *Ad = reinterpret_cast<double *>(smem);
     for (int t = threadIdx.x; t < n1 * 2 * LB; t += 256) {
@@ -422,7 +424,7 @@ struct LaunchP1 {
     {
         using SH = fft::Shape<L, kRad<L, kRadixRhs>>;
         const int np = (a.g.Nz - 1 + 2) / 2;
-        k_p_rhs_ffty<L, R><<<dim3(a.g.Nx - 1, (np + SH::LB - 1) / SH::LB), 256, SH::smem_bytes, s>>>(a);
+        k_p_rhs_ffty<L, R><<<dim3((np + SH::LB - 1) / SH::LB, a.g.Nx - 1), 256, SH::smem_bytes, s>>>(a);
         return cudaSuccess;
     }
 };
