@@ -34,6 +34,7 @@ constexpr double kSigmaSB = 5.670374419e-8;
 #define WF_FFT_MIN_BLOCKS 2
 #endif
 constexpr int kFftMinBlocks = WF_FFT_MIN_BLOCKS;
+int g_poisson_sms = 148;   // multiprocessors of the device, read at set-up (grid of the persistent x-FFT)
 
 using fft::cadd;
 using fft::cconj;
@@ -238,23 +239,63 @@ __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_rhs_ffty(const Poisson
     }
 }
 
-// P2/P4: FFT along x of one slice kk, LB consecutive s per block; the lines
-// are read from and written back to G inside the first and last FFT stages.
+// 16-byte asynchronous copy global -> shared (cp.async, sm_80+ PTX); a
+// source size of 0 writes zeros without reading.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// P2/P4: FFT along x.  A work item is LB consecutive s of one slice kk.  The
+// blocks are persistent and walk the items blockIdx.x, + gridDim.x, ...: the
+// lines of the next item are copied into the second shared buffer while the
+// current item is transformed in place, and the last FFT stage writes the
+// results straight back to G.
 template <int L, bool INV>
-__global__ void __launch_bounds__(256, kFftMinBlocks) k_p_fftx(double2 *__restrict__ G, const FftDesc fx, int n0, int h1)
+__global__ void __launch_bounds__(256, kFftMinBlocks)
+    k_p_fftx(double2 *__restrict__ G, const FftDesc fx, int n0, int h1, int nslices)
 {
     using SH = fft::Shape<L, kRad<L, kRadixFft>>;
+    constexpr int LB = SH::LB, LS = SH::LS;
     extern __shared__ double2 smem[];
-    const int q = threadIdx.x % SH::LB, jj = threadIdx.x / SH::LB;
-    const int s = blockIdx.y * SH::LB + q;
-    const bool act = s < h1;
-    double2 *buf = smem + q * SH::LS;
-    double2 *g = G + (size_t)blockIdx.x * n0 * h1 + (act ? s : 0);
-    line_dft<L, INV, kRadixFft>(
-        fx, buf, jj, [&](int idx) { return act ? g[(size_t)idx * h1] : make_double2(0.0, 0.0); },
-        [&](int idx, double2 v) {
-            if (act) g[(size_t)idx * h1] = v;
-        });
+    const int ngroups = (h1 + LB - 1) / LB;
+    const int nitems = nslices * ngroups;
+    const int q = threadIdx.x % LB, jj = threadIdx.x / LB;
+    // lines of item `it` -> buffer B (zeros for s >= h1)
+    auto fetch = [&](int it, double2 *B) {
+        const int kk = it / ngroups, s0 = (it - kk * ngroups) * LB;
+        const double2 *src = G + (size_t)kk * n0 * h1 + s0;
+        for (int e = threadIdx.x; e < LB * n0; e += 256) {
+            const int l = e % LB, idx = e / LB;
+            const bool ok = s0 + l < h1;
+            cp_async16(B + l * LS + padl<L, kRadixFft>(idx), src + (ok ? (size_t)idx * h1 + l : 0), ok);
+        }
+    };
+    int item = blockIdx.x;
+    if (item < nitems) fetch(item, smem);
+    cp_async_commit();
+    for (int t = 0; item < nitems; item += gridDim.x, t++) {
+        double2 *cur = smem + (t & 1) * (LB * LS);
+        const int next = item + gridDim.x;
+        if (next < nitems) fetch(next, smem + ((t + 1) & 1) * (LB * LS));
+        cp_async_commit();
+        cp_async_wait<1>();   // this item's lines have landed (own copies) ...
+        __syncthreads();      // ... and everyone else's
+        const int kk = item / ngroups, s = (item - kk * ngroups) * LB + q;
+        const bool act = s < h1;
+        double2 *buf = cur + q * LS;
+        double2 *g = G + (size_t)kk * n0 * h1 + (act ? s : 0);
+        line_dft<L, INV, kRadixFft>(
+            fx, buf, jj, [&](int idx) { return buf[padl<L, kRadixFft>(idx)]; },
+            [&](int idx, double2 v) {
+                if (act) g[(size_t)idx * h1] = v;
+            });
+        __syncthreads();      // buffer free before the fetch two items ahead
+    }
+    cp_async_wait<0>();
 }
 
 // P3: tridiagonal solve in z per (r, s) (pressure.cu:356-390, 473-504, 418-443).
@@ -444,7 +485,9 @@ struct LaunchFx {
                                            const int &h1, cudaStream_t &s)
     {
         using SH = fft::Shape<L, kRad<L, kRadixFft>>;
-        k_p_fftx<L, INV><<<dim3(nslices, (h1 + SH::LB - 1) / SH::LB), 256, SH::smem_bytes, s>>>(G, fx, n0, h1);
+        const int nitems = nslices * ((h1 + SH::LB - 1) / SH::LB);
+        const int blocks = min(nitems, kFftMinBlocks * g_poisson_sms);
+        k_p_fftx<L, INV><<<blocks, 256, 2 * SH::smem_bytes, s>>>(G, fx, n0, h1, nslices);
         return cudaSuccess;
     }
 };
@@ -457,15 +500,22 @@ cudaError_t set_attributes_for()
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(k_p_rhs_ffty<L, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, b1))) return e;
     if ((e = cudaFuncSetAttribute(k_p_iffty_out<L, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
-    if ((e = cudaFuncSetAttribute(k_p_fftx<L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
-    if ((e = cudaFuncSetAttribute(k_p_fftx<L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_p_fftx<L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * b))) return e;
+    if ((e = cudaFuncSetAttribute(k_p_fftx<L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * b))) return e;
     if constexpr (L < kMaxL) return set_attributes_for<R, L + 1>();
     return cudaSuccess;
 }
 
 }  // namespace
 
-template <class R> cudaError_t poisson_set_attributes() { return set_attributes_for<R, kMinL>(); }
+template <class R> cudaError_t poisson_set_attributes()
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (!e) e = cudaDeviceGetAttribute(&g_poisson_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (!e) e = set_attributes_for<R, kMinL>();
+    return e;
+}
 template cudaError_t poisson_set_attributes<double>();
 template cudaError_t poisson_set_attributes<float>();
 
