@@ -186,9 +186,10 @@ wf_status wf_pressure(wf_ctx *ctx, const double *y_np1, const double *y_n, doubl
 wf_status wf_rk(wf_ctx *ctx, const double *y_n, double *y_np1);
 
 /* What solve_pressure_iterative reports after the last wf_pressure or step
- * that waited on the host (pressure.cu:596-597): the max-norm change of the
- * last iterate and the iteration count in the reference's convention (the
- * index of the converged iterate, or pressure_solver_iter). */
+ * (pressure.cu:596-597): the max-norm change of the last iterate and the
+ * iteration count in the reference's convention (the index of the converged
+ * iterate, or pressure_solver_iter).  The variable-density loop runs on the
+ * device; this call waits for the context's stream and reads its record. */
 wf_status wf_pressure_report(const wf_ctx *ctx, double *error, int *max_iter);
 
 /* The operator-level entries above use the context's state buffers as

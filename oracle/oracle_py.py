@@ -76,6 +76,16 @@ def pressure(P, y_np1, y_n, p):
     return pp, it
 
 
+def pressure_full(P, y_np1, y_n, p):
+    """pressure() that also returns the last max-norm change: (p, solves, change)."""
+    a = np.ascontiguousarray(y_np1, dtype=np.float64)
+    b = np.ascontiguousarray(y_n, dtype=np.float64)
+    pp = np.array(p, dtype=np.float64, copy=True)
+    err = C.c_double()
+    it = lib().wfo_solve_pressure(_rec(P), _p(a), _p(b), _p(pp), C.byref(err))
+    return pp, it, err.value
+
+
 def project(P, y_np1, y_n, p):
     y1 = np.array(y_np1, dtype=np.float64, copy=True)
     b = np.ascontiguousarray(y_n, dtype=np.float64)

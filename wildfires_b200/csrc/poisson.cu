@@ -542,30 +542,65 @@ cudaError_t launch_poisson_impl(const PoissonArgs<R> &a, const double *zt, cudaS
 template cudaError_t launch_poisson_impl<double>(const PoissonArgs<double> &, const double *, cudaStream_t, cudaEvent_t *);
 template cudaError_t launch_poisson_impl<float>(const PoissonArgs<float> &, const double *, cudaStream_t, cudaEvent_t *);
 
-// ---- max |a - b| reduction (pressure fixed point) ------------------------
+// ---- variable-density fixed point, driven on the device ------------------
+// The loop (pressure.cu:551-606) runs as a CUDA graph WHILE node: its body is
+// one Poisson solve, k_maxdiff_copy and k_piter_next, which sets the node's
+// condition, so no iteration waits for the host.
 namespace {
-__global__ void __launch_bounds__(256) k_maxdiff(const double *__restrict__ a, const double *__restrict__ b, int n,
-                                                  unsigned long long *out)
+__global__ void k_piter_begin(PIterRec *r)
+{
+    r->red = 0ull;
+    r->h = 0.0;
+    r->m = 0;
+    r->done = 0;
+}
+
+__global__ void __launch_bounds__(256) k_maxdiff_copy(const double *__restrict__ a, double *__restrict__ b, int n,
+                                                       unsigned long long *out)
 {
     double m = 0.0;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const double d = fabs(a[t] - b[t]);
+        const double av = a[t];
+        const double d = fabs(av - b[t]);
         m = (d > m || d != d) ? d : m;
+        b[t] = av;
     }
     for (int o = 16; o > 0; o >>= 1) {
         const double v = __shfl_xor_sync(0xffffffffu, m, o);
         m = (v > m || v != v) ? v : m;
     }
-    // non-negative doubles order like their bit patterns; NaN sorts above inf
     if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+__global__ void k_piter_next(PIterRec *r, double tol, int use_tol, int maxit, cudaGraphConditionalHandle cond)
+{
+    const double h = __longlong_as_double((long long)r->red);
+    r->red = 0ull;
+    r->h = h;
+    const int m = r->m + 1;
+    r->m = m;
+    const int done = use_tol && h <= tol;   // NaN never meets the tolerance
+    r->done = done;
+    cudaGraphSetConditional(cond, (!done && m < maxit) ? 1u : 0u);
 }
 }  // namespace
 
-cudaError_t launch_maxdiff(const double *a, const double *b, int n, double *out, cudaStream_t s)
+cudaError_t launch_piter_begin(PIterRec *rec, cudaStream_t s)
 {
-    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double), s);
-    if (e) return e;
-    k_maxdiff<<<592, 256, 0, s>>>(a, b, n, reinterpret_cast<unsigned long long *>(out));
+    k_piter_begin<<<1, 1, 0, s>>>(rec);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_maxdiff_copy(const double *p, double *p_prev, int n, PIterRec *rec, cudaStream_t s)
+{
+    k_maxdiff_copy<<<4 * g_poisson_sms, 256, 0, s>>>(p, p_prev, n, &rec->red);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_piter_next(PIterRec *rec, double tol, int use_tol, int maxit, cudaGraphConditionalHandle cond,
+                              cudaStream_t s)
+{
+    k_piter_next<<<1, 1, 0, s>>>(rec, tol, use_tol, maxit, cond);
     return cudaGetLastError();
 }
 

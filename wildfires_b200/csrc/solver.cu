@@ -129,7 +129,7 @@ struct wf_ctx {
     int cur = 0;
     void *Xa = nullptr, *Xb = nullptr, *acc = nullptr, *utau = nullptr, *bc = nullptr;
     void *Tsrc = nullptr;
-    double *p = nullptr, *p_prev = nullptr, *red = nullptr, *d_diag = nullptr;
+    double *p = nullptr, *p_prev = nullptr, *d_diag = nullptr;
     double2 *G = nullptr;
     double *d_z = nullptr, *d_zc = nullptr, *d_topo = nullptr, *d_kx2 = nullptr, *d_ky2 = nullptr, *d_zt = nullptr;
     double *d_x = nullptr, *d_y = nullptr;
@@ -143,9 +143,16 @@ struct wf_ctx {
     double fuel0 = 0.0;    // fuel integral at upload
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int launches = 0;
-    int last_iters = 0;
-    double last_err = 0.0;   // max |p_m - p_{m-1}| of the last iteration (variable density)
-    int last_ref_iter = 0;   // iteration count as solve_pressure_iterative reports it
+    // variable-density pressure fixed point: device record, the stream the loop
+    // body is captured on, and graphs of the loop alone for steps that are not
+    // replayed from a step graph (keyed by their y_{n+1}, y_n buffers)
+    PIterRec *rec = nullptr;
+    cudaStream_t aux = nullptr;
+    struct PLoop {
+        const void *y1, *yn;
+        cudaGraphExec_t ge;
+    } ploop[4] = {};
+    int ploop_next = 0;
     int closure = 0;         // WF_CLOSURE_SMAGORINSKY / WF_CLOSURE_MLP
     int *d_bcfix = nullptr;  // columns left to k_stage_bc
     int nbcfix = 0;
@@ -158,12 +165,16 @@ namespace wfs {
 
 // Kernel launches of one step: per stage the optional closure inference,
 // k_utau, k_stage_fused and, when some column needs it, k_stage_bc; five
-// pressure kernels per solve; the projection.
+// pressure kernels per solve (variable density: plus the record reset and,
+// per iteration, k_maxdiff_copy and k_piter_next; counted for max_iter
+// iterations, an upper bound when the tolerance ends the loop early); the
+// projection.
 int launches_per_step(const wf_ctx *c)
 {
     const int per_stage = 2 + (c->nbcfix > 0 ? 1 : 0) + (c->closure ? 1 : 0);
-    const int solves = (c->P.variable_density != 0) ? (c->P.pressure_solver_iter > 1 ? c->P.pressure_solver_iter : 1) : 1;
-    return c->nstages * per_stage + 5 * solves + 1;
+    const int maxit = c->P.pressure_solver_iter > 0 ? c->P.pressure_solver_iter : 0;
+    const int pressure = (c->P.variable_density != 0) ? 1 + 7 * maxit : 5;
+    return c->nstages * per_stage + pressure + 1;
 }
 
 wf_status dev_alloc(wf_ctx *c, void **out, size_t bytes)
@@ -428,46 +439,111 @@ template <class R> wf_status enqueue_stages(wf_ctx *c, void *yn, void *y1)
 
 // Pressure solve(s) for y1 given yn.  For variable density the fixed point
 // stops on the max-norm change; that decision is taken on the host.
-template <class R> wf_status enqueue_pressure(wf_ctx *c, const void *y1, const void *yn, bool fixed_only, int *iters)
+// Capture the variable-density fixed point (pressure.cu:551-606) into the
+// stream's capture: p_prev = p, reset of the device record, then a WHILE node
+// whose body (captured on c->aux) is one Poisson solve, the max-norm change
+// with p_prev = p, and k_piter_next, which ends the loop once the change meets
+// the tolerance or maxit solves are done.
+template <class R> wf_status capture_pressure_loop(wf_ctx *c, const PoissonArgs<R> &a, cudaStream_t s)
+{
+    const int maxit = c->P.pressure_solver_iter;
+    const double tol = c->P.pressure_solver_tol;
+    WF_TRY_CUDA(cudaMemcpyAsync(c->p_prev, c->p, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, s));
+    WF_TRY_CUDA(launch_piter_begin(c->rec, s));
+    if (maxit <= 0) return WF_OK;   // the reference's loop body does not run
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    WF_TRY_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) { set_error("pressure loop: stream is not capturing"); return WF_ERR_CUDA; }
+    cudaGraphConditionalHandle cond;
+    WF_TRY_CUDA(cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+    np.conditional.handle = cond;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    WF_TRY_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
+    WF_TRY_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    WF_TRY_CUDA(cudaStreamBeginCaptureToGraph(c->aux, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = launch_poisson_impl<R>(a, c->d_zt, c->aux);
+    if (!e) e = launch_maxdiff_copy(c->p, c->p_prev, c->N, c->rec, c->aux);
+    if (!e) e = launch_piter_next(c->rec, tol, tol >= 0 ? 1 : 0, maxit, cond, c->aux);
+    cudaGraph_t captured = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(c->aux, &captured);
+    if (e || e2) {
+        set_error("pressure loop body capture failed: %s", cudaGetErrorString(e ? e : e2));
+        return WF_ERR_CUDA;
+    }
+    return WF_OK;
+}
+
+// Pressure solve of one step.  Constant density: one solve.  Variable density:
+// the fixed point runs on the device (see capture_pressure_loop); inside a
+// step capture it becomes part of the step graph, otherwise a graph of the loop
+// alone is built once per (y1, yn) pair and launched.
+template <class R> wf_status enqueue_pressure(wf_ctx *c, const void *y1, const void *yn)
 {
     cudaStream_t s = c->stream;
     const PoissonArgs<R> a = poisson_args<R>(c, y1, yn);
     if (c->P.variable_density == 0) {
         WF_TRY_CUDA(launch_poisson_impl<R>(a, c->d_zt, s));
-        if (iters) *iters = 1;
         return WF_OK;
     }
-    const int maxit = c->P.pressure_solver_iter;
-    const bool use_tol = !fixed_only && c->P.pressure_solver_tol >= 0;
-    int m = 0;
-    bool converged = false;
-    double h = 0;
-    for (m = 0; m < maxit; m++) {
-        // the change of the last iterate is measured whenever the host waits anyway
-        const bool measure = use_tol || (!fixed_only && m == maxit - 1);
-        if (measure) WF_TRY_CUDA(cudaMemcpyAsync(c->p_prev, c->p, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, s));
-        WF_TRY_CUDA(launch_poisson_impl<R>(a, c->d_zt, s));
-        if (measure) {
-            WF_TRY_CUDA(launch_maxdiff(c->p, c->p_prev, c->N, c->red, s));
-            WF_TRY_CUDA(cudaMemcpyAsync(&h, c->red, sizeof(double), cudaMemcpyDeviceToHost, s));
-            WF_TRY_CUDA(cudaStreamSynchronize(s));
-            if (use_tol && h <= c->P.pressure_solver_tol) { converged = true; break; }
+    cudaStreamCaptureStatus cs;
+    WF_TRY_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (cs == cudaStreamCaptureStatusActive) return capture_pressure_loop<R>(c, a, s);
+    cudaGraphExec_t ge = nullptr;
+    for (auto &pl : c->ploop)
+        if (pl.ge && pl.y1 == y1 && pl.yn == yn) ge = pl.ge;
+    if (!ge) {
+        cudaGraph_t gph = nullptr;
+        WF_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        wf_status st = capture_pressure_loop<R>(c, a, s);
+        cudaError_t e = cudaStreamEndCapture(s, &gph);
+        if (st) {
+            if (gph) cudaGraphDestroy(gph);
+            return st;
         }
+        if (e != cudaSuccess) { set_error("pressure loop capture failed: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
+        e = cudaGraphInstantiate(&ge, gph, 0);
+        cudaGraphDestroy(gph);
+        if (e != cudaSuccess) { set_error("pressure loop instantiate failed: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
+        auto &slot = c->ploop[c->ploop_next];
+        c->ploop_next = (c->ploop_next + 1) % 4;
+        if (slot.ge) cudaGraphExecDestroy(slot.ge);
+        slot = {y1, yn, ge};
     }
-    if (!fixed_only) {
-        c->last_err = h;
-        c->last_ref_iter = converged ? m : maxit;   // pressure.cu:564-600 reports the breaking index
-    }
-    if (iters) *iters = converged ? m + 1 : m;
+    WF_TRY_CUDA(cudaGraphLaunch(ge, s));
     return WF_OK;
 }
 
-template <class R> wf_status enqueue_step(wf_ctx *c, int cur, int n1, bool fixed_only)
+// Iterations of the last variable-density pressure solve as the device record
+// holds them (waits for the stream): solves done, last max-norm change, and
+// the count solve_pressure_iterative reports (pressure.cu:564-600: the index of
+// the breaking iteration, else max_iter).
+wf_status read_piter(wf_ctx *c, int *solves, double *err, int *ref_iter)
+{
+    PIterRec r;
+    memset(&r, 0, sizeof(r));
+    if (c->P.variable_density != 0) {
+        WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+        WF_TRY_CUDA(cudaMemcpy(&r, c->rec, sizeof(r), cudaMemcpyDeviceToHost));
+    }
+    if (solves) *solves = (c->P.variable_density != 0) ? r.m : 1;
+    if (err) *err = r.h;
+    if (ref_iter) *ref_iter = (c->P.variable_density == 0) ? 0 : (r.done ? r.m - 1 : c->P.pressure_solver_iter);
+    return WF_OK;
+}
+
+template <class R> wf_status enqueue_step(wf_ctx *c, int cur, int n1)
 {
     void *yn = c->ybuf[cur], *y1 = c->ybuf[1 - cur];
     wf_status st = enqueue_stages<R>(c, yn, y1);
     if (st) return st;
-    if ((st = enqueue_pressure<R>(c, y1, yn, fixed_only, &c->last_iters))) return st;
+    if ((st = enqueue_pressure<R>(c, y1, yn))) return st;
     ProjectArgs<R> pa;
     memset(&pa, 0, sizeof(pa));
     pa.g = c->geom;
@@ -490,10 +566,9 @@ template <class R> wf_status enqueue_step(wf_ctx *c, int cur, int n1, bool fixed
     return WF_OK;
 }
 
-wf_status enqueue_step_any(wf_ctx *c, int cur, int n1, bool fixed_only)
+wf_status enqueue_step_any(wf_ctx *c, int cur, int n1)
 {
-    return c->prec == WF_FP64 ? enqueue_step<double>(c, cur, n1, fixed_only)
-                              : enqueue_step<float>(c, cur, n1, fixed_only);
+    return c->prec == WF_FP64 ? enqueue_step<double>(c, cur, n1) : enqueue_step<float>(c, cur, n1);
 }
 
 // A step can be replayed from a graph when its launch sequence does not depend
@@ -501,9 +576,7 @@ wf_status enqueue_step_any(wf_ctx *c, int cur, int n1, bool fixed_only)
 bool step_is_static(const wf_ctx *c, int n1)
 {
     double sc;
-    if (source_mode(c, n1, &sc) != 0) return false;
-    if (c->P.variable_density != 0 && c->P.pressure_solver_tol >= 0) return false;
-    return true;
+    return source_mode(c, n1, &sc) == 0;
 }
 
 template <class R> __global__ void k_to_prec(R *dst, const double *src, size_t n)
@@ -703,7 +776,12 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
     if ((st = dev_alloc(c, (void **)&c->p, sizeof(double) * c->N))) return fail(st);
     if ((st = dev_alloc(c, (void **)&c->p_prev, sizeof(double) * c->N))) return fail(st);
     if ((st = dev_alloc(c, (void **)&c->G, sizeof(double2) * (size_t)Nz * (Nx - 1) * c->h1))) return fail(st);
-    if ((st = dev_alloc(c, (void **)&c->red, 64))) return fail(st);
+    if ((st = dev_alloc(c, (void **)&c->rec, sizeof(PIterRec)))) return fail(st);
+    WF_TRY_CUDA(cudaMemset(c->rec, 0, sizeof(PIterRec)));
+    if (cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error("wf_create: stream creation failed");
+        return fail(WF_ERR_CUDA);
+    }
     if ((st = dev_alloc(c, (void **)&c->d_diag, diag_scratch_bytes()))) return fail(st);
     // tables
     std::vector<double> zc = zcoef_table(c->P, c->hz.data()), zt = tridiag_table(c->P, c->hz.data());
@@ -766,7 +844,10 @@ wf_status wf_destroy(wf_ctx *c)
     if (!c) return WF_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     drop_graphs(c);
+    for (auto &pl : c->ploop)
+        if (pl.ge) cudaGraphExecDestroy(pl.ge);
     for (auto &b : c->bufs) cudaFree(b.p);
+    if (c->aux) cudaStreamDestroy(c->aux);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return WF_OK;
@@ -812,7 +893,7 @@ wf_status wf_step(wf_ctx *c, int nsteps)
             if (!ge) {
                 cudaGraph_t gph;
                 WF_TRY_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-                wf_status st = enqueue_step_any(c, c->cur, n1, true);
+                wf_status st = enqueue_step_any(c, c->cur, n1);
                 cudaError_t e = cudaStreamEndCapture(c->stream, &gph);
                 if (st) return st;
                 if (e != cudaSuccess) { set_error("wf_step: capture failed: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
@@ -822,7 +903,7 @@ wf_status wf_step(wf_ctx *c, int nsteps)
             }
             WF_TRY_CUDA(cudaGraphLaunch(ge, c->stream));
         } else {
-            wf_status st = enqueue_step_any(c, c->cur, n1, false);
+            wf_status st = enqueue_step_any(c, c->cur, n1);
             if (st) return st;
         }
         c->cur = 1 - c->cur;
@@ -953,9 +1034,10 @@ wf_status wf_pressure(wf_ctx *c, const double *y_np1, const double *y_n, double 
     if (st) return st;
     if ((st = put_state(c, bn, y_n))) return st;
     WF_TRY_CUDA(cudaMemcpyAsync(c->p, pr, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
-    int it = 0;
-    st = (c->prec == WF_FP64) ? enqueue_pressure<double>(c, b1, bn, false, &it) : enqueue_pressure<float>(c, b1, bn, false, &it);
+    st = (c->prec == WF_FP64) ? enqueue_pressure<double>(c, b1, bn) : enqueue_pressure<float>(c, b1, bn);
     if (st) return st;
+    int it = 1;
+    if ((st = read_piter(c, &it, nullptr, nullptr))) return st;
     WF_TRY_CUDA(cudaMemcpyAsync(pr, c->p, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
     WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
     if (iters) *iters = it;
@@ -968,8 +1050,7 @@ wf_status wf_pressure(wf_ctx *c, const double *y_np1, const double *y_n, double 
 // its own (the members' streams fork from and join back to one stream), so the
 // GPU runs the members' kernels concurrently and one graph launch replaces
 // 18 launches per member.  Members whose step is not static (ignition source
-// active, host-checked pressure tolerance) are enqueued eagerly on their own
-// streams instead.
+// active) are enqueued eagerly on their own streams instead.
 }  // extern "C"
 
 struct wf_ensemble {
@@ -992,13 +1073,13 @@ void ensemble_drop_graphs(wf_ensemble *e)
         }
 }
 
-wf_status ensemble_enqueue(wf_ensemble *e, bool fixed_only)
+wf_status ensemble_enqueue(wf_ensemble *e)
 {
     WF_TRY_CUDA(cudaEventRecord(e->fork, e->master));
     for (size_t i = 0; i < e->m.size(); i++) {
         wf_ctx *c = e->m[i];
         WF_TRY_CUDA(cudaStreamWaitEvent(c->stream, e->fork, 0));
-        wf_status st = enqueue_step_any(c, c->cur, c->n + 1, fixed_only);
+        wf_status st = enqueue_step_any(c, c->cur, c->n + 1);
         if (st) return st;
         WF_TRY_CUDA(cudaEventRecord(e->join[i], c->stream));
         WF_TRY_CUDA(cudaStreamWaitEvent(e->master, e->join[i], 0));
@@ -1074,7 +1155,7 @@ wf_status wf_ensemble_step(wf_ensemble *e, int nsteps)
             if (!ge) {
                 cudaGraph_t gph;
                 WF_TRY_CUDA(cudaStreamBeginCapture(e->master, cudaStreamCaptureModeThreadLocal));
-                wf_status st = ensemble_enqueue(e, true);
+                wf_status st = ensemble_enqueue(e);
                 cudaError_t err = cudaStreamEndCapture(e->master, &gph);
                 if (st) return st;
                 if (err != cudaSuccess) { set_error("wf_ensemble_step: capture failed: %s", cudaGetErrorString(err)); return WF_ERR_CUDA; }
@@ -1084,7 +1165,7 @@ wf_status wf_ensemble_step(wf_ensemble *e, int nsteps)
             }
             WF_TRY_CUDA(cudaGraphLaunch(ge, e->master));
         } else {
-            wf_status st = ensemble_enqueue(e, false);
+            wf_status st = ensemble_enqueue(e);
             if (st) return st;
         }
         for (wf_ctx *c : e->m) {
@@ -1265,9 +1346,7 @@ wf_status wf_mlp_train(float *theta, const float *x, const float *y, size_t n, i
 wf_status wf_pressure_report(const wf_ctx *c, double *error, int *max_iter)
 {
     if (!c) { set_error("wf_pressure_report: null context"); return WF_ERR_ARG; }
-    if (error) *error = c->last_err;
-    if (max_iter) *max_iter = c->last_ref_iter;
-    return WF_OK;
+    return read_piter(const_cast<wf_ctx *>(c), nullptr, error, max_iter);
 }
 
 wf_status wf_rk(wf_ctx *c, const double *y_n, double *y_np1)

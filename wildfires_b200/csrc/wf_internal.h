@@ -182,6 +182,22 @@ constexpr int kMaxZUnknowns = 256;      // longest supported tridiagonal system 
 // Grid-wide FP64 reductions for the diagnostics and the pressure fixed point.
 template <class R>
 cudaError_t launch_diag(const Geom &g, const Phys &ph, const R *y, const R *y0fuel_ref, double *out, cudaStream_t s);
-cudaError_t launch_maxdiff(const double *a, const double *b, int n, double *out, cudaStream_t s);
+// Device record of the variable-density pressure fixed point (one per context):
+// red accumulates max |p - p_prev| of the running iteration as the bits of a
+// non-negative double; h is the change of the last finished iteration, m the
+// iterations finished, done whether the last one met the tolerance.
+struct PIterRec {
+    unsigned long long red;
+    double h;
+    int m;
+    int done;
+};
+cudaError_t launch_piter_begin(PIterRec *rec, cudaStream_t s);
+// max |p - p_prev| into rec->red, then p_prev = p (one pass over both)
+cudaError_t launch_maxdiff_copy(const double *p, double *p_prev, int n, PIterRec *rec, cudaStream_t s);
+// closes an iteration: h, m, done; sets the loop's condition to "another
+// iteration" (not done and m < maxit)
+cudaError_t launch_piter_next(PIterRec *rec, double tol, int use_tol, int maxit, cudaGraphConditionalHandle cond,
+                              cudaStream_t s);
 
 }  // namespace wf
