@@ -62,6 +62,19 @@ typedef struct wf_diag {
     long long nan_count;     /* NaN values found in u, v, w, T, Y */
 } wf_diag;
 
+/* The reference's per-checkpoint report (timestep_reports, functions.cu:82-185),
+ * with its conventions: T and Y ranges only inside the fuel rectangle
+ * [Y0_x_start, Y0_x_end] x [Y0_y_start, Y0_y_end], starting from T_min = 1e9,
+ * T_max = -1e9, Y_min = 0, Y_max = -1e9; Y read for every k < Nz_Y_max.
+ * nan_field is -1, or the field (0 u, 1 v, 2 w, 3 T, 4 Y) of the first NaN in
+ * the reference's scan order (i, j, k, then u, v, w, T, Y) at node
+ * (nan_i, nan_j, nan_k). */
+typedef struct wf_report {
+    double cfl;              /* dt (max|u|/dx + max|v|/dy + max|w|/dz) over all cells */
+    double Y_min, Y_max, T_min, T_max;
+    int nan_field, nan_i, nan_j, nan_k;
+} wf_report;
+
 /* ---- parameters --------------------------------------------------------- */
 
 /* Parse a `key = value` parameter file with the reference's rules
@@ -92,6 +105,15 @@ wf_status wf_load_fields(const Parameters *p, const char *dir, double *y, double
  * reference's raw FP64 format (output.cu:3-44). */
 wf_status wf_save_fields(const Parameters *p, const char *dir, int n, const double *y, const double *pr);
 
+/* save_domain (output.cu:46-81): `<dir>x.bin`, `y.bin`, `z.bin` (FP64 grid
+ * coordinates) and `t.bin` (the times of the saved steps, n % NT == 0 or
+ * n == Nt, for n = 0..Nt). */
+wf_status wf_save_domain(const Parameters *p, const char *dir);
+
+/* save_topography (output.cu:83-99): `<dir>topography.bin` (FP64, Nx*Ny, j
+ * fastest) and `<dir>Nz_Y.bin` (int32, Nx*Ny). */
+wf_status wf_save_topography(const Parameters *p, const char *dir);
+
 /* ---- solver context ----------------------------------------------------- */
 
 /* Create a solver on the current CUDA device for the given record (copied;
@@ -116,6 +138,27 @@ wf_status wf_time(const wf_ctx *ctx, int *n, double *t);
 
 /* FP64 diagnostics of the current state. */
 wf_status wf_diagnostics(wf_ctx *ctx, wf_diag *out);
+
+/* timestep_reports (functions.cu:82-185) of the current state, reduced on the
+ * device: only the report crosses to the host, not the state.  The reference
+ * logs the first NaN and exits; this call reports it (see wf_report) and
+ * returns WF_OK. */
+wf_status wf_timestep_reports(wf_ctx *ctx, wf_report *out);
+
+/* Asynchronous checkpoint of the current state and p as `<dir>u.bin.<n>` ...
+ * `<dir>p.bin.<n>` in the format of save_data (output.cu:3-44; FP64, also for
+ * the FP32 stencil state).  Enqueues one device-to-device snapshot on the
+ * context's stream and returns; the copy to pinned host memory and the file
+ * writes run in the background while later steps run (solver.cu:248-250 copies
+ * and writes before continuing).  Two host buffers: a dump issued while two are
+ * still being written waits for the older one.  The first call allocates the
+ * snapshot (state + p in FP64) and the two pinned host buffers; they are kept
+ * until wf_destroy.  Write errors are returned by the next wf_dump_wait. */
+wf_status wf_dump_async(wf_ctx *ctx, const char *dir, int n);
+
+/* Wait until every dump of the context is written; returns the first error of
+ * those writes, or WF_OK. */
+wf_status wf_dump_wait(wf_ctx *ctx);
 
 /* Device pointers of the current state (precision-dependent element type:
  * double for WF_FP64, float for WF_FP32_STENCIL) and of p (double).  Valid

@@ -106,3 +106,47 @@ def steps(P, y0, p0, nsteps, first=1):
         if rc != 0:
             raise RuntimeError("oracle step failed")
     return y, p
+
+
+def timestep_reports(P, y):
+    """numpy restatement of timestep_reports (src/cu/functions.cu:82-185) on a
+    packed FP64 state: returns (CFL, Y_min, Y_max, T_min, T_max, first_nan),
+    first_nan = None or (field, i, j, k) of the first NaN in the reference's
+    scan order (i, j, k, then u, v, w, T, Y).  T and Y ranges only inside the
+    fuel rectangle [Y0_x_start, Y0_x_end] x [Y0_y_start, Y0_y_end], from the
+    reference's starting values (T: 1e9 / -1e9, Y: 0 / -1e9); Y is read for
+    k < Nz_Y_max (:125-133), velocity maxima start at 0 (:101-103)."""
+    r = P.rec
+    Nx, Ny, Nz, NzY = r.Nx, r.Ny, r.Nz, r.Nz_Y_max
+    N = Nx * Ny * Nz
+    y = np.asarray(y, dtype=np.float64)
+    u, v, w, T = (y[q * N:(q + 1) * N].reshape(Nx, Ny, Nz) for q in range(4))
+    Y = np.zeros((Nx, Ny, Nz))
+    Y[:, :, :NzY] = y[4 * N:4 * N + Nx * Ny * NzY].reshape(Nx, Ny, NzY)
+    flags = np.stack([np.isnan(a) for a in (u, v, w, T, Y)], axis=-1)
+    first = None
+    if flags.any():
+        q = int(np.flatnonzero(flags.reshape(-1))[0])
+        first = (q % 5, q // 5 // (Ny * Nz), (q // 5 // Nz) % Ny, q // 5 % Nz)
+    x = np.ctypeslib.as_array(r.x, shape=(Nx,))
+    yy = np.ctypeslib.as_array(r.y, shape=(Ny,))
+    zx = (r.Y0_x_start <= x) & (x <= r.Y0_x_end)
+    zy = (r.Y0_y_start <= yy) & (yy <= r.Y0_y_end)
+    zone = zx[:, None] & zy[None, :]
+    ok = ~flags.any(axis=-1)
+
+    def ext(a, mask, f, start):
+        vals = a[mask]
+        return f(np.concatenate([[start], vals])) if vals.size else start
+
+    mu = ext(np.abs(u), ok, np.max, 0.0)
+    mv = ext(np.abs(v), ok, np.max, 0.0)
+    mw = ext(np.abs(w), ok, np.max, 0.0)
+    zmask = zone[:, :, None] & ok
+    T_min = ext(T, zmask, np.min, 1e9)
+    T_max = ext(T, zmask, np.max, -1e9)
+    ymask = zmask & (np.arange(Nz) < NzY)[None, None, :]
+    Y_min = ext(Y, ymask, np.min, 0.0)
+    Y_max = ext(Y, ymask, np.max, -1e9)
+    cfl = r.dt * (mu / r.dx + mv / r.dy + mw / r.dz)
+    return cfl, Y_min, Y_max, T_min, T_max, first

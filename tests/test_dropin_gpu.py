@@ -55,8 +55,8 @@ def test_reference_main_links_and_matches(tmp_path, params_from_text):
     from wildfires_b200 import configs
     case = configs.hill(Nx=33, Ny=33, Nz=16, Nt=10, NT=10, L=100.0, H=20.0, jitter=0.2, seed=3)
     P = params_from_text(configs.param_text(case.params))
-    ours, _ = _run(DROPIN, case, tmp_path / "dropin")
-    ref1, _ = _run(REFMAIN, case, tmp_path / "reference1")
+    ours, out_ours = _run(DROPIN, case, tmp_path / "dropin")
+    ref1, out_ref1 = _run(REFMAIN, case, tmp_path / "reference1")
     ref2, _ = _run(REFMAIN, case, tmp_path / "reference2")
     y_o, p_o = _fields(ours, P, 1)
     host = ref_runner.run(case, "step", flavour="host")
@@ -72,3 +72,21 @@ def test_reference_main_links_and_matches(tmp_path, params_from_text):
     # the drop-in reported through the reference's own logging
     log = open(os.path.join(ours, "log.txt")).read()
     assert "Solver time" in log
+    # checkpoint report: the restatement reproduces what the reference program
+    # printed for its own saved state, and the drop-in (device reduction)
+    # prints what the restatement gives for the drop-in's saved state
+    assert _report_lines(out_ref1) == _expected_lines(P, y1)
+    assert _report_lines(out_ours) == _expected_lines(P, y_o)
+
+
+def _report_lines(stdout):
+    keys = ("CFL:", "Temperature:", "Fuel:")
+    return [ln.strip() for ln in stdout.splitlines() if ln.startswith(keys)]
+
+
+def _expected_lines(P, y):
+    import oracle_py as O
+    cfl, Y_min, Y_max, T_min, T_max, first = O.timestep_reports(P, y)
+    assert first is None
+    return ["CFL: %f" % cfl, "Temperature: Min = %.2f, Max = %.2f" % (T_min, T_max),
+            "Fuel: Min = %.2f, Max = %.2f" % (Y_min, Y_max)]

@@ -15,7 +15,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._abi import WF_FP32_STENCIL, WF_FP64, WfDiag, WfError, check, lib
+from ._abi import WF_FP32_STENCIL, WF_FP64, WfDiag, WfError, WfReport, check, lib
 from ._params import Parameters
 
 __all__ = ["Params", "Solver", "Ensemble", "read_parameters", "WfError", "Parameters"]
@@ -81,6 +81,28 @@ def read_parameters(path):
     rec = Parameters()
     check(lib().wf_read_parameters(str(path).encode(), C.byref(rec)), "wf_read_parameters")
     return Params(rec)
+
+
+def _dir(directory):
+    d = str(directory)
+    return (d if d.endswith("/") else d + "/").encode()
+
+
+def save_fields(params, directory, n, y, p):
+    """Write <dir>u.bin.<n> ... p.bin.<n> (reference save_data format)."""
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    p = np.ascontiguousarray(p, dtype=np.float64)
+    check(lib().wf_save_fields(C.byref(params.rec), _dir(directory), int(n), _ptr(y), _ptr(p)), "wf_save_fields")
+
+
+def save_domain(params, directory):
+    """Write <dir>x.bin, y.bin, z.bin, t.bin (reference save_domain format)."""
+    check(lib().wf_save_domain(C.byref(params.rec), _dir(directory)), "wf_save_domain")
+
+
+def save_topography(params, directory):
+    """Write <dir>topography.bin and Nz_Y.bin (reference save_topography format)."""
+    check(lib().wf_save_topography(C.byref(params.rec), _dir(directory)), "wf_save_topography")
 
 
 def load_fields(params, directory):
@@ -156,6 +178,19 @@ class Solver:
         if not (allow_nan and s == 6):
             check(s, "wf_diagnostics")
         return {f: getattr(d, f) for f, _ in WfDiag._fields_}
+
+    def timestep_reports(self):
+        """The reference's checkpoint report (functions.cu:82-185) reduced on the GPU."""
+        r = WfReport()
+        check(lib().wf_timestep_reports(self._h, C.byref(r)), "wf_timestep_reports")
+        return {f: getattr(r, f) for f, _ in WfReport._fields_}
+
+    def dump_async(self, directory, n):
+        """Checkpoint the current state to <dir>*.bin.<n> in the background."""
+        check(lib().wf_dump_async(self._h, _dir(directory), int(n)), "wf_dump_async")
+
+    def dump_wait(self):
+        check(lib().wf_dump_wait(self._h), "wf_dump_wait")
 
     def phi(self, R_old):
         R_old = np.ascontiguousarray(R_old, dtype=np.float64)

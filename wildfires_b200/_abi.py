@@ -26,6 +26,7 @@ EXPORTS = [
     "wf_ensemble_create", "wf_ensemble_destroy", "wf_ensemble_size", "wf_ensemble_member",
     "wf_ensemble_step", "wf_ensemble_synchronize",
     "wf_closure_param_count", "wf_set_closure", "wf_closure_coefficients", "wf_mlp_loss_grad", "wf_mlp_train",
+    "wf_timestep_reports", "wf_dump_async", "wf_dump_wait", "wf_save_domain", "wf_save_topography",
 ]
 
 
@@ -33,6 +34,11 @@ class WfDiag(C.Structure):
     _fields_ = [(n, C.c_double) for n in (
         "mass", "energy", "fuel", "fuel_consumed", "max_abs_u", "max_abs_v", "max_abs_w",
         "cfl", "T_min", "T_max", "Y_min", "Y_max")] + [("nan_count", C.c_longlong)]
+
+
+class WfReport(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("cfl", "Y_min", "Y_max", "T_min", "T_max")] + \
+        [(n, C.c_int) for n in ("nan_field", "nan_i", "nan_j", "nan_k")]
 
 
 class WfError(RuntimeError):
@@ -103,6 +109,11 @@ def lib():
         "wf_mlp_train": (C.c_int, [fp, fp, fp, C.c_size_t, C.c_int, C.c_int, C.c_float, C.c_ulonglong, dp]),
         "wf_pressure_report": (C.c_int, [vp, dp, C.POINTER(C.c_int)]),
         "wf_last_error": (C.c_char_p, []),
+        "wf_timestep_reports": (C.c_int, [vp, C.POINTER(WfReport)]),
+        "wf_dump_async": (C.c_int, [vp, C.c_char_p, C.c_int]),
+        "wf_dump_wait": (C.c_int, [vp]),
+        "wf_save_domain": (C.c_int, [P, C.c_char_p]),
+        "wf_save_topography": (C.c_int, [P, C.c_char_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -14,6 +14,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <vector>
+
 #include "wf_internal.h"
 
 namespace {
@@ -367,6 +369,54 @@ wf_status wf_load_fields(const Parameters *P, const char *dir, double *y, double
         const size_t n = (q == 4) ? NY : N;
         const wf_status st = read_raw(path, dst, n);
         if (st) return st;
+    }
+    return WF_OK;
+}
+
+wf_status wf_save_domain(const Parameters *P, const char *dir)
+{
+    if (!P || !dir || !P->x || !P->y || !P->z) {
+        wf::set_error("wf_save_domain: null argument or record without grid arrays");
+        return WF_ERR_ARG;
+    }
+    const int NT = P->NT > 0 ? P->NT : P->Nt;
+    std::vector<double> ts;
+    for (int n = 0; n <= P->Nt; n++)
+        if (n % NT == 0 || n == P->Nt) ts.push_back(P->t ? P->t[n] : P->t_min + n * P->dt);
+    const double *src[4] = {P->x, P->y, P->z, ts.data()};
+    const size_t cnt[4] = {(size_t)P->Nx, (size_t)P->Ny, (size_t)P->Nz, ts.size()};
+    const char *names[4] = {"x", "y", "z", "t"};
+    for (int q = 0; q < 4; q++) {
+        char path[1024];
+        snprintf(path, sizeof(path), "%s%s.bin", dir, names[q]);
+        const wf_status st = write_raw(path, src[q], cnt[q]);
+        if (st) return st;
+    }
+    return WF_OK;
+}
+
+wf_status wf_save_topography(const Parameters *P, const char *dir)
+{
+    if (!P || !dir || !P->topography || !P->Nz_Y) {
+        wf::set_error("wf_save_topography: null argument or record without terrain arrays");
+        return WF_ERR_ARG;
+    }
+    const size_t n = (size_t)P->Nx * P->Ny;
+    char path[1024];
+    snprintf(path, sizeof(path), "%stopography.bin", dir);
+    wf_status st = write_raw(path, P->topography, n);
+    if (st) return st;
+    snprintf(path, sizeof(path), "%sNz_Y.bin", dir);
+    FILE *f = fopen(path, "wb");
+    if (!f) {
+        wf::set_error("cannot create %s", path);
+        return WF_ERR_IO;
+    }
+    const size_t w = fwrite(P->Nz_Y, sizeof(int), n, f);
+    fclose(f);
+    if (w != n) {
+        wf::set_error("%s: short write", path);
+        return WF_ERR_IO;
     }
     return WF_OK;
 }

@@ -159,6 +159,8 @@ struct wf_ctx {
     void *coef = nullptr;    // [N] learned coefficient (stencil precision)
     float *d_theta = nullptr;
     int *d_closure_err = nullptr;   // raised by the closure kernel on a timed-out tensor-core wait
+    double *d_rep = nullptr;        // checkpoint report scratch
+    Dumper *dump = nullptr;         // asynchronous dumps (created by the first wf_dump_async)
 };
 
 namespace wfs {
@@ -783,6 +785,7 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
         return fail(WF_ERR_CUDA);
     }
     if ((st = dev_alloc(c, (void **)&c->d_diag, diag_scratch_bytes()))) return fail(st);
+    if ((st = dev_alloc(c, (void **)&c->d_rep, report_scratch_bytes()))) return fail(st);
     // tables
     std::vector<double> zc = zcoef_table(c->P, c->hz.data()), zt = tridiag_table(c->P, c->hz.data());
     std::vector<double> kx2(Nx - 1), ky2(Ny - 1);
@@ -843,6 +846,7 @@ wf_status wf_destroy(wf_ctx *c)
 {
     if (!c) return WF_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    dumper_destroy(c->dump);
     drop_graphs(c);
     for (auto &pl : c->ploop)
         if (pl.ge) cudaGraphExecDestroy(pl.ge);
@@ -930,6 +934,51 @@ wf_status wf_time(const wf_ctx *c, int *n, double *t)
     if (n) *n = c->n;
     if (t) *t = c->P.t_min + c->n * c->P.dt;
     return WF_OK;
+}
+
+wf_status wf_timestep_reports(wf_ctx *c, wf_report *out)
+{
+    if (!c || !out) { set_error("wf_timestep_reports: null argument"); return WF_ERR_ARG; }
+    const double rect[4] = {c->P.Y0_x_start, c->P.Y0_x_end, c->P.Y0_y_start, c->P.Y0_y_end};
+    cudaError_t e = (c->prec == WF_FP64)
+                        ? launch_report<double>(c->geom, (const double *)c->ybuf[c->cur], c->d_x, c->d_y, rect, c->d_rep,
+                                                c->stream)
+                        : launch_report<float>(c->geom, (const float *)c->ybuf[c->cur], c->d_x, c->d_y, rect, c->d_rep,
+                                               c->stream);
+    if (e != cudaSuccess) { set_error("wf_timestep_reports: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
+    double h[8];
+    WF_TRY_CUDA(cudaMemcpyAsync(h, c->d_rep, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+    // functions.cu:180, same operation order
+    out->cfl = c->P.dt * (h[0] / c->P.dx + h[1] / c->P.dy + h[2] / c->P.dz);
+    out->T_min = 0.0 - h[3];
+    out->T_max = h[4];
+    out->Y_min = 0.0 - h[5];
+    out->Y_max = h[6];
+    unsigned long long key;
+    memcpy(&key, &h[7], sizeof(key));
+    out->nan_field = out->nan_i = out->nan_j = out->nan_k = -1;
+    if (key != ~0ull) {
+        const unsigned long long cell = key / 5;
+        out->nan_field = (int)(key % 5);
+        out->nan_k = (int)(cell % (unsigned long long)c->Nz);
+        out->nan_j = (int)((cell / c->Nz) % (unsigned long long)c->Ny);
+        out->nan_i = (int)(cell / ((unsigned long long)c->Nz * c->Ny));
+    }
+    return WF_OK;
+}
+
+wf_status wf_dump_async(wf_ctx *c, const char *dir, int n)
+{
+    if (!c || !dir) { set_error("wf_dump_async: null argument"); return WF_ERR_ARG; }
+    if (!c->dump) c->dump = dumper_create(c->device, c->P, c->S, (size_t)c->N);
+    return dumper_enqueue(c->dump, c->stream, c->ybuf[c->cur], c->prec != WF_FP64, c->p, dir, n);
+}
+
+wf_status wf_dump_wait(wf_ctx *c)
+{
+    if (!c) { set_error("wf_dump_wait: null context"); return WF_ERR_ARG; }
+    return dumper_wait(c->dump);
 }
 
 wf_status wf_diagnostics(wf_ctx *c, wf_diag *out)

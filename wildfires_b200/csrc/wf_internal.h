@@ -182,6 +182,22 @@ constexpr int kMaxZUnknowns = 256;      // longest supported tridiagonal system 
 // Grid-wide FP64 reductions for the diagnostics and the pressure fixed point.
 template <class R>
 cudaError_t launch_diag(const Geom &g, const Phys &ph, const R *y, const R *y0fuel_ref, double *out, cudaStream_t s);
+
+// Reference-style checkpoint report (functions.cu:82-185): scratch[0..6] =
+// max|u|, max|v|, max|w|, -T_min, T_max, -Y_min, Y_max (fuel rectangle for T
+// and Y), scratch[7] = first NaN key ((i Ny + j) Nz + k) * 5 + field as bits, or ~0.
+size_t report_scratch_bytes();
+template <class R>
+cudaError_t launch_report(const Geom &g, const R *y, const double *xg, const double *yg, const double rect[4],
+                          double *scratch, cudaStream_t s);
+
+// Asynchronous double-buffered field dumps (dump.cu).
+struct Dumper;
+Dumper *dumper_create(int device, const Parameters &P, size_t S, size_t N);
+wf_status dumper_enqueue(Dumper *d, cudaStream_t s, const void *state, bool fp32, const double *p, const char *dir,
+                         int n);
+wf_status dumper_wait(Dumper *d);
+void dumper_destroy(Dumper *d);
 // Device record of the variable-density pressure fixed point (one per context):
 // red accumulates max |p - p_prev| of the running iteration as the bits of a
 // non-negative double; h is the change of the last finished iteration, m the

@@ -14,14 +14,10 @@
 #include "wf_dropin.h"
 #include "wildfires_b200.h"
 
-// Defined by the caller's reference objects (functions.cu:82, logs.cu,
-// output.cu:3, utils.cu).
-void timestep_reports(double *y_n, double *CFL, double *Y_min, double *Y_max, double *T_min, double *T_max, int n,
-                      Parameters parameters);
+// Defined by the caller's reference objects (logs.cu, utils.cu).
 void log_timestep(Parameters parameters, int n, double t_n, double step_time, double CFL, double T_min,
                   double T_max, double Y_min, double Y_max);
 void log_message(Parameters parameters, const char *message);
-void save_data(double *data, double *p, int n, Parameters parameters);
 void format_seconds(double seconds, char *formatted_time);
 
 namespace {
@@ -178,8 +174,13 @@ void solve_pressure_iterative(double *y_np1, double *y_n, double *p, double *, d
 }
 
 // The time loop of solver.cu:95-265: Nt steps; every NT steps and at the last
-// one the state is reported, logged and saved through the reference's own
-// routines; y_n and p hold the final state on return.
+// one the state is reported, logged and saved.  The report is the reference's
+// timestep_reports computed on the device (wf_timestep_reports: only the
+// report crosses to the host) and logged through the reference's own
+// log_timestep / log_message, including its NaN message and exit; the save is
+// an asynchronous dump in save_data's format (wf_dump_async), written by a
+// host thread while the next steps run.  y_n and p hold the final state on
+// return.
 void solve_PDE(double *y_n, double *p, Parameters parameters)
 {
     const char *env = getenv("WF_PRECISION");
@@ -206,8 +207,25 @@ void solve_PDE(double *y_n, double *p, Parameters parameters)
         cum_step_time += step_time;
         if (n % log_every == 0) printf("Time step: %d, Average time: %lf s\n", n, cum_step_time / n);
         if (n % NT == 0 || n == Nt) {
-            check_status(wf_download_state(c, yh.data(), ph.data()), "wf_download_state");
-            timestep_reports(yh.data(), &CFL, &Y_min, &Y_max, &T_min, &T_max, n, parameters);
+            wf_report rep;
+            check_status(wf_timestep_reports(c, &rep), "wf_timestep_reports");
+            if (rep.nan_field >= 0) {
+                // the message and exit of timestep_reports (functions.cu:137-166)
+                const char names[] = "uvwTY";
+                char message[256];
+                snprintf(message, sizeof(message),
+                         "NaN value found in %c(%f, %f, %f, %f) in node (%d, %d, %d) at timestep %d (%d). Exiting...",
+                         names[rep.nan_field], parameters.x[rep.nan_i], parameters.y[rep.nan_j],
+                         parameters.z[rep.nan_k], parameters.t[n], rep.nan_i, rep.nan_j, rep.nan_k, n, n / NT);
+                log_message(parameters, message);
+                wf_dump_wait(c);
+                exit(1);
+            }
+            CFL = rep.cfl;
+            T_min = rep.T_min;
+            T_max = rep.T_max;
+            Y_min = rep.Y_min;
+            Y_max = rep.Y_max;
             log_timestep(parameters, n, parameters.t[n], step_time, CFL, T_min, T_max, Y_min, Y_max);
             if (parameters.variable_density == 1) {
                 double e = 0.0;
@@ -217,7 +235,7 @@ void solve_PDE(double *y_n, double *p, Parameters parameters)
                 snprintf(msg, sizeof(msg), "Pressure solver: Error = %e, iterations = %d", e, m);
                 log_message(parameters, msg);
             }
-            save_data(yh.data(), ph.data(), n / NT, parameters);
+            check_status(wf_dump_async(c, parameters.save_path, n / NT), "wf_dump_async");
             printf("\n");
         }
     }
@@ -226,6 +244,7 @@ void solve_PDE(double *y_n, double *p, Parameters parameters)
     format_seconds(seconds_between(start_solver, end_solver), formatted);
     snprintf(msg, sizeof(msg), "\nSolver time: %s", formatted);
     log_message(parameters, msg);
+    check_status(wf_dump_wait(c), "wf_dump_wait");
     check_status(wf_download_state(c, yh.data(), ph.data()), "wf_download_state");
     to_device(y_n, yh);
     to_device(p, ph);
