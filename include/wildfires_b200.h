@@ -127,6 +127,13 @@ wf_status wf_upload_state(wf_ctx *ctx, const double *y, const double *pr);
 /* Download the current packed state and p as FP64. */
 wf_status wf_download_state(wf_ctx *ctx, double *y, double *pr);
 
+/* The reference's initial conditions (initial_conditions + create_y_0,
+ * functions.cu:187-323, solver.cu:41-56) generated on the device straight
+ * into the context's state and p: no host fields, no upload.  The time level
+ * becomes 0.  T0_shape must be "gaussian" or "parallelepiped" (the reference
+ * leaves T unset otherwise); Y entries the reference leaves unwritten are 0. */
+wf_status wf_initial_conditions(wf_ctx *ctx);
+
 /* Advance nsteps time steps (RK stages, pressure solve, projection, boundary
  * rules, clamps, temperature source).  Enqueued on the context's stream; the
  * first call records the step into a CUDA graph that later calls replay. */

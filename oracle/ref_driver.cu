@@ -23,6 +23,10 @@
  *        pressure -- one pressure solve with y_np1 = y_n = y0, p0   -> OUTDIR/p.bin
  *        step     -- solve_PDE for Nt steps; prints SAVE_PATH=...  (files *.bin.N)
  *        time     -- as step, also prints SECONDS=<wall time of solve_PDE>
+ *        ic       -- the reference's initial_conditions + create_y_0
+ *                    (functions.cu:187-323, solver.cu:41-56)          -> OUTDIR/y0.bin, p0.bin
+ *                    (Y entries the reference leaves unwritten are zero here:
+ *                    its main mallocs Y, and large fresh allocations read as zero)
  * The working directory must be writable: read_parameters_file creates
  * data/output/<timestamp>/ there (src/cu/parameters.cu:21-37).
  */
@@ -105,6 +109,19 @@ int main(int argc, char **argv)
     }
     P.threads_per_block = THREADS;
     P.number_of_blocks = BLOCKS;
+    if (strcmp(mode, "ic") == 0) {
+        const size_t N = (size_t)P.Nx * P.Ny * P.Nz, NY = (size_t)P.Nx * P.Ny * P.Nz_Y_max, S = 4 * N + NY;
+        double *u = (double *)calloc(N, 8), *v = (double *)calloc(N, 8), *w = (double *)calloc(N, 8);
+        double *T = (double *)calloc(N, 8), *p = (double *)calloc(N, 8), *Y = (double *)calloc(NY ? NY : 1, 8);
+        double *y0 = (double *)calloc(S, 8);
+        initial_conditions(u, v, w, T, Y, p, P);
+        create_y_0(u, v, w, T, Y, y0, P);
+        if (write_bin(outdir, "y0.bin", y0, S) || write_bin(outdir, "p0.bin", p, N)) {
+            fprintf(stderr, "ref_driver: cannot write %s\n", outdir);
+            return 1;
+        }
+        return 0;
+    }
     if (P.input_path[0] == '\0') {
         fprintf(stderr, "ref_driver: input_path must be set\n");
         return 2;

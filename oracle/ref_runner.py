@@ -52,6 +52,9 @@ def run(case, mode, flavour="host", parallel=False, timeout=3600, keep=None):
             res["y1"] = np.fromfile(os.path.join(out, "y1.bin"))
         elif mode == "pressure":
             res["p"] = np.fromfile(os.path.join(out, "p.bin"))
+        elif mode == "ic":
+            res["ic_y"] = np.fromfile(os.path.join(out, "y0.bin"))
+            res["ic_p"] = np.fromfile(os.path.join(out, "p0.bin"))
         else:
             kv = dict(line.split("=", 1) for line in r.stdout.splitlines() if "=" in line)
             res["seconds"] = float(kv.get("SECONDS", "nan"))

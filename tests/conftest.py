@@ -28,7 +28,9 @@ def built_libraries():
 
 
 def golden_names():
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+    """Fixtures of the time step (the ic_* fixtures hold initial conditions only)."""
+    names = (os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+    return sorted(n for n in names if not n.startswith("ic_"))
 
 
 def load_golden(name):

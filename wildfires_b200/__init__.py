@@ -179,6 +179,10 @@ class Solver:
             check(s, "wf_diagnostics")
         return {f: getattr(d, f) for f, _ in WfDiag._fields_}
 
+    def initial_conditions(self):
+        """The reference's initial conditions, generated on the GPU (time level 0)."""
+        check(lib().wf_initial_conditions(self._h), "wf_initial_conditions")
+
     def timestep_reports(self):
         """The reference's checkpoint report (functions.cu:82-185) reduced on the GPU."""
         r = WfReport()

@@ -27,6 +27,7 @@ EXPORTS = [
     "wf_ensemble_step", "wf_ensemble_synchronize",
     "wf_closure_param_count", "wf_set_closure", "wf_closure_coefficients", "wf_mlp_loss_grad", "wf_mlp_train",
     "wf_timestep_reports", "wf_dump_async", "wf_dump_wait", "wf_save_domain", "wf_save_topography",
+    "wf_initial_conditions",
 ]
 
 
@@ -114,6 +115,7 @@ def lib():
         "wf_dump_wait": (C.c_int, [vp]),
         "wf_save_domain": (C.c_int, [P, C.c_char_p]),
         "wf_save_topography": (C.c_int, [P, C.c_char_p]),
+        "wf_initial_conditions": (C.c_int, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -165,6 +165,8 @@ struct wf_ctx {
 
 namespace wfs {
 
+wf_status finish_upload(wf_ctx *c);
+
 // Kernel launches of one step: per stage the optional closure inference,
 // k_utau, k_stage_fused and, when some column needs it, k_stage_bc; five
 // pressure kernels per solve (variable density: plus the record reset and,
@@ -865,6 +867,50 @@ wf_status wf_upload_state(wf_ctx *c, const double *y, const double *pr)
     wf_status st = put_state(c, c->ybuf[0], y);
     if (st) return st;
     WF_TRY_CUDA(cudaMemcpyAsync(c->p, pr, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
+    return finish_upload(c);
+}
+
+wf_status wf_initial_conditions(wf_ctx *c)
+{
+    if (!c) { set_error("wf_initial_conditions: null context"); return WF_ERR_ARG; }
+    const Parameters &P = c->P;
+    IcArgs a;
+    memset(&a, 0, sizeof(a));
+    if (strcmp(P.T0_shape, "gaussian") == 0) a.T_shape = 0;
+    else if (strcmp(P.T0_shape, "parallelepiped") == 0) a.T_shape = 1;
+    else {
+        set_error("wf_initial_conditions: T0_shape '%s' is neither gaussian nor parallelepiped", P.T0_shape);
+        return WF_ERR_ARG;
+    }
+    a.u_r = P.u_r; a.z_r = P.z_r; a.alpha_u = P.alpha_u;
+    a.T_0 = P.T_0; a.T_inf = P.T_inf;
+    a.x0 = P.T0_x_center; a.y0 = P.T0_y_center; a.z0 = P.T0_z_center;
+    a.sx = P.T0_length; a.sy = P.T0_width; a.sz = P.T0_height;
+    a.Tx0 = P.T0_x_start; a.Tx1 = P.T0_x_end; a.Ty0 = P.T0_y_start; a.Ty1 = P.T0_y_end;
+    a.Tz0 = P.T0_z_start; a.Tz1 = P.T0_z_end;
+    a.Yx0 = P.Y0_x_start; a.Yx1 = P.Y0_x_end; a.Yy0 = P.Y0_y_start; a.Yy1 = P.Y0_y_end;
+    a.xa = P.Y0_xa; a.ya = P.Y0_ya; a.Y_h = P.Y_h;
+    a.p_top = P.p_top;
+    a.dead[0] = P.u_dead_nodes; a.dead[1] = P.v_dead_nodes; a.dead[2] = P.w_dead_nodes;
+    a.dead[3] = P.T_dead_nodes; a.dead[4] = P.Y_dead_nodes;
+    c->cur = 0;
+    c->n = 0;
+    cudaError_t e = (c->prec == WF_FP64)
+                        ? launch_initial_conditions<double>(c->geom, a, c->d_x, c->d_y, (double *)c->ybuf[0], c->p,
+                                                            c->stream)
+                        : launch_initial_conditions<float>(c->geom, a, c->d_x, c->d_y, (float *)c->ybuf[0], c->p,
+                                                           c->stream);
+    if (e != cudaSuccess) { set_error("wf_initial_conditions: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
+    return finish_upload(c);
+}
+
+}  // extern "C"
+
+namespace wfs {
+// After a new initial state: the held temperature source, then the fuel
+// integral the diagnostics report consumption against.
+wf_status finish_upload(wf_ctx *c)
+{
     if (c->Tsrc) {
         // the held source is the initial temperature field (solver.cu:169)
         WF_TRY_CUDA(cudaMemcpyAsync(c->Tsrc, (char *)c->ybuf[0] + (size_t)3 * c->N * c->esz, (size_t)c->N * c->esz,
@@ -872,10 +918,13 @@ wf_status wf_upload_state(wf_ctx *c, const double *y, const double *pr)
     }
     WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
     wf_diag d;
-    st = wf_diagnostics(c, &d);
+    const wf_status st = wf_diagnostics(c, &d);
     c->fuel0 = d.fuel;
     return st == WF_ERR_NAN ? WF_OK : st;
 }
+}  // namespace wfs
+
+extern "C" {
 
 wf_status wf_download_state(wf_ctx *c, double *y, double *pr)
 {

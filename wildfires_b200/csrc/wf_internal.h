@@ -191,6 +191,20 @@ template <class R>
 cudaError_t launch_report(const Geom &g, const R *y, const double *xg, const double *yg, const double rect[4],
                           double *scratch, cudaStream_t s);
 
+// Initial conditions on the device (setup.cu; functions.cu:187-323).
+struct IcArgs {
+    double u_r, z_r, alpha_u;                   // power-law wind
+    int T_shape;                                // 0 gaussian, 1 parallelepiped
+    double T_0, T_inf, x0, y0, z0, sx, sy, sz;  // gaussian centre and widths
+    double Tx0, Tx1, Ty0, Ty1, Tz0, Tz1;        // parallelepiped
+    double Yx0, Yx1, Yy0, Yy1, xa, ya, Y_h;     // fuel rectangle and ramps
+    double p_top;
+    double dead[5];                             // u, v, w, T, Y on dead nodes
+};
+template <class R>
+cudaError_t launch_initial_conditions(const Geom &g, const IcArgs &a, const double *xg, const double *yg, R *state,
+                                      double *p, cudaStream_t s);
+
 // Asynchronous double-buffered field dumps (dump.cu).
 struct Dumper;
 Dumper *dumper_create(int device, const Parameters &P, size_t S, size_t N);
