@@ -21,6 +21,7 @@ sources compiled for the host by oracle/Makefile, OpenMP over its virtual
 threads) on a bounded sample of the same workload.
 """
 import argparse
+import datetime
 import json
 import os
 import subprocess
@@ -102,7 +103,10 @@ def workload_name(name, P, prec):
 
 # ---- clocks sampled during the timed region ----------------------------------
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi clock and throttle-reason samples every 50 ms, started before
+    the warm-up so that it is running when the timed region begins; stop()
+    keeps the samples whose timestamps fall inside the timed window."""
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -114,12 +118,12 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.out, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
-    def stop(self):
+    def stop(self, window=None):
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -132,17 +136,25 @@ class ClockSampler:
         with open(self.out.name) as f:
             for line in f:
                 parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
+                if len(parts) >= 10:
+                    try:
+                        ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    except ValueError:
+                        ts = None
+                    rows.append((ts, parts[1:]))
         os.unlink(self.out.name)
         if not rows:
             return None
+        inside = [r for ts, r in rows if window and ts is not None and window[0] - 0.05 <= ts <= window[1] + 0.05]
+        in_window = bool(inside)
+        rows = inside if inside else [r for _, r in rows]
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows),
+                "samples_from": "timed window" if in_window else "whole run (no sample inside the timed window)"}
 
 
 # ---- algorithmic bytes (roofline model) -------------------------------------
@@ -247,11 +259,14 @@ def _sample_kw(name, n, nsteps):
     return kw
 
 
-def reference_gpu_sample(case_name, n_short=2, n_long=6):
+def reference_gpu_sample(case_name, n_short=2, n_long=10, repeats=2):
     """The reference's own sm_100a build (oracle/_ref/ref_gpu: its src/cu
     sources compiled unmodified, FP64) on the same workload and GPU: wall time
     of its solve_PDE for n_long and n_short steps; the difference divided by
-    the extra steps removes its set-up (allocations, coefficient tables)."""
+    the extra steps removes its set-up (allocations, coefficient tables) and
+    the state it writes at its last step.  Dirty pages are flushed before each
+    run and the faster of `repeats` runs is kept, so that the write-back of
+    one run's files does not land in another run's time."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref_runner
     from wildfires_b200 import configs
@@ -259,13 +274,19 @@ def reference_gpu_sample(case_name, n_short=2, n_long=6):
         return None
     secs = {}
     for n in (n_short, n_long):
-        secs[n] = ref_runner.run(configs.CASES[case_name](Nt=n), "time", flavour="gpu")["seconds"]
+        best = None
+        for _ in range(repeats):
+            os.sync()
+            t = ref_runner.run(configs.CASES[case_name](Nt=n), "time", flavour="gpu")["seconds"]
+            best = t if best is None else min(best, t)
+        secs[n] = best
     per = (secs[n_long] - secs[n_short]) / (n_long - n_short)
     P = build_params_only(case_name)
     cells = P.rec.Nx * P.rec.Ny * P.rec.Nz
     return {"value": round(cells / per / 1e6, 2), "unit": METRIC, "ms_per_step": round(per * 1e3, 2),
-            "dtype": "f64", "how": "reference src/cu built for sm_100a, solve_PDE wall time for %d and %d steps, "
-                                   "difference per step (set-up removed)" % (n_short, n_long)}
+            "dtype": "f64", "how": "reference src/cu built for sm_100a, solve_PDE wall time for %d and %d steps "
+                                   "(fastest of %d runs each), difference per step (set-up removed)"
+                                   % (n_short, n_long, repeats)}
 
 
 # ---- GPU arm --------------------------------------------------------------------
@@ -307,23 +328,24 @@ def run_ours(args):
         barrier()
         torch.cuda.synchronize()
         solver.synchronize()
-        if clocks:
-            clocks.start()
+        t0 = time.time()
         e0.record(stream)
         solver.step(K)
         e1.record(stream)
         solver.synchronize()
         torch.cuda.synchronize()
+        t1 = time.time()
         barrier()
-        info = clocks.stop() if clocks else None
+        info = clocks.stop((t0, t1)) if clocks else None
         return e0.elapsed_time(e1), info
 
     res = {}
     sol = Solver(P, args.precision)
     sol.upload(y0, p0)
+    clocks = ClockSampler(dev)
+    clocks.start()
     sol.step(W)
     sol.synchronize()
-    clocks = ClockSampler(dev)
     ms, clk = timed_steps(sol, K, clocks)
     ms = max_over_ranks(ms)
     ms_step = ms / K
@@ -506,11 +528,14 @@ def run_ensemble(args):
         clk = ClockSampler(local) if rank == 0 else None
         if clk:
             clk.start()
+            time.sleep(0.3)
         barrier()
         t0 = time.perf_counter()
+        w0 = time.time()
         ens.step(args.steps)
         ens.synchronize()
         t_ens = max_over_ranks(time.perf_counter() - t0)
+        w1 = time.time()
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
@@ -518,7 +543,7 @@ def run_ensemble(args):
                 m.step(1)
                 m.synchronize()
         t_ser = max_over_ranks(time.perf_counter() - t0)
-        clocks = clk.stop() if clk else None
+        clocks = clk.stop((w0, w1)) if clk else None
     cells = cells_local
     if world > 1:
         t = torch.tensor([float(cells_local)], dtype=torch.float64, device="cuda")

@@ -323,11 +323,11 @@ template <class R> __device__ __forceinline__ R dz5(const R *w, R m2, R m1, R c,
 }
 
 // One RK stage over TI x TJ x KZ tiles (reference RHS pde.cu:139-787,
-// turbulence.cu:255-454, RK combination solver.cu:14-93).  Persistent: each
-// block walks tiles blockIdx.x, + gridDim.x, ...; while it computes one tile
-// the inputs of its next tile arrive in the other buffer.  Per tile:
-//   1. column tables, z rows, stage input with halo 2, fuel with halo 1
-//      -> shared memory (issued one tile ahead)
+// turbulence.cu:255-454, RK combination solver.cu:14-93).  One tile per block
+// (the grid is the tile count); two blocks per SM in FP32, so one block's tile
+// loads overlap the other's arithmetic.  Per tile:
+//   1. column tables, z rows, stage input with halo 2 -> shared memory
+//      (cp.async; the fuel fraction is read from global memory where needed)
 //   2. SGS inputs (raw mu_sgs, strain S', divergence source) on the tile and
 //      its halo 1 -> shared memory
 //   3. per tile cell: advection, diffusion, forces, reaction, SGS divergence,
@@ -355,9 +355,7 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
         TL t;
         t.bind(smem_raw, sgs);
         const int k0 = (tile % ntk) * KZ, j0 = ((tile / ntk) % ntj) * TJ, i0 = (tile / (ntk * ntj)) * TI;
-        const int nxt = tile + gridDim.x;
-        (void)nxt;
-            cp_async_commit();   // empty group keeps the wait below uniform
+        cp_async_commit();       // empty group keeps the wait below uniform
         cp_async_wait<1>();      // this tile's group has landed
         __syncthreads();
 
@@ -765,6 +763,9 @@ __global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_s
             if (Nz - 1 >= k0 && Nz - 1 < k0 + KZ && bc_top_in_tile(Nz, KZ)) bc_top(a, col, rd, kp, an);
         }
         __syncthreads();         // buffer and SGS inputs free for the next tiles
+        // a grid smaller than the tile count walks on (the launch gives one tile per block)
+        const int nxt = tile + gridDim.x;
+        if (nxt < ntiles) issue_tile<R, TL, NT>(a, t, (nxt / (ntk * ntj)) * TI, ((nxt / ntk) % ntj) * TJ, (nxt % ntk) * KZ);
     }
     cp_async_wait<0>();
 }
