@@ -30,7 +30,7 @@ __device__ __forceinline__ int wrap_p(int v, int n)
 // compiled for 32 registers (a few spilled), so that 16 column blocks of 128
 // threads share an SM instead of 9: 0.542 -> 0.500 ms at 512x512x128.
 template <class R>
-__global__ void __launch_bounds__(512, sizeof(R) == 4 ? 4 : 1) k_project(const ProjectArgs<R> a)
+__global__ void __launch_bounds__(512, sizeof(R) == 4 ? 4 : 0) k_project(const ProjectArgs<R> a)
 {
     extern __shared__ double sh[];
     const Geom &g = a.g;
