@@ -55,3 +55,31 @@ def test_ensemble_members_out_of_step_fall_back_to_eager():
             s.step(k)
             y, p = s.download()
         assert np.array_equal(got[i][0], y) and np.array_equal(got[i][1], p)
+
+
+def test_ensemble_with_pressure_tolerance_equals_members_alone():
+    """Variable density with a tolerance: each member's fixed point runs as a
+    CUDA graph WHILE node inside the ensemble graph (captured on the member's
+    stream); results and iteration reports equal the members stepped alone."""
+    from wildfires_b200 import Ensemble, Solver, configs
+    kw = dict(Nz=32, z_max=31 * 0.3125, Nt=4, jitter=0.2, variable_density=1,
+              pressure_solver_iter=20, pressure_solver_tol=1e-9)
+    built = [configs.materialize(c) for c in (configs.scenario(33, 48, seed=4, **kw),
+                                              configs.scenario(48, 40, seed=5, **kw))]
+    alone = []
+    for P, y0, p0 in built:
+        with Solver(P, "fp64") as s:
+            s.upload(y0, p0)
+            s.step(3)
+            alone.append((s.download(), s.pressure_report()))
+    with Ensemble([b[0] for b in built], "fp64") as ens:
+        for i, (P, y0, p0) in enumerate(built):
+            ens[i].upload(y0, p0)
+        ens.step(3)
+        ens.synchronize()
+        for i in range(len(built)):
+            y, p = ens[i].download()
+            (ya, pa), rep = alone[i]
+            assert np.array_equal(y, ya) and np.array_equal(p, pa), i
+            err, it = ens[i].pressure_report()
+            assert (err, it) == rep and 0 <= it < 20
