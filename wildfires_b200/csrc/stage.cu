@@ -305,13 +305,36 @@ __device__ __forceinline__ void issue_tile(const StageArgs<R> &a, TL &t, int i0,
         const bool ok = gk >= 0 && gk < Nz;
         cp_async<sizeof(R)>(t.kr + c, a.krow + (ok ? (size_t)gk * KROW + c % KROW : 0), ok);
     }
-    for (int c = threadIdx.x; c < TL::SR; c += NT) {
-        const int kk = c % TL::SK - 2, jj = (c / TL::SK) % TL::SJ - 2, ii = c / (TL::SK * TL::SJ) - 2;
-        const int gk = k0 + kk;
-        const bool ok = gk >= 0 && gk < Nz && i0 + ii <= Nx + 1 && j0 + jj <= Ny + 1;
-        const size_t o = ok ? ((size_t)wrap_p(i0 + ii, Nx - 1) * Ny + wrap_p(j0 + jj, Ny - 1)) * Nz + gk : 0;
+    if constexpr (TL::PAIRED && TL::SK * TL::SJ <= NT) {
+        // FP32 tile: thread (k, j) of the SK x SJ cross-section walks the SI
+        // planes in i, so the k/j arithmetic and the j wrap happen once per
+        // thread (lanes k fastest: global reads stay coalesced along k)
+        if (threadIdx.x < TL::SK * TL::SJ) {
+            const int kk = threadIdx.x % TL::SK - 2, jj = threadIdx.x / TL::SK - 2;
+            const int gk = k0 + kk, gj = j0 + jj;
+            const bool okjk = gk >= 0 && gk < Nz && gj <= Ny + 1;
+            const size_t cj = okjk ? (size_t)wrap_p(gj, Ny - 1) * Nz + gk : 0;
+            const size_t plane = (size_t)Ny * Nz;
+#pragma unroll 4
+            for (int ii = -2; ii < TL::SI - 2; ii++) {
+                const int gi = i0 + ii;
+                const bool ok = okjk && gi <= Nx + 1;
+                const size_t o = ok ? (size_t)wrap_p(gi, Nx - 1) * plane + cj : 0;
+                const int sidx = TL::s(ii, jj, kk);
 #pragma unroll
-        for (int f = 0; f < 4; f++) cp_async<sizeof(R)>(t.st + TL::so(f, TL::s(ii, jj, kk)), X + (size_t)f * N + o, ok);
+                for (int f = 0; f < 4; f++) cp_async<sizeof(R)>(t.st + TL::so(f, sidx), X + (size_t)f * N + o, ok);
+            }
+        }
+    } else {
+        for (int c = threadIdx.x; c < TL::SR; c += NT) {
+            const int kk = c % TL::SK - 2, jj = (c / TL::SK) % TL::SJ - 2, ii = c / (TL::SK * TL::SJ) - 2;
+            const int gk = k0 + kk;
+            const bool ok = gk >= 0 && gk < Nz && i0 + ii <= Nx + 1 && j0 + jj <= Ny + 1;
+            const size_t o = ok ? ((size_t)wrap_p(i0 + ii, Nx - 1) * Ny + wrap_p(j0 + jj, Ny - 1)) * Nz + gk : 0;
+#pragma unroll
+            for (int f = 0; f < 4; f++)
+                cp_async<sizeof(R)>(t.st + TL::so(f, TL::s(ii, jj, kk)), X + (size_t)f * N + o, ok);
+        }
     }
     cp_async_commit();
 }
