@@ -405,6 +405,7 @@ def run_ours(args):
     e2e = {"value": round(cells * ke * world / e2e_s / 1e6, 2), "unit": METRIC,
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
            "note": "per step: upload of the FP64 packed state and p from pinned host memory, one step, download"}
+    stage_tile = sol.stage_tile()
     sol.close()
 
     # plain FP64 path on the same workload
@@ -452,6 +453,7 @@ def run_ours(args):
             "config": workload_config(args.config, P, args.precision, world),
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roof,
             "kernels": kernels, "cpu_baseline": cpu, "clocks": clk, "fp64": fp64,
+            "stage_tile": "%dx%dx8 (picked by the per-context tuner)" % stage_tile,
             "reference_gpu": None if (args.no_refgpu or world > 1) else reference_gpu_sample(args.config),
         }
         print(json.dumps(out), flush=True)

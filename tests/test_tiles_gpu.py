@@ -1,0 +1,53 @@
+"""Tile shapes of the fused stage pass: every compiled shape gives bit-identical
+states (a cell's arithmetic does not depend on the tiling, and the Van Driest
+shortcut only skips factors that are exactly 1), and the per-context tuner
+picks one of them."""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+SHAPES32 = [(8, 16), (8, 8), (4, 16)]
+
+
+def _run(P, g, prec, shape, n):
+    from wildfires_b200 import Solver
+    with Solver(P, prec) as s:
+        if shape is not None:
+            s.set_stage_tile(*shape)
+        s.upload(g["y0"], g["p0"])
+        s.step(n)
+        return s.download(), s.stage_tile()
+
+
+@pytest.mark.parametrize("name", ["hill_rk4", "flat_33x33x16_10", "stretched_rk2"])
+def test_tile_shapes_give_identical_states(name, params_from_text):
+    g = load_golden(name)
+    P = params_from_text(g["params"])
+    n = int(g["nsteps"])
+    (y0, p0), _ = _run(P, g, "fp32", SHAPES32[0], n)
+    for shape in SHAPES32[1:]:
+        (y, p), used = _run(P, g, "fp32", shape, n)
+        assert used == shape
+        assert np.array_equal(y, y0) and np.array_equal(p, p0), shape
+
+
+def test_tuner_picks_a_compiled_shape(params_from_text):
+    g = load_golden("flat_33x33x16_10")
+    P = params_from_text(g["params"])
+    (y, p), used = _run(P, g, "fp32", None, 2)
+    assert used in SHAPES32
+    (yr, pr), _ = _run(P, g, "fp32", SHAPES32[0], 2)
+    assert np.array_equal(y, yr) and np.array_equal(p, pr)
+    (_, _), used64 = _run(P, g, "fp64", None, 1)
+    assert used64 == (8, 8)
+
+
+def test_unknown_shape_is_rejected(params_from_text):
+    from wildfires_b200 import Solver, WfError
+    g = load_golden("hill_rk4")
+    P = params_from_text(g["params"])
+    with Solver(P, "fp32") as s:
+        with pytest.raises(WfError):
+            s.set_stage_tile(16, 16)

@@ -179,6 +179,15 @@ class Solver:
             check(s, "wf_diagnostics")
         return {f: getattr(d, f) for f, _ in WfDiag._fields_}
 
+    def stage_tile(self):
+        """(TI, TJ) of the fused stage pass (picked by the first step)."""
+        ti, tj = C.c_int(), C.c_int()
+        check(lib().wf_stage_tile(self._h, C.byref(ti), C.byref(tj)), "wf_stage_tile")
+        return ti.value, tj.value
+
+    def set_stage_tile(self, ti, tj):
+        check(lib().wf_set_stage_tile(self._h, int(ti), int(tj)), "wf_set_stage_tile")
+
     def initial_conditions(self):
         """The reference's initial conditions, generated on the GPU (time level 0)."""
         check(lib().wf_initial_conditions(self._h), "wf_initial_conditions")

@@ -27,7 +27,7 @@ EXPORTS = [
     "wf_ensemble_step", "wf_ensemble_synchronize",
     "wf_closure_param_count", "wf_set_closure", "wf_closure_coefficients", "wf_mlp_loss_grad", "wf_mlp_train",
     "wf_timestep_reports", "wf_dump_async", "wf_dump_wait", "wf_save_domain", "wf_save_topography",
-    "wf_initial_conditions",
+    "wf_initial_conditions", "wf_stage_tile", "wf_set_stage_tile",
 ]
 
 
@@ -116,6 +116,8 @@ def lib():
         "wf_save_domain": (C.c_int, [P, C.c_char_p]),
         "wf_save_topography": (C.c_int, [P, C.c_char_p]),
         "wf_initial_conditions": (C.c_int, [vp]),
+        "wf_stage_tile": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "wf_set_stage_tile": (C.c_int, [vp, C.c_int, C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -10,6 +10,7 @@
 #include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <string>
@@ -161,11 +162,14 @@ struct wf_ctx {
     int *d_closure_err = nullptr;   // raised by the closure kernel on a timed-out tensor-core wait
     double *d_rep = nullptr;        // checkpoint report scratch
     Dumper *dump = nullptr;         // asynchronous dumps (created by the first wf_dump_async)
+    int tile = 0;                   // tile shape of the fused stage pass (index)
+    bool tile_set = false;          // chosen by the tuner, WF_STAGE_TILE or wf_set_stage_tile
 };
 
 namespace wfs {
 
 wf_status finish_upload(wf_ctx *c);
+wf_status tune_tiles(wf_ctx *c);
 
 // Kernel launches of one step: per stage the optional closure inference,
 // k_utau, k_stage_fused and, when some column needs it, k_stage_bc; five
@@ -386,6 +390,7 @@ template <class R> StageArgs<R> stage_args(wf_ctx *c, const void *X, const void 
     a.closure_err = c->d_closure_err;
     a.bcfix = c->d_bcfix;
     a.nbcfix = c->nbcfix;
+    a.tile = c->tile;
     const double dt = c->P.dt;
     if (c->method == 0) a.a_next = dt;
     else if (c->method == 1) a.a_next = (stage == 1) ? dt : 0.5 * dt;
@@ -441,8 +446,6 @@ template <class R> wf_status enqueue_stages(wf_ctx *c, void *yn, void *y1)
     return WF_OK;
 }
 
-// Pressure solve(s) for y1 given yn.  For variable density the fixed point
-// stops on the max-norm change; that decision is taken on the host.
 // Capture the variable-density fixed point (pressure.cu:551-606) into the
 // stream's capture: p_prev = p, reset of the device record, then a WHILE node
 // whose body (captured on c->aux) is one Poisson solve, the max-norm change
@@ -922,6 +925,68 @@ wf_status finish_upload(wf_ctx *c)
     c->fuel0 = d.fuel;
     return st == WF_ERR_NAN ? WF_OK : st;
 }
+
+// Tile shape of the fused stage pass for this context.  WF_STAGE_TILE=TIxTJ in
+// the environment forces a shape; otherwise, when more than one shape is
+// compiled, each is timed on the context's own grid and current state (a
+// stage that stores k_s into a scratch buffer, so the state is untouched: one
+// warm-up launch, then enough launches for about 2 ms, at least 3) and the
+// fastest kept.  Every shape gives
+// bit-identical results: a cell's arithmetic does not depend on the tiling.
+template <class R> wf_status tune_tiles_impl(wf_ctx *c)
+{
+    const int prec = c->prec == WF_FP64 ? 0 : 1, count = stage_tile_count(prec);
+    c->tile_set = true;
+    if (const char *env = getenv("WF_STAGE_TILE")) {
+        int ti = 0, tj = 0;
+        if (sscanf(env, "%dx%d", &ti, &tj) == 2)
+            for (int q = 0; q < count; q++) {
+                int a = 0, b = 0;
+                stage_tile_shape(prec, q, &a, &b);
+                if (a == ti && b == tj) { c->tile = q; return WF_OK; }
+            }
+        set_error("WF_STAGE_TILE=%s is not a compiled tile shape", env);
+        return WF_ERR_ARG;
+    }
+    if (count < 2) return WF_OK;
+    void *in = c->ybuf[c->cur], *scratch = c->Xa ? c->Xa : c->ybuf[1 - c->cur];
+    const int saved = c->method;
+    c->method = 3;
+    cudaEvent_t e0, e1;
+    WF_TRY_CUDA(cudaEventCreate(&e0));
+    WF_TRY_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int pick = 0;
+    cudaError_t err = cudaSuccess;
+    for (int q = 0; q < count && !err; q++) {
+        c->tile = q;
+        const StageArgs<R> a = stage_args<R>(c, in, in, scratch, 1);
+        float ms = 0.0f;
+        int reps = 1;
+        for (int pass = 0; pass < 2 && !err; pass++) {   // pass 0 warms up and sizes pass 1
+            err = cudaEventRecord(e0, c->stream);
+            for (int r = 0; r < reps && !err; r++) err = launch_stage<R>(a, c->stream);
+            if (!err) err = cudaEventRecord(e1, c->stream);
+            if (!err) err = cudaEventSynchronize(e1);
+            if (!err) err = cudaEventElapsedTime(&ms, e0, e1);
+            if (pass == 0) reps = ms > 0.0f ? (int)fminf(fmaxf(2.0f / ms, 3.0f), 64.0f) : 3;
+        }
+        ms /= (float)reps;
+        if (!err && ms < best) { best = ms; pick = q; }
+    }
+    c->method = saved;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->tile = pick;
+    if (err) { set_error("stage tile tuning: %s", cudaGetErrorString(err)); return WF_ERR_CUDA; }
+    return WF_OK;
+}
+
+wf_status tune_tiles(wf_ctx *c)
+{
+    if (c->tile_set) return WF_OK;
+    return c->prec == WF_FP64 ? tune_tiles_impl<double>(c) : tune_tiles_impl<float>(c);
+}
 }  // namespace wfs
 
 extern "C" {
@@ -939,6 +1004,10 @@ wf_status wf_download_state(wf_ctx *c, double *y, double *pr)
 wf_status wf_step(wf_ctx *c, int nsteps)
 {
     if (!c || nsteps < 0) { set_error("wf_step: invalid argument"); return WF_ERR_ARG; }
+    if (nsteps > 0) {
+        const wf_status st = tune_tiles(c);
+        if (st) return st;
+    }
     for (int q = 0; q < nsteps; q++) {
         const int n1 = c->n + 1;
         if (step_is_static(c, n1)) {
@@ -1015,6 +1084,31 @@ wf_status wf_timestep_reports(wf_ctx *c, wf_report *out)
         out->nan_i = (int)(cell / ((unsigned long long)c->Nz * c->Ny));
     }
     return WF_OK;
+}
+
+wf_status wf_stage_tile(const wf_ctx *c, int *ti, int *tj)
+{
+    if (!c || !ti || !tj) { set_error("wf_stage_tile: null argument"); return WF_ERR_ARG; }
+    stage_tile_shape(c->prec == WF_FP64 ? 0 : 1, c->tile, ti, tj);
+    return WF_OK;
+}
+
+wf_status wf_set_stage_tile(wf_ctx *c, int ti, int tj)
+{
+    if (!c) { set_error("wf_set_stage_tile: null context"); return WF_ERR_ARG; }
+    const int prec = c->prec == WF_FP64 ? 0 : 1;
+    for (int q = 0; q < stage_tile_count(prec); q++) {
+        int a = 0, b = 0;
+        stage_tile_shape(prec, q, &a, &b);
+        if (a == ti && b == tj) {
+            c->tile = q;
+            c->tile_set = true;
+            drop_graphs(c);
+            return WF_OK;
+        }
+    }
+    set_error("wf_set_stage_tile: %dx%d is not a compiled tile shape", ti, tj);
+    return WF_ERR_ARG;
 }
 
 wf_status wf_dump_async(wf_ctx *c, const char *dir, int n)
@@ -1242,6 +1336,10 @@ wf_ctx *wf_ensemble_member(wf_ensemble *e, int i)
 wf_status wf_ensemble_step(wf_ensemble *e, int nsteps)
 {
     if (!e || nsteps < 0) { set_error("wf_ensemble_step: invalid argument"); return WF_ERR_ARG; }
+    for (wf_ctx *c : e->m) {
+        const wf_status st = nsteps > 0 ? tune_tiles(c) : WF_OK;
+        if (st) return st;
+    }
     for (int q = 0; q < nsteps; q++) {
         bool same = true, fixed = true;
         for (wf_ctx *c : e->m) {

@@ -357,7 +357,7 @@ template <class R> __device__ __forceinline__ R dz5(const R *w, R m2, R m1, R c,
 //      RK update.  Cells the boundary rules overwrite (k <= cut node, top) are
 //      left to k_stage_bc; the values it needs are stored in a.bc.
 template <class R, int TI, int TJ, int KZ, int NT>
-__global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? 2 : 1) k_stage_fused(const StageArgs<R> a, int ntk, int ntj, int nti)
+__global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? (TI * TJ <= 64 ? 3 : 2) : 1) k_stage_fused(const StageArgs<R> a, int ntk, int ntj, int nti)
 {
     using TL = Tile<R, TI, TJ, KZ>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -814,40 +814,61 @@ __global__ void __launch_bounds__(128) k_stage_bc(const StageArgs<R> a, int KZ)
 
 }  // namespace
 
-template <class R> struct StageCfg;
-template <> struct StageCfg<float> {
-    static constexpr int TI = 8, TJ = 16, KZ = 8, NT = 256;
+// Tile shapes of the fused pass: TI x TJ columns of KZ = 8 planes, 256 threads.
+// FP32 compiles three shapes (8x16 is the default; the smaller ones give more,
+// shorter blocks, which can balance small grids better); the per-context tuner
+// in solver.cu times them on the context's own grid.  FP64 has one shape.
+template <class R, int TI_, int TJ_> struct StageShape {
+    static constexpr int TI = TI_, TJ = TJ_, KZ = 8, NT = 256;
+    using TL = Tile<R, TI, TJ, KZ>;
+    static size_t smem() { return TL::bytes(); }
 };
-template <> struct StageCfg<double> {
-    static constexpr int TI = 8, TJ = 8, KZ = 8, NT = 256;
+template <class R> struct StageShapes;
+template <> struct StageShapes<float> {
+    static constexpr int count = 3;
+    static constexpr int ti[3] = {8, 8, 4}, tj[3] = {16, 8, 16};
 };
+template <> struct StageShapes<double> {
+    static constexpr int count = 1;
+    static constexpr int ti[1] = {8}, tj[1] = {8};
+};
+
+// the shape with index idx, as a type, for f(Shape)
+template <class R, class F> cudaError_t with_shape(int idx, F f)
+{
+    if constexpr (sizeof(R) == 4) {
+        switch (idx) {
+        case 0: return f(StageShape<R, 8, 16>());
+        case 1: return f(StageShape<R, 8, 8>());
+        case 2: return f(StageShape<R, 4, 16>());
+        default: return cudaErrorInvalidValue;
+        }
+    } else {
+        if (idx != 0) return cudaErrorInvalidValue;
+        return f(StageShape<R, 8, 8>());
+    }
+}
 
 int g_stage_sms = 0;   // multiprocessors of the device, read at set-up
 
-template <class R> size_t stage_smem_bytes()
-{
-    using C = StageCfg<R>;
-    return Tile<R, C::TI, C::TJ, C::KZ>::bytes();
-}
-template size_t stage_smem_bytes<double>();
-template size_t stage_smem_bytes<float>();
-
 template <class R> cudaError_t stage_set_attributes()
 {
-    using C = StageCfg<R>;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (!e) e = cudaDeviceGetAttribute(&g_stage_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e) return e;
-    return cudaFuncSetAttribute(k_stage_fused<R, C::TI, C::TJ, C::KZ, C::NT>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem_bytes<R>());
+    for (int q = 0; !e && q < StageShapes<R>::count; q++)
+        e = with_shape<R>(q, [](auto sh) {
+            using SH = decltype(sh);
+            return cudaFuncSetAttribute(k_stage_fused<R, SH::TI, SH::TJ, SH::KZ, SH::NT>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::smem());
+        });
+    return e;
 }
 template cudaError_t stage_set_attributes<double>();
 template cudaError_t stage_set_attributes<float>();
 
 template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t s, cudaEvent_t *ev)
 {
-    using C = StageCfg<R>;
     const int ncol = a.g.Nx * a.g.Ny;
     if (a.coef) {
         cudaError_t e = launch_closure_coef_tc<R>(a.X, a.g, a.ph.dx, a.ph.dy, a.theta, a.coef, a.closure_err, s);
@@ -855,17 +876,32 @@ template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t 
     }
     k_utau<R><<<(ncol + 127) / 128, 128, 0, s>>>(a);
     if (ev) cudaEventRecord(ev[0], s);
-    const int ntk = (a.g.Nz + C::KZ - 1) / C::KZ, ntj = (a.g.Ny + C::TJ - 1) / C::TJ, nti = (a.g.Nx + C::TI - 1) / C::TI;
-    const int ntiles = ntk * ntj * nti;
-    const int blocks = ntiles;
-    k_stage_fused<R, C::TI, C::TJ, C::KZ, C::NT><<<blocks, C::NT, stage_smem_bytes<R>(), s>>>(a, ntk, ntj, nti);
+    cudaError_t e = with_shape<R>(a.tile, [&](auto sh) {
+        using SH = decltype(sh);
+        const int ntk = (a.g.Nz + SH::KZ - 1) / SH::KZ, ntj = (a.g.Ny + SH::TJ - 1) / SH::TJ;
+        const int nti = (a.g.Nx + SH::TI - 1) / SH::TI;
+        k_stage_fused<R, SH::TI, SH::TJ, SH::KZ, SH::NT><<<ntk * ntj * nti, SH::NT, SH::smem(), s>>>(a, ntk, ntj, nti);
+        return cudaSuccess;
+    });
+    if (e) return e;
     if (ev) cudaEventRecord(ev[1], s);
-    if (a.nbcfix > 0) k_stage_bc<R><<<(a.nbcfix + 127) / 128, 128, 0, s>>>(a, C::KZ);
+    if (a.nbcfix > 0) k_stage_bc<R><<<(a.nbcfix + 127) / 128, 128, 0, s>>>(a, 8);
     if (ev) cudaEventRecord(ev[2], s);
     return cudaGetLastError();
 }
 
-int stage_tile_planes(int precision) { return precision == 0 ? StageCfg<double>::KZ : StageCfg<float>::KZ; }
+int stage_tile_planes(int precision) { (void)precision; return 8; }
+int stage_tile_count(int precision) { return precision == 0 ? StageShapes<double>::count : StageShapes<float>::count; }
+void stage_tile_shape(int precision, int idx, int *ti, int *tj)
+{
+    if (precision == 0) {
+        *ti = StageShapes<double>::ti[idx];
+        *tj = StageShapes<double>::tj[idx];
+    } else {
+        *ti = StageShapes<float>::ti[idx];
+        *tj = StageShapes<float>::tj[idx];
+    }
+}
 
 template cudaError_t launch_stage<double>(const StageArgs<double> &, cudaStream_t, cudaEvent_t *);
 template cudaError_t launch_stage<float>(const StageArgs<float> &, cudaStream_t, cudaEvent_t *);

@@ -111,6 +111,7 @@ struct StageArgs {
     int *closure_err;      // set by the closure kernel when a tensor-core wait times out
     const int *bcfix;      // columns whose cut node or top the fused pass leaves to k_stage_bc
     int nbcfix;
+    int tile;              // tile shape of the fused pass (index into the compiled shapes)
 };
 
 // Learned closure (closure.cu).
@@ -127,6 +128,10 @@ cudaError_t launch_adam(float *theta, float *m, float *v, const float *g, int st
 template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t s, cudaEvent_t *ev = nullptr);
 template <class R> cudaError_t stage_set_attributes();
 int stage_tile_planes(int precision);   // z planes of a fused-stage tile
+// Tile shapes compiled for the fused pass (all with the same z planes, so the
+// boundary-column list does not depend on the choice): count and TI x TJ.
+int stage_tile_count(int precision);
+void stage_tile_shape(int precision, int idx, int *ti, int *tj);
 
 template <class R>
 struct ProjectArgs {
