@@ -283,6 +283,36 @@ def evaluate(th, seed=100, Nc=(33, 33, 9), steps=120, precision="fp32"):
     return out
 
 
+def cost_study(th, Nc=(65, 65, 17), steps=40, precision="fp32"):
+    """Cost of the 4x refinement at a size where the GPU, not launch latency,
+    sets the pace: seconds per step of the fine run and of the coarse run
+    with Smagorinsky and with the network, the same time step for both (the
+    study's setting), timed around device synchronisations after a warm-up
+    that also records the step graphs.  Only cost is measured here; the
+    accuracy comparison is `evaluate`."""
+    import ctypes as C
+    from . import Solver, configs
+    from ._abi import check, lib
+    out = {"coarse_grid": list(Nc), "fine_grid": [FACTOR * (n - 1) + 1 for n in Nc], "steps": steps}
+    runs = (("fine", True, None), ("smagorinsky", False, None), ("mlp", False, th))
+    for name, fine, params in runs:
+        P, y0, p0 = configs.materialize(study_case(Nc, fine=fine, seed=100, Nt=steps))
+        with Solver(P, precision) as s:
+            if params is not None:
+                p = np.ascontiguousarray(params, dtype=np.float32)
+                check(lib().wf_set_closure(s._h, 1, p.ctypes.data_as(C.POINTER(C.c_float))), "wf_set_closure")
+            s.upload(y0, p0)
+            s.step(4)
+            s.synchronize()
+            t0 = time.perf_counter()
+            s.step(steps)
+            s.synchronize()
+            out[name + "_ms_per_step"] = (time.perf_counter() - t0) / steps * 1e3
+    out["fine_over_mlp"] = out["fine_ms_per_step"] / out["mlp_ms_per_step"]
+    out["fine_over_smagorinsky"] = out["fine_ms_per_step"] / out["smagorinsky_ms_per_step"]
+    return out
+
+
 def main(argv=None):
     """python -m wildfires_b200.closure [out.npz]: build the dataset from fine
     runs (seeds 0-2), train, evaluate on seed 100, save the parameters."""
@@ -293,6 +323,7 @@ def main(argv=None):
     th, hist = train(X, y)
     np.save(path, th)
     res = evaluate(th)
+    res["cost"] = cost_study(th)
     res["train"] = {"samples": int(len(y)), "loss_first": float(hist[0]), "loss_last": float(hist[-1]),
                     "target_mean": float(y.mean())}
     print(json.dumps(res))
