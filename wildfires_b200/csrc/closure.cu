@@ -46,6 +46,19 @@ __device__ __forceinline__ float gelu_grad(float x)
     const float t = tanhf(kGeluK * (x + 0.044715f * x * x * x));
     return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * kGeluK * (1.0f + 3.0f * 0.044715f * x * x);
 }
+// Inference form: the hardware tanh approximation (PTX tanh.approx.f32, about
+// 2^-11 relative error) is well inside the BF16 rounding the hidden
+// activations get anyway; training keeps tanhf (its gradients are checked to 1e-4).
+__device__ __forceinline__ float tanh_approx(float x)
+{
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float gelu_fast(float x)
+{
+    return 0.5f * x * (1.0f + tanh_approx(kGeluK * (x + 0.044715f * x * x * x)));
+}
 __device__ __forceinline__ float softplus(float x) { return x > 20.0f ? x : log1pf(expf(x)); }
 __device__ __forceinline__ float sigmoid(float x) { return 1.0f / (1.0f + expf(-x)); }
 
@@ -275,10 +288,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_closure_coef_tc(const R *__re
 #pragma unroll
         for (int c = 0; c < 8; c++) {
             uint4 w;
-            w.x = pack_bf16(gelu(acc[8 * c + 0] + sb1[8 * c + 0]), gelu(acc[8 * c + 1] + sb1[8 * c + 1]));
-            w.y = pack_bf16(gelu(acc[8 * c + 2] + sb1[8 * c + 2]), gelu(acc[8 * c + 3] + sb1[8 * c + 3]));
-            w.z = pack_bf16(gelu(acc[8 * c + 4] + sb1[8 * c + 4]), gelu(acc[8 * c + 5] + sb1[8 * c + 5]));
-            w.w = pack_bf16(gelu(acc[8 * c + 6] + sb1[8 * c + 6]), gelu(acc[8 * c + 7] + sb1[8 * c + 7]));
+            w.x = pack_bf16(gelu_fast(acc[8 * c + 0] + sb1[8 * c + 0]), gelu_fast(acc[8 * c + 1] + sb1[8 * c + 1]));
+            w.y = pack_bf16(gelu_fast(acc[8 * c + 2] + sb1[8 * c + 2]), gelu_fast(acc[8 * c + 3] + sb1[8 * c + 3]));
+            w.z = pack_bf16(gelu_fast(acc[8 * c + 4] + sb1[8 * c + 4]), gelu_fast(acc[8 * c + 5] + sb1[8 * c + 5]));
+            w.w = pack_bf16(gelu_fast(acc[8 * c + 6] + sb1[8 * c + 6]), gelu_fast(acc[8 * c + 7] + sb1[8 * c + 7]));
             *reinterpret_cast<uint4 *>(smem + kTcA2 + tc_off(tid, 8 * c, 8)) = w;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -299,7 +312,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_closure_coef_tc(const R *__re
         tc_ld64(lane_base + 64, acc);
         float o = sb3[0];
 #pragma unroll
-        for (int q = 0; q < 64; q++) o += gelu(acc[q] + sb2[q]) * sW3[q];
+        for (int q = 0; q < 64; q++) o += gelu_fast(acc[q] + sb2[q]) * sW3[q];
         if (cell < N) coef[cell] = (R)softplus(o);
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();   // TMEM and operands free for the next tile
