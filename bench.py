@@ -453,7 +453,7 @@ def run_ours(args):
             "config": workload_config(args.config, P, args.precision, world),
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roof,
             "kernels": kernels, "cpu_baseline": cpu, "clocks": clk, "fp64": fp64,
-            "stage_tile": "%dx%dx8 (picked by the per-context tuner)" % stage_tile,
+            "stage_tile": "%dx%dx8 columns, %d threads per block (picked by the per-context tuner)" % stage_tile,
             "reference_gpu": None if (args.no_refgpu or world > 1) else reference_gpu_sample(args.config),
         }
         print(json.dumps(out), flush=True)

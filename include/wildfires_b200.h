@@ -140,15 +140,17 @@ wf_status wf_initial_conditions(wf_ctx *ctx);
 wf_status wf_step(wf_ctx *ctx, int nsteps);
 wf_status wf_synchronize(wf_ctx *ctx);
 
-/* Tile shape (TI x TJ columns of 8 planes) of the fused stage pass.  The first
- * wf_step of a context picks it: WF_STAGE_TILE=TIxTJ in the environment forces
- * one, otherwise each compiled shape (FP32: 8x16, 8x8, 4x16; FP64: 8x8) is
- * timed on the context's own grid and state and the fastest is kept.  All
- * shapes give bit-identical results.  wf_set_stage_tile forces a shape (call
- * it before stepping; WF_ERR_ARG for a shape that is not compiled).  The tiling
- * is a property of this implementation; the reference has no counterpart. */
-wf_status wf_stage_tile(const wf_ctx *ctx, int *ti, int *tj);
-wf_status wf_set_stage_tile(wf_ctx *ctx, int ti, int tj);
+/* Tile shape of the fused stage pass: TI x TJ columns of 8 planes, processed
+ * by `threads` threads per block.  The first wf_step of a context picks it:
+ * WF_STAGE_TILE=TIxTJ[/threads] in the environment forces one, otherwise each
+ * compiled form (FP32: 8x16/512, 8x16/384, 8x8/256; FP64: 8x8/256) is timed on
+ * the context's own grid and state and the fastest is kept.  All forms give
+ * bit-identical results.  wf_set_stage_tile forces a form (threads <= 0: the
+ * first with that TI x TJ; call it before stepping; WF_ERR_ARG for a form that
+ * is not compiled).  threads may be NULL in wf_stage_tile.  The tiling is a
+ * property of this implementation; the reference has no counterpart. */
+wf_status wf_stage_tile(const wf_ctx *ctx, int *ti, int *tj, int *threads);
+wf_status wf_set_stage_tile(wf_ctx *ctx, int ti, int tj, int threads);
 
 /* Current time level n and time t[n]. */
 wf_status wf_time(const wf_ctx *ctx, int *n, double *t);

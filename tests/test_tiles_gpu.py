@@ -8,7 +8,7 @@ import pytest
 from conftest import load_golden
 
 pytestmark = pytest.mark.gpu
-SHAPES32 = [(8, 16), (8, 8), (4, 16)]
+SHAPES32 = [(8, 16, 512), (8, 16, 384), (8, 8, 256)]
 
 
 def _run(P, g, prec, shape, n):
@@ -41,7 +41,7 @@ def test_tuner_picks_a_compiled_shape(params_from_text):
     (yr, pr), _ = _run(P, g, "fp32", SHAPES32[0], 2)
     assert np.array_equal(y, yr) and np.array_equal(p, pr)
     (_, _), used64 = _run(P, g, "fp64", None, 1)
-    assert used64 == (8, 8)
+    assert used64 == (8, 8, 256)
 
 
 def test_unknown_shape_is_rejected(params_from_text):
@@ -51,3 +51,5 @@ def test_unknown_shape_is_rejected(params_from_text):
     with Solver(P, "fp32") as s:
         with pytest.raises(WfError):
             s.set_stage_tile(16, 16)
+        with pytest.raises(WfError):
+            s.set_stage_tile(8, 16, 256)

@@ -180,13 +180,13 @@ class Solver:
         return {f: getattr(d, f) for f, _ in WfDiag._fields_}
 
     def stage_tile(self):
-        """(TI, TJ) of the fused stage pass (picked by the first step)."""
-        ti, tj = C.c_int(), C.c_int()
-        check(lib().wf_stage_tile(self._h, C.byref(ti), C.byref(tj)), "wf_stage_tile")
-        return ti.value, tj.value
+        """(TI, TJ, threads) of the fused stage pass (picked by the first step)."""
+        ti, tj, nt = C.c_int(), C.c_int(), C.c_int()
+        check(lib().wf_stage_tile(self._h, C.byref(ti), C.byref(tj), C.byref(nt)), "wf_stage_tile")
+        return ti.value, tj.value, nt.value
 
-    def set_stage_tile(self, ti, tj):
-        check(lib().wf_set_stage_tile(self._h, int(ti), int(tj)), "wf_set_stage_tile")
+    def set_stage_tile(self, ti, tj, threads=0):
+        check(lib().wf_set_stage_tile(self._h, int(ti), int(tj), int(threads)), "wf_set_stage_tile")
 
     def initial_conditions(self):
         """The reference's initial conditions, generated on the GPU (time level 0)."""

@@ -116,8 +116,8 @@ def lib():
         "wf_save_domain": (C.c_int, [P, C.c_char_p]),
         "wf_save_topography": (C.c_int, [P, C.c_char_p]),
         "wf_initial_conditions": (C.c_int, [vp]),
-        "wf_stage_tile": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
-        "wf_set_stage_tile": (C.c_int, [vp, C.c_int, C.c_int]),
+        "wf_stage_tile": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "wf_set_stage_tile": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

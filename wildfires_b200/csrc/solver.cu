@@ -938,12 +938,13 @@ template <class R> wf_status tune_tiles_impl(wf_ctx *c)
     const int prec = c->prec == WF_FP64 ? 0 : 1, count = stage_tile_count(prec);
     c->tile_set = true;
     if (const char *env = getenv("WF_STAGE_TILE")) {
-        int ti = 0, tj = 0;
-        if (sscanf(env, "%dx%d", &ti, &tj) == 2)
+        int ti = 0, tj = 0, nt = 0;
+        const int got = sscanf(env, "%dx%d/%d", &ti, &tj, &nt);   // TIxTJ, optionally /threads
+        if (got >= 2)
             for (int q = 0; q < count; q++) {
-                int a = 0, b = 0;
-                stage_tile_shape(prec, q, &a, &b);
-                if (a == ti && b == tj) { c->tile = q; return WF_OK; }
+                int a = 0, b = 0, n = 0;
+                stage_tile_shape(prec, q, &a, &b, &n);
+                if (a == ti && b == tj && (got < 3 || n == nt)) { c->tile = q; return WF_OK; }
             }
         set_error("WF_STAGE_TILE=%s is not a compiled tile shape", env);
         return WF_ERR_ARG;
@@ -1086,28 +1087,28 @@ wf_status wf_timestep_reports(wf_ctx *c, wf_report *out)
     return WF_OK;
 }
 
-wf_status wf_stage_tile(const wf_ctx *c, int *ti, int *tj)
+wf_status wf_stage_tile(const wf_ctx *c, int *ti, int *tj, int *threads)
 {
     if (!c || !ti || !tj) { set_error("wf_stage_tile: null argument"); return WF_ERR_ARG; }
-    stage_tile_shape(c->prec == WF_FP64 ? 0 : 1, c->tile, ti, tj);
+    stage_tile_shape(c->prec == WF_FP64 ? 0 : 1, c->tile, ti, tj, threads);
     return WF_OK;
 }
 
-wf_status wf_set_stage_tile(wf_ctx *c, int ti, int tj)
+wf_status wf_set_stage_tile(wf_ctx *c, int ti, int tj, int threads)
 {
     if (!c) { set_error("wf_set_stage_tile: null context"); return WF_ERR_ARG; }
     const int prec = c->prec == WF_FP64 ? 0 : 1;
     for (int q = 0; q < stage_tile_count(prec); q++) {
-        int a = 0, b = 0;
-        stage_tile_shape(prec, q, &a, &b);
-        if (a == ti && b == tj) {
+        int a = 0, b = 0, n = 0;
+        stage_tile_shape(prec, q, &a, &b, &n);
+        if (a == ti && b == tj && (threads <= 0 || n == threads)) {
             c->tile = q;
             c->tile_set = true;
             drop_graphs(c);
             return WF_OK;
         }
     }
-    set_error("wf_set_stage_tile: %dx%d is not a compiled tile shape", ti, tj);
+    set_error("wf_set_stage_tile: %dx%d with %d threads is not a compiled tile shape", ti, tj, threads);
     return WF_ERR_ARG;
 }
 

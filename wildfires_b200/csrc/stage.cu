@@ -357,7 +357,7 @@ template <class R> __device__ __forceinline__ R dz5(const R *w, R m2, R m1, R c,
 //      RK update.  Cells the boundary rules overwrite (k <= cut node, top) are
 //      left to k_stage_bc; the values it needs are stored in a.bc.
 template <class R, int TI, int TJ, int KZ, int NT>
-__global__ void __launch_bounds__(NT, (NT == 256 && sizeof(R) == 4) ? (TI * TJ <= 64 ? 3 : 2) : 1) k_stage_fused(const StageArgs<R> a, int ntk, int ntj, int nti)
+__global__ void __launch_bounds__(NT, sizeof(R) != 4 ? 1 : NT > 256 ? 2 : (TI * TJ <= 64 ? 3 : 2)) k_stage_fused(const StageArgs<R> a, int ntk, int ntj, int nti)
 {
     using TL = Tile<R, TI, TJ, KZ>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -814,23 +814,26 @@ __global__ void __launch_bounds__(128) k_stage_bc(const StageArgs<R> a, int KZ)
 
 }  // namespace
 
-// Tile shapes of the fused pass: TI x TJ columns of KZ = 8 planes, 256 threads.
-// FP32 compiles three shapes (8x16 is the default; the smaller ones give more,
-// shorter blocks, which can balance small grids better); the per-context tuner
-// in solver.cu times them on the context's own grid.  FP64 has one shape.
-template <class R, int TI_, int TJ_> struct StageShape {
-    static constexpr int TI = TI_, TJ = TJ_, KZ = 8, NT = 256;
+// Tile shapes of the fused pass: TI x TJ columns of KZ = 8 planes, NT threads.
+// FP32 compiles three block forms, all at 24 or 32 warps per SM: 8x16 columns
+// with 512 threads (two blocks, 64 registers) or 384 threads (two blocks, 80
+// registers), and 8x8 columns with 256 threads (three blocks, 80 registers;
+// more halo work per cell).  The per-context tuner in solver.cu times them on
+// the context's own grid.  (Measured and dropped: 8x16 with 256 threads at 118
+// registers, 16 warps per SM, 3-4% slower; 4x16 and 4x8 tiles.)  FP64 has one.
+template <class R, int TI_, int TJ_, int NT_ = 256> struct StageShape {
+    static constexpr int TI = TI_, TJ = TJ_, KZ = 8, NT = NT_;
     using TL = Tile<R, TI, TJ, KZ>;
     static size_t smem() { return TL::bytes(); }
 };
 template <class R> struct StageShapes;
 template <> struct StageShapes<float> {
     static constexpr int count = 3;
-    static constexpr int ti[3] = {8, 8, 4}, tj[3] = {16, 8, 16};
+    static constexpr int ti[3] = {8, 8, 8}, tj[3] = {16, 16, 8}, nt[3] = {512, 384, 256};
 };
 template <> struct StageShapes<double> {
     static constexpr int count = 1;
-    static constexpr int ti[1] = {8}, tj[1] = {8};
+    static constexpr int ti[1] = {8}, tj[1] = {8}, nt[1] = {256};
 };
 
 // the shape with index idx, as a type, for f(Shape)
@@ -838,9 +841,9 @@ template <class R, class F> cudaError_t with_shape(int idx, F f)
 {
     if constexpr (sizeof(R) == 4) {
         switch (idx) {
-        case 0: return f(StageShape<R, 8, 16>());
-        case 1: return f(StageShape<R, 8, 8>());
-        case 2: return f(StageShape<R, 4, 16>());
+        case 0: return f(StageShape<R, 8, 16, 512>());
+        case 1: return f(StageShape<R, 8, 16, 384>());
+        case 2: return f(StageShape<R, 8, 8>());
         default: return cudaErrorInvalidValue;
         }
     } else {
@@ -892,14 +895,16 @@ template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t 
 
 int stage_tile_planes(int precision) { (void)precision; return 8; }
 int stage_tile_count(int precision) { return precision == 0 ? StageShapes<double>::count : StageShapes<float>::count; }
-void stage_tile_shape(int precision, int idx, int *ti, int *tj)
+void stage_tile_shape(int precision, int idx, int *ti, int *tj, int *nt)
 {
     if (precision == 0) {
         *ti = StageShapes<double>::ti[idx];
         *tj = StageShapes<double>::tj[idx];
+        if (nt) *nt = StageShapes<double>::nt[idx];
     } else {
         *ti = StageShapes<float>::ti[idx];
         *tj = StageShapes<float>::tj[idx];
+        if (nt) *nt = StageShapes<float>::nt[idx];
     }
 }
 

@@ -131,7 +131,7 @@ int stage_tile_planes(int precision);   // z planes of a fused-stage tile
 // Tile shapes compiled for the fused pass (all with the same z planes, so the
 // boundary-column list does not depend on the choice): count and TI x TJ.
 int stage_tile_count(int precision);
-void stage_tile_shape(int precision, int idx, int *ti, int *tj);
+void stage_tile_shape(int precision, int idx, int *ti, int *tj, int *nt = nullptr);
 
 template <class R>
 struct ProjectArgs {
