@@ -143,7 +143,7 @@ wf_status wf_synchronize(wf_ctx *ctx);
 /* Tile shape of the fused stage pass: TI x TJ columns of 8 planes, processed
  * by `threads` threads per block.  The first wf_step of a context picks it:
  * WF_STAGE_TILE=TIxTJ[/threads] in the environment forces one, otherwise each
- * compiled form (FP32: 8x16/512, 8x16/384, 8x8/256; FP64: 8x8/256) is timed on
+ * compiled form (FP32: 8x16/512, 8x16/384, 8x8/256; FP64: 8x8/512, 8x8/256) is timed on
  * the context's own grid and state and the fastest is kept.  All forms give
  * bit-identical results.  wf_set_stage_tile forces a form (threads <= 0: the
  * first with that TI x TJ; call it before stepping; WF_ERR_ARG for a form that

@@ -820,7 +820,9 @@ __global__ void __launch_bounds__(128) k_stage_bc(const StageArgs<R> a, int KZ)
 // registers), and 8x8 columns with 256 threads (three blocks, 80 registers;
 // more halo work per cell).  The per-context tuner in solver.cu times them on
 // the context's own grid.  (Measured and dropped: 8x16 with 256 threads at 118
-// registers, 16 warps per SM, 3-4% slower; 4x16 and 4x8 tiles.)  FP64 has one.
+// registers, 16 warps per SM, 3-4% slower; 4x16 and 4x8 tiles.)  FP64: 8x8
+// columns with 512 threads (one block, 124 registers, 16 warps: 8.20 -> 6.09 ms
+// per launch at 512x512x128) or 256 threads (200 registers, 8 warps).
 template <class R, int TI_, int TJ_, int NT_ = 256> struct StageShape {
     static constexpr int TI = TI_, TJ = TJ_, KZ = 8, NT = NT_;
     using TL = Tile<R, TI, TJ, KZ>;
@@ -832,8 +834,8 @@ template <> struct StageShapes<float> {
     static constexpr int ti[3] = {8, 8, 8}, tj[3] = {16, 16, 8}, nt[3] = {512, 384, 256};
 };
 template <> struct StageShapes<double> {
-    static constexpr int count = 1;
-    static constexpr int ti[1] = {8}, tj[1] = {8}, nt[1] = {256};
+    static constexpr int count = 2;
+    static constexpr int ti[2] = {8, 8}, tj[2] = {8, 8}, nt[2] = {512, 256};
 };
 
 // the shape with index idx, as a type, for f(Shape)
@@ -847,8 +849,11 @@ template <class R, class F> cudaError_t with_shape(int idx, F f)
         default: return cudaErrorInvalidValue;
         }
     } else {
-        if (idx != 0) return cudaErrorInvalidValue;
-        return f(StageShape<R, 8, 8>());
+        switch (idx) {
+        case 0: return f(StageShape<R, 8, 8, 512>());
+        case 1: return f(StageShape<R, 8, 8>());
+        default: return cudaErrorInvalidValue;
+        }
     }
 }
 
