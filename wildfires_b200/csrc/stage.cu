@@ -308,15 +308,19 @@ __device__ __forceinline__ void issue_tile(const StageArgs<R> &a, TL &t, int i0,
     if constexpr (TL::PAIRED && TL::SK * TL::SJ <= NT) {
         // FP32 tile: thread (k, j) of the SK x SJ cross-section walks the SI
         // planes in i, so the k/j arithmetic and the j wrap happen once per
-        // thread (lanes k fastest: global reads stay coalesced along k)
-        if (threadIdx.x < TL::SK * TL::SJ) {
-            const int kk = threadIdx.x % TL::SK - 2, jj = threadIdx.x / TL::SK - 2;
+        // thread (lanes k fastest: global reads stay coalesced along k).  With
+        // twice the threads, two threads share a (k, j), half the planes each.
+        constexpr int KJ = TL::SK * TL::SJ, NSPLIT = (NT >= 2 * KJ && TL::SI % 2 == 0) ? 2 : 1;
+        if (threadIdx.x < KJ * NSPLIT) {
+            const int kj = threadIdx.x % KJ, part = threadIdx.x / KJ;
+            const int kk = kj % TL::SK - 2, jj = kj / TL::SK - 2;
             const int gk = k0 + kk, gj = j0 + jj;
             const bool okjk = gk >= 0 && gk < Nz && gj <= Ny + 1;
             const size_t cj = okjk ? (size_t)wrap_p(gj, Ny - 1) * Nz + gk : 0;
             const size_t plane = (size_t)Ny * Nz;
-#pragma unroll 4
-            for (int ii = -2; ii < TL::SI - 2; ii++) {
+            const int ii0 = -2 + part * (TL::SI / NSPLIT);
+#pragma unroll 2
+            for (int ii = ii0; ii < ii0 + TL::SI / NSPLIT; ii++) {
                 const int gi = i0 + ii;
                 const bool ok = okjk && gi <= Nx + 1;
                 const size_t o = ok ? (size_t)wrap_p(gi, Nx - 1) * plane + cj : 0;
