@@ -300,13 +300,23 @@ __global__ void __launch_bounds__(256, kFftMinBlocks)
 
 // P3: tridiagonal solve in z per (r, s) (pressure.cu:356-390, 473-504, 418-443).
 // zt holds per-k constants: [0..nk) a, [nk..2nk) c, [2nk..3nk) D (b = -(kk + D)),
-// followed by b0, c0base, inv_dz1, half_dz0, cl.  The right-hand sides are
-// fetched eight planes ahead of the recurrence so the loads overlap.
+// followed by b0, c0base, inv_dz1, half_dz0, cl.  Thomas algorithm without
+// storing its forward sweep: the forward pass keeps only the modified
+// diagonal u and right-hand side y at the end of every kSeg-plane segment
+// (local checkpoints); the back substitution walks the segments from the top,
+// recomputes each segment's u and y from the previous checkpoint and the
+// original right-hand sides (still in G: a segment's solution is written only
+// after it has been recomputed), then solves it.  The recomputation repeats the
+// forward pass operation for operation, so the result is that of the plain
+// two-sweep form, while G is read twice and written once (the two-sweep form
+// also writes and re-reads the modified right-hand sides, and spills u).
+constexpr int kSeg = 4;
+constexpr int kMaxSeg = 128;   // nk <= kSeg * kMaxSeg = 512 planes (Nz <= 513)
+
 __global__ void __launch_bounds__(128, 8) k_p_tridiag(double2 *__restrict__ G, const double *__restrict__ kx2,
                                                    const double *__restrict__ ky2, const double *__restrict__ zt,
                                                    int n0, int h1, int nk)
 {
-    constexpr int CH = 8;
     const int r = blockIdx.x;
     const int s = blockIdx.y * blockDim.x + threadIdx.x;
     if (s >= h1) return;
@@ -314,55 +324,72 @@ __global__ void __launch_bounds__(128, 8) k_p_tridiag(double2 *__restrict__ G, c
     const double *za = zt, *zcc = zt + nk, *zD = zt + 2 * nk;
     const double b0 = zt[3 * nk], c0base = zt[3 * nk + 1], inv_dz1 = zt[3 * nk + 2];
     const double half_dz0 = zt[3 * nk + 3], cl = zt[3 * nk + 4];
+    const double c0 = c0base - half_dz0 * kk2 - inv_dz1;   // c[0]
     const size_t stride = (size_t)n0 * h1;
     double2 *g = G + (size_t)r * h1 + s;
-    double uk[256];
     // row 0 uses the source of slice 1; rows 1..nk-2 their own; the last row
     // subtracts the top pressure divided by its coupling coefficient
     const double2 pt = g[stride * nk];
-    const double2 d0 = g[stride * 1];
-    double2 y = make_double2(half_dz0 * d0.x, half_dz0 * d0.y);
-    double u = b0;
-    uk[0] = u;
-    double cprev = c0base - half_dz0 * kk2 - inv_dz1;   // c[0]
-    g[0] = y;
-    for (int k0 = 1; k0 < nk; k0 += CH) {
-        double2 dv[CH];
+    const double2 d1 = g[stride * 1];
+    const double y0x = half_dz0 * d1.x, y0y = half_dz0 * d1.y;
+    double cku[kMaxSeg];   // u at the last plane of each segment
+    double2 cky[kMaxSeg];  // y there
+    const int nseg = (nk + kSeg - 1) / kSeg;
+    // one step of the forward recurrence at plane k >= 1 (u, y: values at k-1 on entry)
+    auto fwd = [&](int k, double2 dk, double &u, double2 &y) {
+        const double l = za[k - 1] / u;
+        const double cprev = (k == 1) ? c0 : zcc[k - 1];
+        const double bk = -(kk2 + zD[k]);
+        u = bk - l * cprev;
+        if (k == nk - 1) dk = make_double2(dk.x - pt.x / cl, dk.y - pt.y / cl);
+        y = make_double2(dk.x - l * y.x, dk.y - l * y.y);
+    };
+    // forward pass: checkpoints only
+    {
+        double u = b0;
+        double2 y = make_double2(y0x, y0y);
+        for (int m = 0; m < nseg; m++) {
+            const int kb = m * kSeg;
+            double2 dv[kSeg];
 #pragma unroll
-        for (int q = 0; q < CH; q++)
-            if (k0 + q < nk) dv[q] = g[stride * (k0 + q)];
+            for (int q = 0; q < kSeg; q++)
+                if (kb + q >= 1 && kb + q < nk) dv[q] = g[stride * (kb + q)];
 #pragma unroll
-        for (int q = 0; q < CH; q++) {
-            const int k = k0 + q;
-            if (k < nk) {
-                const double l = za[k - 1] / u;
-                const double bk = -(kk2 + zD[k]);
-                u = bk - l * cprev;
-                uk[k & 255] = u;
-                double2 dk = dv[q];
-                if (k == nk - 1) dk = make_double2(dk.x - pt.x / cl, dk.y - pt.y / cl);
-                y = make_double2(dk.x - l * y.x, dk.y - l * y.y);
-                g[stride * k] = y;
-                cprev = zcc[k];
-            }
+            for (int q = 0; q < kSeg; q++)
+                if (kb + q >= 1 && kb + q < nk) fwd(kb + q, dv[q], u, y);
+            cku[m] = u;
+            cky[m] = y;
         }
     }
-    double2 x = make_double2(y.x / u, y.y / u);
-    g[stride * (nk - 1)] = x;
-    for (int k0 = nk - 2; k0 >= 0; k0 -= CH) {
-        double2 yv[CH];
+    // back substitution, one recomputed segment at a time from the top
+    double2 x = make_double2(0.0, 0.0);
+    for (int m = nseg - 1; m >= 0; m--) {
+        const int kb = m * kSeg;
+        double u = (m == 0) ? b0 : cku[m - 1];
+        double2 y = (m == 0) ? make_double2(y0x, y0y) : cky[m - 1];
+        double uu[kSeg];
+        double2 yy[kSeg], dv[kSeg];
 #pragma unroll
-        for (int q = 0; q < CH; q++)
-            if (k0 - q >= 0) yv[q] = g[stride * (k0 - q)];
+        for (int q = 0; q < kSeg; q++)
+            if (kb + q >= 1 && kb + q < nk) dv[q] = g[stride * (kb + q)];
 #pragma unroll
-        for (int q = 0; q < CH; q++) {
-            const int k = k0 - q;
-            if (k >= 0) {
-                const double ck = (k == 0) ? (c0base - half_dz0 * kk2 - inv_dz1) : zcc[k];
-                const double uu = uk[k & 255];
-                x = make_double2((yv[q].x - ck * x.x) / uu, (yv[q].y - ck * x.y) / uu);
-                g[stride * k] = x;
+        for (int q = 0; q < kSeg; q++) {
+            if (kb + q >= nk) continue;
+            if (kb + q >= 1) fwd(kb + q, dv[q], u, y);
+            uu[q] = u;
+            yy[q] = y;
+        }
+#pragma unroll
+        for (int q = kSeg - 1; q >= 0; q--) {
+            const int k = kb + q;
+            if (k >= nk) continue;
+            if (k == nk - 1) {
+                x = make_double2(yy[q].x / uu[q], yy[q].y / uu[q]);
+            } else {
+                const double ck = (k == 0) ? c0 : zcc[k];
+                x = make_double2((yy[q].x - ck * x.x) / uu[q], (yy[q].y - ck * x.y) / uu[q]);
             }
+            g[stride * k] = x;
         }
     }
 }
@@ -530,6 +557,7 @@ cudaError_t launch_poisson_impl(const PoissonArgs<R> &a, const double *zt, cudaS
     double2 *G = a.G;
     if ((e = by_length<LaunchFx<false>>(a.fx.L, G, a.fx, ns, n0, h1, s))) return e;
     if (ev) cudaEventRecord(ev[1], s);
+    if (nk > kSeg * kMaxSeg) return cudaErrorInvalidValue;
     k_p_tridiag<<<dim3(n0, (h1 + 127) / 128), 128, 0, s>>>(a.G, a.kx2, a.ky2, zt, n0, h1, nk);
     if (ev) cudaEventRecord(ev[2], s);
     ns = nk;
