@@ -97,25 +97,71 @@ Dumper *dumper_create(int device, const Parameters &P, size_t S, size_t N)
     return d;
 }
 
+// Releases what a failed set-up allocated, so that a later dump tries again.
+static void dumper_release(Dumper *d)
+{
+    for (int b = 0; b < 2; b++) {
+        if (d->d2h[b]) cudaEventDestroy(d->d2h[b]);
+        if (d->h[b]) cudaFreeHost(d->h[b]);
+        d->d2h[b] = nullptr;
+        d->h[b] = nullptr;
+    }
+    if (d->staged) cudaEventDestroy(d->staged);
+    if (d->cs) cudaStreamDestroy(d->cs);
+    if (d->d_stage) cudaFree(d->d_stage);
+    d->staged = nullptr;
+    d->cs = nullptr;
+    d->d_stage = nullptr;
+    cudaGetLastError();
+}
+
 static wf_status dumper_setup(Dumper *d)
 {
     const size_t bytes = sizeof(double) * (d->S + d->N);
-    if (cudaMalloc(&d->d_stage, bytes) != cudaSuccess) {
-        cudaGetLastError();
+    bool ok = cudaMalloc(&d->d_stage, bytes) == cudaSuccess;
+    if (!ok) {
+        dumper_release(d);
         set_error("dump: device snapshot of %zu bytes could not be allocated", bytes);
         return WF_ERR_OOM;
     }
-    for (int b = 0; b < 2; b++)
-        if (cudaHostAlloc((void **)&d->h[b], bytes, cudaHostAllocDefault) != cudaSuccess) {
-            cudaGetLastError();
-            set_error("dump: pinned host buffer of %zu bytes could not be allocated", bytes);
-            return WF_ERR_OOM;
-        }
-    WF_TRY_CUDA(cudaStreamCreateWithFlags(&d->cs, cudaStreamNonBlocking));
-    WF_TRY_CUDA(cudaEventCreateWithFlags(&d->staged, cudaEventDisableTiming));
-    for (int b = 0; b < 2; b++) WF_TRY_CUDA(cudaEventCreateWithFlags(&d->d2h[b], cudaEventDisableTiming));
+    for (int b = 0; b < 2 && ok; b++) ok = cudaHostAlloc((void **)&d->h[b], bytes, cudaHostAllocDefault) == cudaSuccess;
+    if (!ok) {
+        dumper_release(d);
+        set_error("dump: pinned host buffer of %zu bytes could not be allocated", bytes);
+        return WF_ERR_OOM;
+    }
+    cudaError_t e = cudaStreamCreateWithFlags(&d->cs, cudaStreamNonBlocking);
+    if (!e) e = cudaEventCreateWithFlags(&d->staged, cudaEventDisableTiming);
+    for (int b = 0; b < 2 && !e; b++) e = cudaEventCreateWithFlags(&d->d2h[b], cudaEventDisableTiming);
+    if (e) {
+        dumper_release(d);
+        set_error("dump: stream or event creation failed: %s", cudaGetErrorString(e));
+        return WF_ERR_CUDA;
+    }
     d->writer = std::thread([d] { d->run(); });
     return WF_OK;
+}
+
+// Device side of one dump into host buffer b (snapshot, then copy to host).
+static cudaError_t dumper_copy(Dumper *d, cudaStream_t s, const void *state, bool fp32, const double *p, int b)
+{
+    cudaError_t e = cudaSuccess;
+    // the previous dump's copy must have left the snapshot before it is rewritten
+    if (d->d2h_pending) e = cudaStreamWaitEvent(s, d->d2h[1 - b], 0);
+    if (!e) {
+        if (fp32) {
+            k_widen<<<592, 256, 0, s>>>(d->d_stage, (const float *)state, d->S);
+            e = cudaGetLastError();
+        } else {
+            e = cudaMemcpyAsync(d->d_stage, state, sizeof(double) * d->S, cudaMemcpyDeviceToDevice, s);
+        }
+    }
+    if (!e) e = cudaMemcpyAsync(d->d_stage + d->S, p, sizeof(double) * d->N, cudaMemcpyDeviceToDevice, s);
+    if (!e) e = cudaEventRecord(d->staged, s);
+    if (!e) e = cudaStreamWaitEvent(d->cs, d->staged, 0);
+    if (!e) e = cudaMemcpyAsync(d->h[b], d->d_stage, sizeof(double) * (d->S + d->N), cudaMemcpyDeviceToHost, d->cs);
+    if (!e) e = cudaEventRecord(d->d2h[b], d->cs);
+    return e;
 }
 
 wf_status dumper_enqueue(Dumper *d, cudaStream_t s, const void *state, bool fp32, const double *p, const char *dir,
@@ -133,19 +179,16 @@ wf_status dumper_enqueue(Dumper *d, cudaStream_t s, const void *state, bool fp32
         d->busy[b] = true;
         d->next = 1 - b;
     }
-    // the previous dump's copy must have left the snapshot before it is rewritten
-    if (d->d2h_pending) WF_TRY_CUDA(cudaStreamWaitEvent(s, d->d2h[1 - b], 0));
-    if (fp32) {
-        k_widen<<<592, 256, 0, s>>>(d->d_stage, (const float *)state, d->S);
-        WF_TRY_CUDA(cudaGetLastError());
-    } else {
-        WF_TRY_CUDA(cudaMemcpyAsync(d->d_stage, state, sizeof(double) * d->S, cudaMemcpyDeviceToDevice, s));
+    const cudaError_t e = dumper_copy(d, s, state, fp32, p, b);
+    if (e) {
+        {
+            std::lock_guard<std::mutex> lk(d->mu);
+            d->busy[b] = false;   // nothing will write this buffer: free it again
+        }
+        d->cv.notify_all();
+        set_error("dump: %s", cudaGetErrorString(e));
+        return WF_ERR_CUDA;
     }
-    WF_TRY_CUDA(cudaMemcpyAsync(d->d_stage + d->S, p, sizeof(double) * d->N, cudaMemcpyDeviceToDevice, s));
-    WF_TRY_CUDA(cudaEventRecord(d->staged, s));
-    WF_TRY_CUDA(cudaStreamWaitEvent(d->cs, d->staged, 0));
-    WF_TRY_CUDA(cudaMemcpyAsync(d->h[b], d->d_stage, sizeof(double) * (d->S + d->N), cudaMemcpyDeviceToHost, d->cs));
-    WF_TRY_CUDA(cudaEventRecord(d->d2h[b], d->cs));
     d->d2h_pending = true;
     {
         std::lock_guard<std::mutex> lk(d->mu);
@@ -180,13 +223,7 @@ void dumper_destroy(Dumper *d)
         d->writer.join();
     }
     if (d->cs) cudaStreamSynchronize(d->cs);
-    for (int b = 0; b < 2; b++) {
-        if (d->d2h[b]) cudaEventDestroy(d->d2h[b]);
-        if (d->h[b]) cudaFreeHost(d->h[b]);
-    }
-    if (d->staged) cudaEventDestroy(d->staged);
-    if (d->cs) cudaStreamDestroy(d->cs);
-    if (d->d_stage) cudaFree(d->d_stage);
+    dumper_release(d);
     delete d;
 }
 
