@@ -27,6 +27,34 @@ struct Part {
 
 __device__ __forceinline__ double dmax(double a, double b) { return (b > a || b != b) ? b : a; }
 
+// the 13 reduced values of a Part, in its memory order: sums, extrema, NaN count
+constexpr int kVals = kSums + kExt + 1;
+static_assert(sizeof(Part) == kVals * sizeof(double), "Part is a plain array of doubles");
+__host__ __device__ constexpr bool is_sum(int q) { return q < kSums || q == kVals - 1; }
+__device__ __forceinline__ double combine(int q, double a, double b) { return is_sum(q) ? a + b : dmax(a, b); }
+
+// Reduces v over the block (warp butterflies, then the warps in order) and
+// writes the kVals results to dst.  Every thread of the block must call it.
+__device__ __forceinline__ void block_reduce(double (&v)[kVals], double *dst)
+{
+    __shared__ double red[kDiagThreads / 32][kVals];
+#pragma unroll
+    for (int q = 0; q < kVals; q++)
+        for (int o = 16; o > 0; o >>= 1) v[q] = combine(q, v[q], __shfl_xor_sync(0xffffffffu, v[q], o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < kVals; q++) red[warp][q] = v[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < kVals) {
+        const int q = threadIdx.x;
+        double r = red[0][q];
+        for (int w = 1; w < kDiagThreads / 32; w++) r = combine(q, r, red[w][q]);
+        dst[q] = r;
+    }
+}
+
 template <class R>
 __global__ void __launch_bounds__(kDiagThreads) k_diag_part(const Geom g, const Phys ph, const R *__restrict__ y,
                                                             Part *__restrict__ parts)
@@ -66,39 +94,29 @@ __global__ void __launch_bounds__(kDiagThreads) k_diag_part(const Geom g, const 
             if (k < nzy) s[2] += Yv * dV;
         }
     }
-    __shared__ double sh[kDiagThreads];
-    Part out;
-    for (int q = 0; q < kSums + kExt + 1; q++) {
-        double v = (q < kSums) ? s[q] : (q < kSums + kExt) ? e[q - kSums] : nan;
-        sh[threadIdx.x] = v;
-        __syncthreads();
-        for (int h = kDiagThreads / 2; h > 0; h >>= 1) {
-            if (threadIdx.x < h) {
-                const double o = sh[threadIdx.x + h];
-                sh[threadIdx.x] = (q < kSums || q == kSums + kExt) ? sh[threadIdx.x] + o : dmax(sh[threadIdx.x], o);
-            }
-            __syncthreads();
-        }
-        if (q < kSums) out.sum[q] = sh[0];
-        else if (q < kSums + kExt) out.ext[q - kSums] = sh[0];
-        else out.nan = sh[0];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) parts[blockIdx.x] = out;
+    double v[kVals];
+#pragma unroll
+    for (int q = 0; q < kSums; q++) v[q] = s[q];
+#pragma unroll
+    for (int q = 0; q < kExt; q++) v[kSums + q] = e[q];
+    v[kVals - 1] = nan;
+    block_reduce(v, reinterpret_cast<double *>(parts + blockIdx.x));
 }
 
-__global__ void k_diag_final(const Part *__restrict__ parts, int n, double *__restrict__ out)
+// One block: thread t folds partials t, t + 256, ... in that order, then the
+// block reduction (a fixed order: results are bit-reproducible).
+__global__ void __launch_bounds__(kDiagThreads) k_diag_final(const Part *__restrict__ parts, int n,
+                                                             double *__restrict__ out)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    Part r = parts[0];
-    for (int b = 1; b < n; b++) {
-        for (int q = 0; q < kSums; q++) r.sum[q] += parts[b].sum[q];
-        for (int q = 0; q < kExt; q++) r.ext[q] = dmax(r.ext[q], parts[b].ext[q]);
-        r.nan += parts[b].nan;
+    double v[kVals];
+#pragma unroll
+    for (int q = 0; q < kVals; q++) v[q] = is_sum(q) ? 0.0 : -INFINITY;
+    for (int b = threadIdx.x; b < n; b += kDiagThreads) {
+        const double *pb = reinterpret_cast<const double *>(parts + b);
+#pragma unroll
+        for (int q = 0; q < kVals; q++) v[q] = combine(q, v[q], pb[q]);
     }
-    for (int q = 0; q < kSums; q++) out[q] = r.sum[q];
-    for (int q = 0; q < kExt; q++) out[kSums + q] = r.ext[q];
-    out[kSums + kExt] = r.nan;
+    block_reduce(v, out);
 }
 
 }  // namespace
@@ -111,7 +129,7 @@ cudaError_t launch_diag(const Geom &g, const Phys &ph, const R *y, const R *unus
     (void)unused;
     Part *parts = reinterpret_cast<Part *>(scratch + 16);
     k_diag_part<R><<<kDiagBlocks, kDiagThreads, 0, s>>>(g, ph, y, parts);
-    k_diag_final<<<1, 32, 0, s>>>(parts, kDiagBlocks, scratch);
+    k_diag_final<<<1, kDiagThreads, 0, s>>>(parts, kDiagBlocks, scratch);
     return cudaGetLastError();
 }
 template cudaError_t launch_diag<double>(const Geom &, const Phys &, const double *, const double *, double *, cudaStream_t);

@@ -86,16 +86,44 @@ __global__ void __launch_bounds__(kRepThreads) k_report_part(const Geom g, const
     if (threadIdx.x == 0) parts[blockIdx.x] = out;
 }
 
-__global__ void k_report_final(const RepPart *__restrict__ parts, int n, double *__restrict__ out)
+// One block: thread t folds partials t, t + 256, ..., then warp butterflies
+// and the warps in order (maxima and the smallest key: any order gives the
+// same result).
+__global__ void __launch_bounds__(kRepThreads) k_report_final(const RepPart *__restrict__ parts, int n,
+                                                              double *__restrict__ out)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    RepPart r = parts[0];
-    for (int b = 1; b < n; b++) {
-        for (int q = 0; q < 7; q++) r.ext[q] = rmax(r.ext[q], parts[b].ext[q]);
-        r.nan = min(r.nan, parts[b].nan);
+    double e[7];
+#pragma unroll
+    for (int q = 0; q < 7; q++) e[q] = -INFINITY;
+    unsigned long long key = ~0ull;
+    for (int b = threadIdx.x; b < n; b += kRepThreads) {
+#pragma unroll
+        for (int q = 0; q < 7; q++) e[q] = rmax(e[q], parts[b].ext[q]);
+        key = min(key, parts[b].nan);
     }
-    for (int q = 0; q < 7; q++) out[q] = r.ext[q];
-    reinterpret_cast<unsigned long long *>(out)[7] = r.nan;
+#pragma unroll
+    for (int q = 0; q < 7; q++)
+        for (int o = 16; o > 0; o >>= 1) e[q] = rmax(e[q], __shfl_xor_sync(0xffffffffu, e[q], o));
+    for (int o = 16; o > 0; o >>= 1) key = min(key, __shfl_xor_sync(0xffffffffu, key, o));
+    __shared__ double red[kRepThreads / 32][7];
+    __shared__ unsigned long long redk[kRepThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < 7; q++) red[warp][q] = e[q];
+        redk[warp] = key;
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        const int q = threadIdx.x;
+        double r = red[0][q];
+        for (int w = 1; w < kRepThreads / 32; w++) r = rmax(r, red[w][q]);
+        out[q] = r;
+    } else if (threadIdx.x == 7) {
+        unsigned long long k = redk[0];
+        for (int w = 1; w < kRepThreads / 32; w++) k = min(k, redk[w]);
+        reinterpret_cast<unsigned long long *>(out)[7] = k;
+    }
 }
 
 }  // namespace
@@ -109,7 +137,7 @@ cudaError_t launch_report(const Geom &g, const R *y, const double *xg, const dou
     RepPart *parts = reinterpret_cast<RepPart *>(scratch + 8);
     k_report_part<R><<<kRepBlocks, kRepThreads, 0, s>>>(g, y, xg, yg, make_double4(rect[0], rect[1], rect[2], rect[3]),
                                                          parts);
-    k_report_final<<<1, 32, 0, s>>>(parts, kRepBlocks, scratch);
+    k_report_final<<<1, kRepThreads, 0, s>>>(parts, kRepBlocks, scratch);
     return cudaGetLastError();
 }
 template cudaError_t launch_report<double>(const Geom &, const double *, const double *, const double *,
