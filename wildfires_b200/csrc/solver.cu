@@ -366,6 +366,13 @@ Phys make_phys(const Parameters &P)
     ph.sutherland_conductivity = P.sutherland_conductivity;
     ph.variable_density = P.variable_density;
     ph.velocity_correction_fd = P.velocity_correction_fd;
+    if (P.z && P.Nz >= 3) {
+        const int k = P.Nz - 1;
+        const double a1 = P.z[k] - P.z[k - 1], a2 = P.z[k - 1] - P.z[k - 2];
+        const double den = a2 * (a2 + 2 * a1);
+        ph.top_w1 = (a2 + a1) * (a2 + a1) / den;
+        ph.top_w2 = a1 * a1 / den;
+    }
     return ph;
 }
 

@@ -46,6 +46,8 @@ struct Phys {
     double u_dead, v_dead, w_dead, T_dead, Y_dead;
     int temperature_convection, sutherland_viscosity, sutherland_conductivity;
     int variable_density, velocity_correction_fd;
+    // top-plane extrapolation f_{Nz-1} = top_w1 f_{Nz-2} - top_w2 f_{Nz-3} (FP32 projection path)
+    double top_w1, top_w2;
 };
 
 // Model scalars in the stencil precision R, derived once on the host from
@@ -148,6 +150,8 @@ struct ProjectArgs {
     double TS[12];         // source box/gaussian parameters (ramped source)
     int TS_gauss;
     double T_source;
+    // FP32 path constants, set by launch_project: 0.5/dx, 0.5/dy, dt/rho_inf, dt/(T_inf rho_inf)
+    double hx, hy, s_rho0, s_rhoT;
 };
 template <class R> cudaError_t launch_project(const ProjectArgs<R> &a, cudaStream_t s);
 
