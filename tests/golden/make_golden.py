@@ -3,7 +3,7 @@ solver (its src/cu sources compiled for the CPU by oracle/Makefile -> oracle/_re
 
 Run from the repository root in a container where the reference tree exists:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [name ...]
 
 Each fixture <name>.npz holds the parameter file text, the reference parser's
 view of the grid (z, Nz_Y, cut_nodes), the seeded initial state and the
@@ -47,13 +47,28 @@ def cases():
                                     pressure_solver_iter=3, pressure_solver_tol=-1.0)
     # more steps on a slightly larger grid (growth of rounding differences)
     c["flat_33x33x16_10"] = configs.flat(Nx=33, Ny=33, Nz=16, Nt=10, jitter=0.1, seed=6)
+    # ramped temperature sources (temperature_source_delay, src/cu/functions.cu:325-380):
+    # gaussian, ramp ending within the run; box, source switched off before the last step
+    c["ramp_gauss_rk4"] = configs.hill(Nx=13, Ny=13, Nz=12, Nt=3, jitter=0.2, seed=7, L=30.0, H=8.0,
+                                       t_source_start=2.5 * 0.003, t_source_end=10 * 0.003,
+                                       T_source_shape="gaussian", T_source=800.0, TS_x_start=8.0,
+                                       TS_x_end=16.0, TS_y_start=10.0, TS_y_end=20.0, TS_z_start=0.0,
+                                       TS_z_end=2.0)
+    c["ramp_box_euler"] = configs.flat(Nx=13, Ny=13, Nz=12, Nt=3, jitter=0.2, seed=8, method="Euler",
+                                       t_source_start=1.5 * 0.005, t_source_end=2.5 * 0.005,
+                                       T_source_shape="parallelepiped", T_source=700.0, TS_x_start=40.0,
+                                       TS_x_end=90.0, TS_y_start=60.0, TS_y_end=140.0, TS_z_start=0.0,
+                                       TS_z_end=3.0)
     return c
 
 
 def main():
     if not ref_runner.available("host"):
         sys.exit("oracle/_ref/ref_host missing: run `make -C oracle ref` where the reference tree exists")
+    only = set(sys.argv[1:])   # optional: fixture names to (re)generate
     for name, case in cases().items():
+        if only and name not in only:
+            continue
         data = {"params": np.array(configs.param_text(case.params))}
         res = ref_runner.run(case, "phi")
         P = res["P"]
