@@ -98,3 +98,40 @@ def test_create_without_device_reports_no_device(params_from_text):
     with pytest.raises(WfError) as e:
         Solver(P)
     assert e.value.status in (2, 7)
+
+
+@pytest.mark.parametrize("text,expect", [
+    ("Nx = 8\nNy = 8\nNz = 258\n", "Nz-1 must be <= 256"),        # longest tridiagonal system
+    ("Nx = 2050\nNy = 5\nNz = 8\n", "Nx-1 and Ny-1 must be <= 2048"),  # longest transform
+    ("Nx = 5\nNy = 2050\nNz = 8\n", "Nx-1 and Ny-1 must be <= 2048"),
+    ("Nx = 8\nNy = 8\nNz = 4\n", "too small"),   # the parser takes Nz = 4, the solver needs 5
+])
+def test_create_rejects_grids_beyond_the_engine_limits(text, expect, params_from_text):
+    """Argument checks come before any device call, so they hold on any host."""
+    from wildfires_b200 import Solver, WfError
+    P = params_from_text(text + "Nt = 1\nx_max = 7\ny_max = 7\nz_max = 7\nt_max = 1\n")
+    with pytest.raises(WfError) as e:
+        Solver(P)
+    assert e.value.status == 1 and expect in str(e.value), str(e.value)
+
+
+def test_parser_rejects_grids_below_four_nodes(params_from_text):
+    from wildfires_b200 import WfError
+    with pytest.raises(WfError) as e:
+        params_from_text("Nx = 3\nNy = 8\nNz = 8\nNt = 1\nx_max = 7\ny_max = 7\nz_max = 7\nt_max = 1\n")
+    assert e.value.status == 4 and "Nx, Ny, Nz >= 4" in str(e.value), str(e.value)
+
+
+def test_create_rejects_unknown_precision_and_high_terrain(params_from_text):
+    from wildfires_b200 import Solver, WfError, _abi
+    P = params_from_text("Nx = 8\nNy = 8\nNz = 8\nNt = 1\nx_max = 7\ny_max = 7\nz_max = 7\nt_max = 1\n")
+    h = C.c_void_p()
+    assert _abi.lib().wf_create(C.byref(P.rec), 7, C.byref(h)) == 1 and not h.value
+    assert b"unknown precision" in _abi.lib().wf_last_error()
+    # a column whose terrain reaches the top planes leaves no room for the boundary rules
+    topo = np.zeros((8, 8))
+    topo[3, 4] = 6.5
+    P.set_topography(topo)
+    with pytest.raises(WfError) as e:
+        Solver(P)
+    assert e.value.status == 1 and "above Nz-4" in str(e.value), str(e.value)
