@@ -791,7 +791,10 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
     if ((st = dev_alloc(c, (void **)&c->p_prev, sizeof(double) * c->N))) return fail(st);
     if ((st = dev_alloc(c, (void **)&c->G, sizeof(double2) * (size_t)Nz * (Nx - 1) * c->h1))) return fail(st);
     if ((st = dev_alloc(c, (void **)&c->rec, sizeof(PIterRec)))) return fail(st);
-    WF_TRY_CUDA(cudaMemset(c->rec, 0, sizeof(PIterRec)));
+    if (cudaMemset(c->rec, 0, sizeof(PIterRec)) != cudaSuccess) {
+        set_error("wf_create: clearing the pressure-loop record failed");
+        return fail(WF_ERR_CUDA);
+    }
     if (cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess) {
         set_error("wf_create: stream creation failed");
         return fail(WF_ERR_CUDA);
@@ -847,8 +850,9 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
         c->nbcfix = (int)fix.size();
         if (!fix.empty() && (st = upload(c, &c->d_bcfix, fix.data(), fix.size()))) return fail(st);
     }
-    WF_TRY_CUDA(cudaMemsetAsync(c->p, 0, sizeof(double) * c->N, c->stream));
-    WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+    e = cudaMemsetAsync(c->p, 0, sizeof(double) * c->N, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) { set_error("wf_create: %s", cudaGetErrorString(e)); return fail(WF_ERR_CUDA); }
     c->launches = launches_per_step(c);
     *out = c;
     return WF_OK;
