@@ -1025,11 +1025,14 @@ wf_status wf_step(wf_ctx *c, int nsteps)
         if (step_is_static(c, n1)) {
             cudaGraphExec_t &ge = c->graph[c->cur];
             if (!ge) {
-                cudaGraph_t gph;
+                cudaGraph_t gph = nullptr;
                 WF_TRY_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
                 wf_status st = enqueue_step_any(c, c->cur, n1);
                 cudaError_t e = cudaStreamEndCapture(c->stream, &gph);
-                if (st) return st;
+                if (st) {
+                    if (gph) cudaGraphDestroy(gph);
+                    return st;
+                }
                 if (e != cudaSuccess) { set_error("wf_step: capture failed: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
                 e = cudaGraphInstantiate(&ge, gph, 0);
                 cudaGraphDestroy(gph);
@@ -1361,11 +1364,14 @@ wf_status wf_ensemble_step(wf_ensemble *e, int nsteps)
         if (same && fixed) {
             cudaGraphExec_t &ge = e->graph[e->m[0]->cur];
             if (!ge) {
-                cudaGraph_t gph;
+                cudaGraph_t gph = nullptr;
                 WF_TRY_CUDA(cudaStreamBeginCapture(e->master, cudaStreamCaptureModeThreadLocal));
                 wf_status st = ensemble_enqueue(e);
                 cudaError_t err = cudaStreamEndCapture(e->master, &gph);
-                if (st) return st;
+                if (st) {
+                    if (gph) cudaGraphDestroy(gph);
+                    return st;
+                }
                 if (err != cudaSuccess) { set_error("wf_ensemble_step: capture failed: %s", cudaGetErrorString(err)); return WF_ERR_CUDA; }
                 err = cudaGraphInstantiate(&ge, gph, 0);
                 cudaGraphDestroy(gph);
