@@ -135,3 +135,62 @@ def test_create_rejects_unknown_precision_and_high_terrain(params_from_text):
     with pytest.raises(WfError) as e:
         Solver(P)
     assert e.value.status == 1 and "above Nz-4" in str(e.value), str(e.value)
+
+
+def test_every_entry_point_rejects_null_arguments():
+    """Null handles and buffers give WF_ERR_ARG (or the documented neutral
+    value) before any device call: no entry point dereferences them."""
+    from wildfires_b200 import _abi
+    L = _abi.lib()
+    ARG = _abi.WF_ERR_ARG
+    calls = {
+        "wf_read_parameters": ((None, None), ARG),
+        "wf_set_topography": ((None, None), ARG),
+        "wf_state_size": ((None,), 0),
+        "wf_load_fields": ((None, None, None, None), ARG),
+        "wf_save_fields": ((None, None, 0, None, None), ARG),
+        "wf_create": ((None, 0, None), ARG),
+        "wf_destroy": ((None,), 0),
+        "wf_upload_state": ((None, None, None), ARG),
+        "wf_download_state": ((None, None, None), ARG),
+        "wf_step": ((None, 1), ARG),
+        "wf_synchronize": ((None,), ARG),
+        "wf_time": ((None, None, None), ARG),
+        "wf_diagnostics": ((None, None), ARG),
+        "wf_device_state": ((None, None, None), ARG),
+        "wf_stream": ((None,), None),
+        "wf_phi": ((None, None, None), ARG),
+        "wf_pressure": ((None, None, None, None, None), ARG),
+        "wf_launches_per_step": ((None,), 0),
+        "wf_profile_phases": ((None, 1, None, None), ARG),
+        "wf_pressure_noalloc": ((None, None, None, None), ARG),
+        "wf_rk": ((None, None, None), ARG),
+        "wf_ensemble_create": ((None, 0, 0, None), ARG),
+        "wf_ensemble_destroy": ((None,), 0),
+        "wf_ensemble_size": ((None,), 0),
+        "wf_ensemble_member": ((None, 0), None),
+        "wf_ensemble_step": ((None, 1), ARG),
+        "wf_ensemble_synchronize": ((None,), ARG),
+        "wf_set_closure": ((None, 0, None), ARG),
+        "wf_closure_coefficients": ((None, None, None), ARG),
+        "wf_mlp_loss_grad": ((None, None, None, 0, None, None), ARG),
+        "wf_mlp_train": ((None, None, None, 0, 0, 0, 0.0, 0, None), ARG),
+        "wf_pressure_report": ((None, None, None), ARG),
+        "wf_timestep_reports": ((None, None), ARG),
+        "wf_dump_async": ((None, None, 0), ARG),
+        "wf_dump_wait": ((None,), ARG),
+        "wf_save_domain": ((None, None), ARG),
+        "wf_save_topography": ((None, None), ARG),
+        "wf_initial_conditions": ((None,), ARG),
+        "wf_stage_tile": ((None, None, None, None), ARG),
+        "wf_set_stage_tile": ((None, 8, 16, 0), ARG),
+    }
+    for name, (args, expect) in calls.items():
+        assert getattr(L, name)(*args) == expect, name
+    L.wf_free_parameters(None)
+    assert L.wf_phase_name(-1) is None and L.wf_phase_name(_abi.WF_NPHASES) is None
+    assert L.wf_phase_name(0) is not None and L.wf_status_string(ARG)
+    # every declared entry point that takes a pointer is in the table above
+    takes_pointer = {n for n in _abi.EXPORTS if n not in ("wf_status_string", "wf_last_error", "wf_phase_name",
+                                                          "wf_closure_param_count", "wf_free_parameters")}
+    assert takes_pointer == set(calls), takes_pointer ^ set(calls)
