@@ -27,6 +27,10 @@
  *                    (functions.cu:187-323, solver.cu:41-56)          -> OUTDIR/y0.bin, p0.bin
  *                    (Y entries the reference leaves unwritten are zero here:
  *                    its main mallocs Y, and large fresh allocations read as zero)
+ *        params   -- the record read_parameters_file built (raw bytes, before
+ *                    this driver sets its launch sizes)              -> OUTDIR/params.bin
+ *                    and its arrays x, y, z, t, kx, ky, topography   -> OUTDIR/<name>.bin
+ *                    (FP64), cut_nodes, Nz_Y                         -> OUTDIR/<name>.bin (int32)
  * The working directory must be writable: read_parameters_file creates
  * data/output/<timestamp>/ there (src/cu/parameters.cu:21-37).
  */
@@ -106,6 +110,30 @@ int main(int argc, char **argv)
             }
             ibm_parameters(&P);
         }
+    }
+    if (strcmp(mode, "params") == 0) {
+        char path[1024];
+        snprintf(path, sizeof(path), "%s/params.bin", outdir);
+        FILE *f = fopen(path, "wb");
+        if (!f || fwrite(&P, sizeof(P), 1, f) != 1) {
+            fprintf(stderr, "ref_driver: cannot write %s\n", path);
+            return 1;
+        }
+        fclose(f);
+        const size_t nc = (size_t)P.Nx * P.Ny;
+        int rc = write_bin(outdir, "x.bin", P.x, P.Nx) || write_bin(outdir, "y.bin", P.y, P.Ny) ||
+                 write_bin(outdir, "z.bin", P.z, P.Nz) || write_bin(outdir, "t.bin", P.t, P.Nt + 1) ||
+                 write_bin(outdir, "kx.bin", P.kx, P.Nx - 1) || write_bin(outdir, "ky.bin", P.ky, P.Ny - 1) ||
+                 write_bin(outdir, "topography.bin", P.topography, nc);
+        const int *ia[2] = {P.cut_nodes, P.Nz_Y};
+        const char *in[2] = {"cut_nodes.bin", "Nz_Y.bin"};
+        for (int q = 0; q < 2 && !rc; q++) {
+            snprintf(path, sizeof(path), "%s/%s", outdir, in[q]);
+            FILE *g = fopen(path, "wb");
+            rc = !g || fwrite(ia[q], sizeof(int), nc, g) != nc;
+            if (g) fclose(g);
+        }
+        return rc ? 1 : 0;
     }
     P.threads_per_block = THREADS;
     P.number_of_blocks = BLOCKS;

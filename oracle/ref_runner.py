@@ -55,6 +55,13 @@ def run(case, mode, flavour="host", parallel=False, timeout=3600, keep=None):
         elif mode == "ic":
             res["ic_y"] = np.fromfile(os.path.join(out, "y0.bin"))
             res["ic_p"] = np.fromfile(os.path.join(out, "p0.bin"))
+        elif mode == "params":
+            with open(os.path.join(out, "params.bin"), "rb") as f:
+                res["record"] = f.read()
+            for nm in ("x", "y", "z", "t", "kx", "ky", "topography"):
+                res[nm] = np.fromfile(os.path.join(out, nm + ".bin"))
+            for nm in ("cut_nodes", "Nz_Y"):
+                res[nm] = np.fromfile(os.path.join(out, nm + ".bin"), dtype=np.int32)
         else:
             kv = dict(line.split("=", 1) for line in r.stdout.splitlines() if "=" in line)
             res["seconds"] = float(kv.get("SECONDS", "nan"))

@@ -28,9 +28,10 @@ def built_libraries():
 
 
 def golden_names():
-    """Fixtures of the time step (the ic_* fixtures hold initial conditions only)."""
+    """Fixtures of the time step (the ic_* fixtures hold initial conditions
+    only, parser_records the parsed records)."""
     names = (os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
-    return sorted(n for n in names if not n.startswith("ic_"))
+    return sorted(n for n in names if not n.startswith(("ic_", "parser_")))
 
 
 def load_golden(name):
