@@ -31,6 +31,8 @@
  *                    this driver sets its launch sizes)              -> OUTDIR/params.bin
  *                    and its arrays x, y, z, t, kx, ky, topography   -> OUTDIR/<name>.bin
  *                    (FP64), cut_nodes, Nz_Y                         -> OUTDIR/<name>.bin (int32)
+ *        domain   -- the reference's save_domain + save_topography
+ *                    (output.cu:46-99) with save_path = OUTDIR/    -> x y z t topography Nz_Y .bin
  * The working directory must be writable: read_parameters_file creates
  * data/output/<timestamp>/ there (src/cu/parameters.cu:21-37).
  */
@@ -43,6 +45,7 @@
 
 #include "functions.cuh"
 #include "input.cuh"
+#include "output.cuh"
 #include "parameters.cuh"
 #include "pde.cuh"
 #include "pressure.cuh"
@@ -134,6 +137,12 @@ int main(int argc, char **argv)
             if (g) fclose(g);
         }
         return rc ? 1 : 0;
+    }
+    if (strcmp(mode, "domain") == 0) {
+        snprintf(P.save_path, sizeof(P.save_path), "%s/", outdir);
+        save_domain(P);
+        save_topography(P);
+        return 0;
     }
     P.threads_per_block = THREADS;
     P.number_of_blocks = BLOCKS;

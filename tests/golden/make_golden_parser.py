@@ -9,7 +9,9 @@ Run from the repository root in a container where the reference tree exists:
 For each case the fixture holds the file text, the reference record's raw
 bytes (the record layout is shared: include/wf_parameters.h) and the arrays
 it points to (x, y, z, t, kx, ky, topography as FP64; cut_nodes, Nz_Y as
-int32).  tests/test_parser_golden.py compares this package's parser with them.
+int32); for DOMAIN_CASES also the bytes of the files the reference's
+save_domain and save_topography write (file_<name>).
+tests/test_parser_golden.py compares this package's parser and writers with them.
 """
 import os
 import shutil
@@ -138,7 +140,17 @@ z_domain = 2
 k_transition = 5
 z_transition = 3
 """,
+    # flat terrain, a save interval that does not divide Nt, two-zone z grid
+    "flat_nt": GRID + """NT = 4
+topo_shape = flat
+z_domain = 2
+k_transition = 5
+z_transition = 3
+""",
 }
+# cases whose files also go through the reference's save_domain / save_topography
+# (output.cu:46-99); they need NT >= 1, which the reference divides by
+DOMAIN_CASES = ("full", "flat_nt")
 
 
 def main():
@@ -163,6 +175,16 @@ def main():
                 data[name + "/" + nm] = np.fromfile(os.path.join(out, nm + ".bin"))
             for nm in ("cut_nodes", "Nz_Y"):
                 data[name + "/" + nm] = np.fromfile(os.path.join(out, nm + ".bin"), dtype=np.int32)
+            if name in DOMAIN_CASES:
+                dom = os.path.join(work, "dom")
+                os.makedirs(dom)
+                r = subprocess.run([ref_runner.binary("host"), "domain", "parameters.txt", "dom"], cwd=work,
+                                   capture_output=True, text=True, timeout=600)
+                if r.returncode != 0:
+                    sys.exit("reference driver (domain) failed on %s:\n%s" % (name, r.stderr[-2000:]))
+                for nm in ("x", "y", "z", "t", "topography", "Nz_Y"):
+                    with open(os.path.join(dom, nm + ".bin"), "rb") as f:
+                        data[name + "/file_" + nm] = np.frombuffer(f.read(), dtype=np.uint8)
         finally:
             shutil.rmtree(work, ignore_errors=True)
         print("parsed", name)

@@ -58,3 +58,20 @@ def test_parser_record_equals_the_reference_parsers(case, params_from_text):
         np.testing.assert_array_equal(mine, g[case + "/" + nm], err_msg=nm)
     np.testing.assert_array_equal(P.cut_nodes().reshape(-1), g[case + "/cut_nodes"])
     np.testing.assert_array_equal(P.nz_y().reshape(-1), g[case + "/Nz_Y"])
+
+
+DOMAIN = sorted({k.split("/")[0] for k in np.load(FIX).files if "/file_" in k}) if os.path.exists(FIX) else []
+
+
+@pytest.mark.parametrize("case", DOMAIN)
+def test_domain_files_equal_the_reference_writers(case, tmp_path, params_from_text):
+    """wf_save_domain / wf_save_topography against the bytes the reference's
+    save_domain / save_topography (output.cu:46-99) write for the same file."""
+    from wildfires_b200 import save_domain, save_topography
+    g = np.load(FIX)
+    P = params_from_text(str(g[case + "/text"]))
+    save_domain(P, tmp_path)
+    save_topography(P, tmp_path)
+    for nm in ("x", "y", "z", "t", "topography", "Nz_Y"):
+        with open(tmp_path / (nm + ".bin"), "rb") as f:
+            assert f.read() == g[case + "/file_" + nm].tobytes(), nm
