@@ -875,6 +875,7 @@ wf_status wf_destroy(wf_ctx *c)
 
 wf_status wf_upload_state(wf_ctx *c, const double *y, const double *pr)
 {
+    const NvtxRange range("wf_upload_state");
     if (!c || !y || !pr) { set_error("wf_upload_state: null argument"); return WF_ERR_ARG; }
     c->cur = 0;
     c->n = 0;
@@ -1005,6 +1006,7 @@ extern "C" {
 
 wf_status wf_download_state(wf_ctx *c, double *y, double *pr)
 {
+    const NvtxRange range("wf_download_state");
     if (!c || !y || !pr) { set_error("wf_download_state: null argument"); return WF_ERR_ARG; }
     wf_status st = get_state(c, y, c->ybuf[c->cur]);
     if (st) return st;
@@ -1015,6 +1017,7 @@ wf_status wf_download_state(wf_ctx *c, double *y, double *pr)
 
 wf_status wf_step(wf_ctx *c, int nsteps)
 {
+    const NvtxRange range("wf_step");
     if (!c || nsteps < 0) { set_error("wf_step: invalid argument"); return WF_ERR_ARG; }
     if (nsteps > 0) {
         const wf_status st = tune_tiles(c);
@@ -1071,6 +1074,7 @@ wf_status wf_time(const wf_ctx *c, int *n, double *t)
 
 wf_status wf_timestep_reports(wf_ctx *c, wf_report *out)
 {
+    const NvtxRange range("wf_timestep_reports");
     if (!c || !out) { set_error("wf_timestep_reports: null argument"); return WF_ERR_ARG; }
     const double rect[4] = {c->P.Y0_x_start, c->P.Y0_x_end, c->P.Y0_y_start, c->P.Y0_y_end};
     cudaError_t e = (c->prec == WF_FP64)
@@ -1128,6 +1132,7 @@ wf_status wf_set_stage_tile(wf_ctx *c, int ti, int tj, int threads)
 
 wf_status wf_dump_async(wf_ctx *c, const char *dir, int n)
 {
+    const NvtxRange range("wf_dump_async");
     if (!c || !dir) { set_error("wf_dump_async: null argument"); return WF_ERR_ARG; }
     if (!c->dump) c->dump = dumper_create(c->device, c->P, c->S, (size_t)c->N);
     return dumper_enqueue(c->dump, c->stream, c->ybuf[c->cur], c->prec != WF_FP64, c->p, dir, n);
@@ -1141,6 +1146,7 @@ wf_status wf_dump_wait(wf_ctx *c)
 
 wf_status wf_diagnostics(wf_ctx *c, wf_diag *out)
 {
+    const NvtxRange range("wf_diagnostics");
     if (!c || !out) return WF_ERR_ARG;
     cudaError_t e = (c->prec == WF_FP64)
                         ? launch_diag<double>(c->geom, c->ph, (const double *)c->ybuf[c->cur], nullptr, c->d_diag, c->stream)
@@ -1235,6 +1241,7 @@ wf_status wf_phi(wf_ctx *c, const double *R_old, double *R_new)
 
 wf_status wf_pressure(wf_ctx *c, const double *y_np1, const double *y_n, double *pr, int *iters)
 {
+    const NvtxRange range("wf_pressure");
     if (!c || !y_np1 || !y_n || !pr) { set_error("wf_pressure: null argument"); return WF_ERR_ARG; }
     void *b1 = c->ybuf[1 - c->cur], *bn = c->Xa ? c->Xa : c->ybuf[c->cur];
     wf_status st = put_state(c, b1, y_np1);
@@ -1350,6 +1357,7 @@ wf_ctx *wf_ensemble_member(wf_ensemble *e, int i)
 
 wf_status wf_ensemble_step(wf_ensemble *e, int nsteps)
 {
+    const NvtxRange range("wf_ensemble_step");
     if (!e || nsteps < 0) { set_error("wf_ensemble_step: invalid argument"); return WF_ERR_ARG; }
     for (wf_ctx *c : e->m) {
         const wf_status st = nsteps > 0 ? tune_tiles(c) : WF_OK;

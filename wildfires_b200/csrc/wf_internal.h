@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include "../../include/wildfires_b200.h"
@@ -11,6 +12,15 @@ namespace wf {
 
 // Records a formatted message for wf_last_error() on this host thread.
 void set_error(const char *fmt, ...);
+
+// NVTX range around a host entry point, for timelines of profilers (no effect
+// unless a tool is attached).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 #define WF_TRY_CUDA(call)                                                                  \
     do {                                                                                   \
