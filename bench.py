@@ -18,7 +18,7 @@ is the aggregate over ranks, timed as the max over ranks.
 
 --impl reference times the reference's own CPU implementation (its src/cu
 sources compiled for the host by oracle/Makefile, OpenMP over its virtual
-threads) on a bounded sample of the same workload.
+threads) on the same full workload: W + K steps, the last K timed.
 """
 import argparse
 import datetime
@@ -217,46 +217,23 @@ def traffic_table():
 
 
 # ---- CPU reference ------------------------------------------------------------
-def cpu_reference_sample(case_name, target_s=20.0, steps=None):
-    """Time the reference's own solver on the host cores on a bounded sample of
-    the workload (same spacing and physics, fewer cells)."""
+def cpu_reference_sample(case_name, warmup=1, steps=1):
+    """The reference's own solver on the host cores, on the full workload for a
+    bounded number of steps (one warm-up step, one timed by the reference's
+    own step timer: about 35 s of CPU work at 512 x 512 x 128 on 16 cores)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref_runner
     from wildfires_b200 import configs
     if not ref_runner.available("host"):
         return None
-    cores = os.cpu_count()
-    # calibrate on a small grid, then size the sample for ~target_s seconds
-    cal = configs.CASES[case_name](**_sample_kw(case_name, 64, 2))
-    r = ref_runner.run(cal, "time", parallel=True)
-    rate = 64 * 64 * _nz(case_name) * 2 / r["seconds"]          # cell-steps per second
-    nsteps = steps or 2
-    n = 64
-    while (2 * n) ** 2 * _nz(case_name) * nsteps / rate <= target_s and 2 * n <= _full_n(case_name):
-        n *= 2
-    case = configs.CASES[case_name](**_sample_kw(case_name, n, nsteps))
-    r = ref_runner.run(case, "time", parallel=True)
-    cells = n * n * _nz(case_name)
-    return {"value": cells * nsteps / r["seconds"] / 1e6, "unit": METRIC, "cores": cores, "kind": "reference",
-            "sample": "%s workload at %dx%dx%d (same spacing), %d steps, %.1f s" % (case_name, n, n, _nz(case_name), nsteps, r["seconds"]),
-            "seconds": r["seconds"], "steps": nsteps}
-
-
-def _nz(name):
-    return {"hills8": 128, "hill": 128, "flat": 64}[name]
-
-
-def _full_n(name):
-    return {"hills8": 512, "hill": 256, "flat": 128}[name]
-
-
-def _sample_kw(name, n, nsteps):
-    full = _full_n(name)
-    L = {"hills8": 800.0, "hill": 400.0, "flat": 200.0}[name] * (n - 1) / (full - 1)
-    kw = dict(Nx=n, Ny=n, Nt=nsteps)
-    if name in ("hills8", "hill"):
-        kw["L"] = L
-    return kw
+    seconds, P = ref_runner.time_steps(configs.CASES[case_name](Nt=warmup + steps), warmup)
+    r = P.rec
+    cells = r.Nx * r.Ny * r.Nz
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    return {"value": cells * steps / seconds / 1e6, "unit": METRIC, "cores": cores, "kind": "reference",
+            "sample": "full %s workload %dx%dx%d, %d step timed after %d warm-up step (%.1f s), the reference's "
+                      "own per-step timer" % (case_name, r.Nx, r.Ny, r.Nz, steps, warmup, seconds),
+            "seconds": seconds, "steps": steps}
 
 
 def reference_gpu_sample(case_name, n_short=2, n_long=10, repeats=2):
@@ -464,24 +441,39 @@ def run_ours(args):
 
 
 def run_reference(args):
+    """The reference's own CPU implementation of the step (its src/cu sources
+    built for the host by oracle/Makefile, OpenMP over its virtual threads, all
+    host cores) on the FULL workload of the GPU arm: W + K steps in one run,
+    the last K timed by the reference's own step timer.  The inputs are built
+    with the reference's own parser and immersed-boundary precompute (the
+    driver's params mode); this repository's library is not loaded."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref_runner
+    from wildfires_b200 import configs
     if not ref_runner.available("host"):
         print(json.dumps({"impl": "reference", "unavailable": "reference host build (oracle/_ref/ref_host) not present"}))
         return None
-    # each step of this arm is a bounded sample of the workload; K steps in one run
-    cpu = cpu_reference_sample(args.config, target_s=max(5.0, 120.0 / max(args.steps, 1)), steps=args.steps)
-    out = {"impl": "reference", "metric": METRIC, "value": round(cpu["value"], 4), "unit": METRIC,
-           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": round(cpu["seconds"] / cpu["steps"] * 1e3, 2), "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded fields)",
-           "config": workload_config(args.config, build_params_only(args.config), args.precision,
-                                     int(os.environ.get("WORLD_SIZE", "1"))),
-           "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
-           "e2e": {"value": round(cpu["value"], 4), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    K, W = args.steps, args.warmup
+    case = configs.CASES[args.config](Nt=W + K)
+    seconds, P = ref_runner.time_steps(case, W)
+    r = P.rec
+    cells = r.Nx * r.Ny * r.Nz
+    value = cells * K / seconds / 1e6
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    sample = ("full %s workload %dx%dx%d, %d timed steps after %d warm-up steps (%.1f s), the reference's own "
+              "per-step timer" % (args.config, r.Nx, r.Ny, r.Nz, K, W, seconds))
+    cfg = workload_config(args.config, P, args.precision, int(os.environ.get("WORLD_SIZE", "1")))
+    cfg["workload"] = workload_name(args.config, P, "fp64")
+    out = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": METRIC,
+           "n_gpus": args.gpus, "steps": K, "warmup": W, "ms_per_step": round(seconds / K * 1e3, 2),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded fields)", "config": cfg,
+           "cpu_baseline": {"value": round(value, 4), "unit": METRIC, "cores": cores, "kind": "reference",
+                            "sample": sample},
+           "e2e": {"value": round(value, 4), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return out
 

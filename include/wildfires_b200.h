@@ -185,6 +185,15 @@ wf_status wf_dump_wait(wf_ctx *ctx);
 wf_status wf_device_state(wf_ctx *ctx, void **y, double **pr);
 /* The CUDA stream (cudaStream_t) the context enqueues on. */
 void *wf_stream(wf_ctx *ctx);
+/* Enqueue the context's work on the caller's stream (a cudaStream_t; NULL:
+ * the context's own stream again), so that it orders with the caller's own
+ * kernels without host synchronisation.  Work already enqueued on the previous
+ * stream comes first.  Step graphs are still captured on the context's own
+ * stream and launched on this one, so any stream may be given, the legacy
+ * default stream (cudaStreamLegacy) included.  Not for ensemble members
+ * (WF_ERR_ARG).  The reference runs everything on the default stream and
+ * synchronises after every launch (solver.cu:178-265). */
+wf_status wf_set_stream(wf_ctx *ctx, void *stream);
 
 /* ---- learned subgrid closure (no reference counterpart) ------------------- */
 
@@ -203,6 +212,19 @@ int wf_closure_param_count(void);
 wf_status wf_set_closure(wf_ctx *ctx, int kind, const float *params);
 /* The learned coefficient of every cell of a packed host state (N values). */
 wf_status wf_closure_coefficients(wf_ctx *ctx, const double *y, double *coef);
+/* The learned coefficient softplus(MLP(x)) of n rows of the 12 raw features
+ * (strain rate, vorticity, grad T in the closure's feature order, before the
+ * per-feature scales of params), evaluated on the current device by the same
+ * BF16 tensor-core kernel the solver runs before each stage; host buffers
+ * (features: n x 12 row-major, out: n values).  For evaluating a network on
+ * data other than a solver state. */
+wf_status wf_closure_predict(const float *params, const float *features, size_t n, float *out);
+/* Polls of each bounded tensor-core completion wait of the context's closure
+ * inference (default 4194304).  When a wait runs out the kernel gives the
+ * matrix operations in flight their full drain limit, frees its tensor memory
+ * and raises an error flag; the next wf_synchronize or wf_closure_coefficients
+ * returns WF_ERR_CUDA once and clears it.  A small limit exercises that path. */
+wf_status wf_set_closure_wait_limit(wf_ctx *ctx, int polls);
 /* Training on the current device with the library's own kernels.  x: n x 12
  * normalised features (row-major), y: n target coefficients.  Loss: mean
  * squared error of softplus(MLP(x)) against y. */
@@ -247,6 +269,16 @@ wf_status wf_pressure(wf_ctx *ctx, const double *y_np1, const double *y_n, doubl
  * (RK4 / RK2 / euler, solver.cu:59-93): y_np1 from y_n on host buffers. */
 wf_status wf_rk(wf_ctx *ctx, const double *y_n, double *y_np1);
 
+/* The same three operators on DEVICE buffers (packed FP64 state and FP64 p in
+ * the reference's layout), enqueued on the context's stream with no host copy
+ * and no host synchronisation: what the reference's own Phi, RK4 and
+ * solve_pressure do with the device pointers they are given (pde.cu:910-917,
+ * solver.cu:76-93, pressure.cu:506-549).  wf_pressure_device writes p in place;
+ * its iteration count is read by wf_pressure_report. */
+wf_status wf_phi_device(wf_ctx *ctx, const double *R_old, double *R_new);
+wf_status wf_rk_device(wf_ctx *ctx, const double *y_n, double *y_np1);
+wf_status wf_pressure_device(wf_ctx *ctx, const double *y_np1, const double *y_n, double *pr);
+
 /* What solve_pressure_iterative reports after the last wf_pressure or step
  * (pressure.cu:596-597): the max-norm change of the last iterate and the
  * iteration count in the reference's convention (the index of the converged
@@ -289,14 +321,20 @@ const char *wf_phase_name(int q);
  * half-spectrum buffer dominates: Nz*(Nx-1)*((Ny-1)/2+1) 16-byte cells, so a
  * 128 x 128 x 64 grid needs 8 MiB, 257 x 257 x 64 needs 33 MiB, and
  * 512 x 512 x 128 does not fit; grids that do not fit are rejected with
- * WF_ERR_ARG and a message naming the size.  Only variable_density = 0 is
- * accepted.  The first call on a device looks up the array's device address
- * and configures the kernels; make that first call before any stream capture.
- * Every call reuses the same array (and static host staging tables), so calls
- * that overlap on the GPU or run concurrently from several host threads race;
- * nothing in the array needs to start at zero, each call writes every element
- * it reads.  The call returns after the table upload, with the solve enqueued
- * on the stream. */
+ * WF_ERR_ARG and a message naming the size, before any CUDA call.  Only
+ * variable_density = 0 is accepted.  The first call on a device looks up the
+ * array's device address and configures the kernels; make that first call
+ * before any stream capture.  The FFT, wavenumber and tridiagonal tables stay
+ * in the array from one call to the next: a call on the same grid as the
+ * previous call on that device (same Nx, Ny, Nz, z, kx, ky) only enqueues the
+ * solve and returns; a call on another grid first rebuilds the tables on the
+ * host, copies them into the array and waits for that copy on the stream.
+ * Every call on a device shares the one array and keeps what the previous
+ * call left in it, so calls whose GPU work overlaps race -- on one stream or
+ * several, from one host thread or several; issue them one after another.
+ * The host side of concurrent calls (set-up, table rebuild) is serialised by a
+ * lock.  Nothing in the array needs to start at zero: each call writes every
+ * element it reads before reading it. */
 wf_status wf_pressure_noalloc(const Parameters *p, const double *y_np1, double *pr, void *stream);
 
 const char *wf_status_string(wf_status s);

@@ -79,3 +79,106 @@ def run(case, mode, flavour="host", parallel=False, timeout=3600, keep=None):
         return res
     finally:
         shutil.rmtree(work, ignore_errors=True)
+
+
+# ---- the reference's own parameter record, without this repository's library -----
+class RefRecord:
+    """The record the reference's read_parameters_file (+ ibm_parameters for a
+    terrain override) built, read back from the driver's `params` mode, with
+    the interface the case builders use (rec, z(), topo(), cut_nodes(),
+    nz_y(), state_size).  Its pointer members are meaningless in this process
+    (they were the driver's); the arrays come from the driver's files."""
+
+    def __init__(self, outdir):
+        from wildfires_b200._params import Parameters
+        with open(os.path.join(outdir, "params.bin"), "rb") as f:
+            raw = f.read()
+        self.rec = Parameters.from_buffer_copy(raw)
+        r = self.rec
+        self._z = np.fromfile(os.path.join(outdir, "z.bin"))
+        self._topo = np.fromfile(os.path.join(outdir, "topography.bin")).reshape(r.Nx, r.Ny)
+        self._cut = np.fromfile(os.path.join(outdir, "cut_nodes.bin"), dtype=np.int32).reshape(r.Nx, r.Ny)
+        self._nzy = np.fromfile(os.path.join(outdir, "Nz_Y.bin"), dtype=np.int32).reshape(r.Nx, r.Ny)
+
+    @property
+    def state_size(self):
+        r = self.rec
+        return 4 * r.Nx * r.Ny * r.Nz + r.Nx * r.Ny * r.Nz_Y_max
+
+    def z(self):
+        return self._z.copy()
+
+    def topo(self):
+        return self._topo.copy()
+
+    def cut_nodes(self):
+        return self._cut.copy()
+
+    def nz_y(self):
+        return self._nzy.copy()
+
+
+def _driver(flavour, mode, work, parallel=False, timeout=3600):
+    cmd = [binary(flavour), mode, "parameters.txt", "out"]
+    if parallel:
+        cmd.append("parallel")
+    os.makedirs(os.path.join(work, "out"), exist_ok=True)
+    r = subprocess.run(cmd, cwd=work, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError("reference driver failed (%d):\n%s\n%s" % (r.returncode, r.stdout[-2000:], r.stderr[-2000:]))
+    return r.stdout
+
+
+def write_case_reference(case, work, **overrides):
+    """Write `case` for the reference driver using the reference's own parser
+    and immersed-boundary precompute (the driver's params mode) to build the
+    record the fields are generated on -- this repository's library is not
+    loaded.  Returns the RefRecord and the initial fields."""
+    from wildfires_b200.configs import param_text
+    params = dict(case.params)
+    params["input_path"] = "in/"
+    params.update(overrides)
+    with open(os.path.join(work, "parameters.txt"), "w") as f:
+        f.write(param_text(params))
+    _driver("host", "params", work)
+    P = RefRecord(os.path.join(work, "out"))
+    topo = case.topography(P)
+    if topo is not None:
+        np.ascontiguousarray(topo, dtype=np.float64).tofile(os.path.join(work, "topography.bin"))
+        _driver("host", "params", work)             # the driver applies topography.bin and ibm_parameters
+        P = RefRecord(os.path.join(work, "out"))
+    y0, p0 = case.fields(P)
+    r = P.rec
+    N = r.Nx * r.Ny * r.Nz
+    ind = os.path.join(work, "in")
+    os.makedirs(ind, exist_ok=True)
+    for q, nm in enumerate("uvwT"):
+        y0[q * N:(q + 1) * N].tofile(os.path.join(ind, nm + ".bin"))
+    y0[4 * N:].tofile(os.path.join(ind, "Y.bin"))
+    p0.tofile(os.path.join(ind, "p.bin"))
+    return P
+
+
+def time_steps(case, warmup, timeout=7200):
+    """The reference's own solver (host build, all cores) on `case`, its Nt
+    time steps in one run; the per-step times come from its own step timer
+    (solver.cu:178-265 prints the running average every time_step_log steps;
+    here every step).  Returns the seconds of the steps after the first
+    `warmup` and the record."""
+    work = tempfile.mkdtemp(prefix="wf_reftime_")
+    try:
+        n = int(case.params["Nt"])
+        P = write_case_reference(case, work, time_step_log=1)
+        out = _driver("host", "time", work, parallel=True, timeout=timeout)
+        avg = {}
+        for line in out.splitlines():
+            if line.startswith("Time step:") and "Average time:" in line:
+                a, b = line.split(",")
+                avg[int(a.split(":")[1])] = float(b.split(":")[1].strip().split()[0])
+        if n not in avg:
+            raise RuntimeError("reference step times missing from its output:\n" + out[-2000:])
+        cum_n = avg[n] * n
+        cum_w = avg[warmup] * warmup if warmup > 0 else 0.0
+        return cum_n - cum_w, P
+    finally:
+        shutil.rmtree(work, ignore_errors=True)

@@ -3,7 +3,7 @@ solver (its src/cu sources compiled for the CPU by oracle/Makefile -> oracle/_re
 
 Run from the repository root in a container where the reference tree exists:
 
-    make -C oracle ref && python tests/golden/make_golden.py [name ...]
+    make -C oracle ref REF=<reference tree> && python tests/golden/make_golden.py [name ...]
 
 Each fixture <name>.npz holds the parameter file text, the reference parser's
 view of the grid (z, Nz_Y, cut_nodes), the seeded initial state and the
@@ -64,7 +64,7 @@ def cases():
 
 def main():
     if not ref_runner.available("host"):
-        sys.exit("oracle/_ref/ref_host missing: run `make -C oracle ref` where the reference tree exists")
+        sys.exit("oracle/_ref/ref_host missing: run `make -C oracle ref REF=<reference tree>`")
     only = set(sys.argv[1:])   # optional: fixture names to (re)generate
     for name, case in cases().items():
         if only and name not in only:

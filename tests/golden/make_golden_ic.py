@@ -5,7 +5,7 @@ src/cu/solver.cu:41-56) from its src/cu sources compiled for the CPU
 
 Run from the repository root in a container where the reference tree exists:
 
-    make -C oracle ref && python tests/golden/make_golden_ic.py
+    make -C oracle ref REF=<reference tree> && python tests/golden/make_golden_ic.py
 
 Each fixture holds the parameter-file text, the terrain override (if any) and
 the packed initial state and pressure.  Y entries the reference leaves
@@ -47,7 +47,7 @@ def cases():
 
 def main():
     if not ref_runner.available("host"):
-        sys.exit("oracle/_ref/ref_host missing: run `make -C oracle ref` where the reference tree exists")
+        sys.exit("oracle/_ref/ref_host missing: run `make -C oracle ref REF=<reference tree>`")
     for name, case in cases().items():
         res = ref_runner.run(case, "ic")
         P = res["P"]

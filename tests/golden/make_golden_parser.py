@@ -4,7 +4,7 @@ of parameter files, through oracle/_ref/ref_host in mode `params`.
 
 Run from the repository root in a container where the reference tree exists:
 
-    make -C oracle ref && python tests/golden/make_golden_parser.py
+    make -C oracle ref REF=<reference tree> && python tests/golden/make_golden_parser.py
 
 For each case the fixture holds the file text, the reference record's raw
 bytes (the record layout is shared: include/wf_parameters.h) and the arrays
@@ -155,7 +155,7 @@ DOMAIN_CASES = ("full", "flat_nt")
 
 def main():
     if not ref_runner.available("host"):
-        sys.exit("oracle/_ref/ref_host missing: run `make -C oracle ref` where the reference tree exists")
+        sys.exit("oracle/_ref/ref_host missing: run `make -C oracle ref REF=<reference tree>`")
     data = {}
     for name, text in CASES.items():
         work = tempfile.mkdtemp(prefix="wf_parser_")

@@ -101,7 +101,7 @@ def test_create_without_device_reports_no_device(params_from_text):
 
 
 @pytest.mark.parametrize("text,expect", [
-    ("Nx = 8\nNy = 8\nNz = 258\n", "Nz-1 must be <= 256"),        # longest tridiagonal system
+    ("Nx = 8\nNy = 8\nNz = 513\n", "Nz-1 must be <= 511"),        # longest tridiagonal system
     ("Nx = 2050\nNy = 5\nNz = 8\n", "Nx-1 and Ny-1 must be <= 2048"),  # longest transform
     ("Nx = 5\nNy = 2050\nNz = 8\n", "Nx-1 and Ny-1 must be <= 2048"),
     ("Nx = 8\nNy = 8\nNz = 4\n", "too small"),   # the parser takes Nz = 4, the solver needs 5
@@ -184,6 +184,12 @@ def test_every_entry_point_rejects_null_arguments():
         "wf_initial_conditions": ((None,), ARG),
         "wf_stage_tile": ((None, None, None, None), ARG),
         "wf_set_stage_tile": ((None, 8, 16, 0), ARG),
+        "wf_set_stream": ((None, None), ARG),
+        "wf_phi_device": ((None, None, None), ARG),
+        "wf_rk_device": ((None, None, None), ARG),
+        "wf_pressure_device": ((None, None, None, None), ARG),
+        "wf_closure_predict": ((None, None, 0, None), ARG),
+        "wf_set_closure_wait_limit": ((None, 0), ARG),
     }
     for name, (args, expect) in calls.items():
         assert getattr(L, name)(*args) == expect, name
@@ -194,3 +200,24 @@ def test_every_entry_point_rejects_null_arguments():
     takes_pointer = {n for n in _abi.EXPORTS if n not in ("wf_status_string", "wf_last_error", "wf_phase_name",
                                                           "wf_closure_param_count", "wf_free_parameters")}
     assert takes_pointer == set(calls), takes_pointer ^ set(calls)
+
+
+@pytest.mark.parametrize("extra, grid, message", [
+    ("variable_density = 1\n", (16, 16, 16), "variable_density"),
+    ("variable_density = 0\n", (2050, 8, 16), "Nx-1, Ny-1 must be <="),
+    ("variable_density = 0\n", (8, 2050, 16), "Nx-1, Ny-1 must be <="),
+    ("variable_density = 0\n", (8, 8, 600), "Nz-1 <="),
+    ("variable_density = 0\n", (512, 512, 64), "MiB of scratch"),
+])
+def test_noalloc_pressure_rejects_before_any_cuda_call(params_from_text, extra, grid, message):
+    """wf_pressure_noalloc checks the density mode, the transform and tridiagonal
+    limits and the size of its fixed array on the host, before it touches a
+    device: the buffers passed here are not device memory and are never read."""
+    from wildfires_b200 import _abi
+    L = _abi.lib()
+    Nx, Ny, Nz = grid
+    P = params_from_text("Nx = %d\nNy = %d\nNz = %d\nNt = 1\nx_max = 10\ny_max = 10\nz_max = 5\nt_max = 1\n%s"
+                         % (Nx, Ny, Nz, extra))
+    st = L.wf_pressure_noalloc(C.byref(P.rec), C.c_void_p(16), C.c_void_p(16), None)
+    assert st == _abi.WF_ERR_ARG
+    assert message in L.wf_last_error().decode()

@@ -27,7 +27,8 @@ def test_parameter_layout_and_smagorinsky_weights():
     assert closure.NPARAM == M.NPARAM == 5057
     th = closure.smagorinsky_params(0.173)
     X = np.random.default_rng(1).normal(size=(20, 12))
-    np.testing.assert_allclose(closure.predict(th, X), 0.173 ** 2, rtol=1e-6)
+    c = M.forward(th[:M.NPARAM].astype(np.float64), X * th[M.NPARAM:])[0]
+    np.testing.assert_allclose(c, 0.173 ** 2, rtol=1e-6)
     th = closure.init_params(0, c0=0.05)
     p = M.unpack(th[:M.NPARAM])
     assert not p["b1"].any() and not p["b2"].any() and p["W1"].any() and p["W2"].any() and p["W3"].any()

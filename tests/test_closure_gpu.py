@@ -19,6 +19,12 @@ def _f32(a):
     return np.ascontiguousarray(a, dtype=np.float32)
 
 
+def _oracle_predict(th, X):
+    """float64 forward pass of the oracle on unnormalised features."""
+    th = np.asarray(th, dtype=np.float64)
+    return M.forward(th[:M.NPARAM], np.asarray(X, dtype=np.float64) * th[M.NPARAM:])[0]
+
+
 def _batch(n, seed=0):
     rng = np.random.default_rng(seed)
     th = rng.normal(0, 0.25, M.NPARAM + 12).astype(np.float32)
@@ -89,7 +95,7 @@ def test_tensor_core_inference_matches_oracle():
             check(lib().wf_closure_coefficients(s._h, y0.ctypes.data_as(dp), c.ctypes.data_as(dp)), "coef")
         u, v, w, T = (y0[q * N:(q + 1) * N].reshape(r.Nx, r.Ny, r.Nz) for q in range(4))
         F = closure.features(u, v, w, T, r.dx, r.dy, P.z())
-        ref = closure.predict(th, F.reshape(-1, 12))
+        ref = _oracle_predict(th, F.reshape(-1, 12))
         rel = np.abs(c - ref) / np.maximum(np.abs(ref), 1e-3)
         assert np.median(rel) <= 5e-3 and rel.max() <= 5e-2, (prec, np.median(rel), rel.max())
 
@@ -112,15 +118,62 @@ def test_smagorinsky_weights_reproduce_the_smagorinsky_path():
         assert l2 <= 1e-5, (f, l2)
 
 
+def test_feature_rows_inference_matches_oracle():
+    """wf_closure_predict (the solver's tensor-core kernel on rows of features)
+    against the float64 oracle forward pass, on features spread like a
+    state's (several hundred tiles, a partial last tile)."""
+    from wildfires_b200 import closure
+    rng = np.random.default_rng(4)
+    th = closure.init_params(2, scales=rng.uniform(0.5, 2.0, 12).astype(np.float32), c0=0.03)
+    X = rng.normal(0, 1.5, (128 * 300 + 77, 12))
+    c = closure.predict(th, X)
+    ref = _oracle_predict(th, X)
+    rel = np.abs(c - ref) / np.maximum(np.abs(ref), 1e-3)
+    assert np.median(rel) <= 5e-3 and rel.max() <= 5e-2, (np.median(rel), rel.max())
+
+
+def test_timed_out_wait_reports_and_recovers():
+    """A tensor-core completion wait that runs out (limit 0 polls) raises the
+    kernel's error flag: the call returns WF_ERR_CUDA with the timeout message,
+    the kernel drains its matrix operations with the full limit and frees its
+    tensor memory, and with the limit restored the same context computes the
+    same coefficients as before."""
+    from wildfires_b200 import Solver, closure
+    from wildfires_b200._abi import check, lib
+    P, y0, p0 = _small_state()
+    th = closure.init_params(3, c0=0.04)
+    N = P.rec.Nx * P.rec.Ny * P.rec.Nz
+    with Solver(P, "fp32") as s:
+        check(lib().wf_set_closure(s._h, 1, _f32(th).ctypes.data_as(fp)), "wf_set_closure")
+        c0 = np.empty(N)
+        check(lib().wf_closure_coefficients(s._h, y0.ctypes.data_as(dp), c0.ctypes.data_as(dp)), "coef")
+        check(lib().wf_set_closure_wait_limit(s._h, 0), "wait limit")
+        c1 = np.empty(N)
+        st = lib().wf_closure_coefficients(s._h, y0.ctypes.data_as(dp), c1.ctypes.data_as(dp))
+        assert st == 2, st
+        assert b"timed out" in lib().wf_last_error()
+        check(lib().wf_set_closure_wait_limit(s._h, 1 << 22), "wait limit")
+        c2 = np.empty(N)
+        check(lib().wf_closure_coefficients(s._h, y0.ctypes.data_as(dp), c2.ctypes.data_as(dp)), "coef")
+        assert np.array_equal(c0, c2)
+        s.upload(y0, p0)
+        s.step(2)
+        s.synchronize()
+
+
 def test_trained_network_beats_constant_coefficient_a_priori():
     """Filtered fine runs (two seeds) train the network; on a third seed's
-    filtered data its coefficient is closer to the target than C_s^2."""
+    filtered data its coefficient -- as the solver's tensor-core inference
+    computes it -- is closer to the target than C_s^2."""
     from wildfires_b200 import closure
     Nc = (17, 17, 9)
     X, y = closure.dataset([0, 1], Nc=Nc, steps=100, every=20)
     Xh, yh = closure.dataset([2], Nc=Nc, steps=100, every=20)
     th, hist = closure.train(X, y, steps=800, batch=4096, lr=2e-3)
-    mse_net = float(np.mean((closure.predict(th, Xh) - yh) ** 2))
+    c_tc = closure.predict(th, Xh)
+    c_ref = _oracle_predict(th, Xh)
+    assert np.median(np.abs(c_tc - c_ref) / np.maximum(np.abs(c_ref), 1e-3)) <= 5e-3
+    mse_net = float(np.mean((c_tc - yh) ** 2))
     mse_smag = float(np.mean((0.173 ** 2 - yh) ** 2))
     mse_mean = float(np.mean((y.mean() - yh) ** 2))
     print("a priori MSE: network %.3e, C_s^2 %.3e, training mean %.3e" % (mse_net, mse_smag, mse_mean))

@@ -1,0 +1,125 @@
+"""The benchmark configurations at their stated sizes.
+
+C2 -- 256 x 256 x 128 under a 10 m gaussian hill (the reference's own
+simple_hill terrain, src/cu/ibm.cu:13-28), log wind u_r = 8 m/s, 100 m line
+ignition, dt = 0.003 s: the FP64 path against the reference's own CUDA build
+(oracle/_ref/ref_gpu) on the same inputs, at the 1e-10 gate within the
+predictable horizon, and after the stated 500 steps inside the model's own
+sensitivity to a 1e-15 relative change of the initial temperature (the gate
+tests/test_reference_gpu.py applies to C1).
+
+C3 -- 512 x 512 x 128, eight seeded hills: the FP32 stencil path (the
+benchmark's chosen form) against the plain FP64 path, every field within 1e-5
+relative L2, and at a longer horizon within the FP64 model's own sensitivity
+to a perturbation of FP32 rounding size (2^-24 relative) of the initial
+temperature.
+"""
+import numpy as np
+import pytest
+
+import ref_runner
+from conftest import _rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _errors(P, ours, ref):
+    """Per-field (L-inf, L2) relative errors on the periodic cell set."""
+    r = P.rec
+    N = r.Nx * r.Ny * r.Nz
+    out = {}
+    for q, nm in enumerate("uvwT"):
+        a = ours[q * N:(q + 1) * N].reshape(r.Nx, r.Ny, r.Nz)[:-1, :-1]
+        b = ref[q * N:(q + 1) * N].reshape(r.Nx, r.Ny, r.Nz)[:-1, :-1]
+        out[nm] = _rel(a.ravel(), b.ravel())
+    nzy = P.nz_y()
+    k = np.arange(r.Nz_Y_max)[None, None, :]
+    m = (k < nzy[:, :, None])
+    m[-1] = False
+    m[:, -1] = False
+    out["Y"] = _rel(ours[4 * N:][m.reshape(-1)], ref[4 * N:][m.reshape(-1)])
+    return out
+
+
+def _run(P, y0, p0, n, prec="fp64"):
+    from wildfires_b200 import Solver
+    with Solver(P, prec) as s:
+        s.upload(y0, p0)
+        s.step(n)
+        y, _ = s.download()
+        d = s.diagnostics(allow_nan=True)
+    assert d["nan_count"] == 0
+    return y
+
+
+needs_ref = pytest.mark.skipif(not ref_runner.available("gpu"), reason="oracle/_ref/ref_gpu not built")
+
+
+@needs_ref
+def test_c2_hill_fp64_matches_reference_cuda_within_predictable_horizon():
+    from wildfires_b200 import configs
+    res = ref_runner.run(configs.hill(Nt=40), "step", flavour="gpu", timeout=1800)
+    y = _run(res["P"], res["y0"], res["p0"], 40)
+    errs = _errors(res["P"], y, res["y"])
+    bad = {f: e for f, e in errs.items() if e[0] > 1e-10 or e[1] > 1e-10}
+    assert not bad, errs
+
+
+@needs_ref
+def test_c2_hill_fp64_after_500_steps_within_model_sensitivity():
+    from wildfires_b200 import configs
+    res = ref_runner.run(configs.hill(Nt=500), "step", flavour="gpu", timeout=3600)
+    P = res["P"]
+    y = _run(P, res["y0"], res["p0"], 500)
+    N = P.rec.Nx * P.rec.Ny * P.rec.Nz
+    own = {f: 0.0 for f in "uvwT"}
+    for seed in (0, 1):
+        yp0 = res["y0"].copy()
+        yp0[3 * N:4 * N] *= 1 + 1e-15 * np.random.default_rng(seed).standard_normal(N)
+        e = _errors(P, _run(P, yp0, res["p0"], 500), y)
+        own = {f: max(own[f], e[f][1]) for f in "uvwT"}
+    vs_ref = _errors(P, y, res["y"])
+    print("C2 500 steps: vs reference", {f: vs_ref[f][1] for f in "uvwT"}, "own sensitivity", own)
+    for f in "uvwT":
+        assert vs_ref[f][1] <= max(own[f], 1e-10), (f, vs_ref[f], own[f])
+
+
+def _c3(Nt):
+    from wildfires_b200 import configs, read_parameters
+    import os
+    import tempfile
+    case = configs.hills8(Nt=Nt)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "parameters.txt")
+        with open(path, "w") as f:
+            f.write(configs.param_text(case.params))
+        P = read_parameters(path)
+    P.set_topography(case.topography(P))
+    y0, p0 = case.fields(P)
+    return P, y0, p0
+
+
+def test_c3_fp32_stencil_within_1e5_of_fp64():
+    P, y0, p0 = _c3(30)
+    y64 = _run(P, y0, p0, 30)
+    y32 = _run(P, y0, p0, 30, "fp32")
+    errs = _errors(P, y32, y64)
+    print("C3 30 steps, FP32 vs FP64 (rel. L2):", {f: e[1] for f, e in errs.items()})
+    bad = {f: e for f, e in errs.items() if e[1] > 1e-5}
+    assert not bad, errs
+
+
+def test_c3_fp32_stencil_within_fp32_sized_perturbation_envelope():
+    n = 100
+    P, y0, p0 = _c3(n)
+    N = P.rec.Nx * P.rec.Ny * P.rec.Nz
+    y64 = _run(P, y0, p0, n)
+    y32 = _run(P, y0, p0, n, "fp32")
+    yp0 = y0.copy()
+    yp0[3 * N:4 * N] *= 1 + 2.0 ** -24 * np.random.default_rng(0).standard_normal(N)
+    own = _errors(P, _run(P, yp0, p0, n), y64)
+    errs = _errors(P, y32, y64)
+    print("C3 %d steps, FP32 vs FP64:" % n, {f: e[1] for f, e in errs.items()},
+          "FP64 with 2^-24 perturbed T:", {f: e[1] for f, e in own.items()})
+    for f in "uvwT":
+        assert errs[f][1] <= max(10 * own[f][1], 1e-5), (f, errs[f], own[f])

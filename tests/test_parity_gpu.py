@@ -99,7 +99,36 @@ def test_steps_one_at_a_time_equal_batched(params_from_text):
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 
 
+def _numpy_integrals(P, y):
+    """Mass, energy and fuel of a packed state: sums over the periodic cell set
+    (duplicate planes i = Nx-1, j = Ny-1 left out) with the node volume
+    dx dy (z_{k+1} - z_{k-1}) / 2 (one-sided at the walls); mass and energy
+    over the cells at or above the cut node, fuel over the stored fuel cells
+    k < Nz_Y(i, j)."""
+    r = P.rec
+    N = r.Nx * r.Ny * r.Nz
+    z = P.z()
+    zl = np.concatenate([[z[0]], z[:-1]])
+    zh = np.concatenate([z[1:], [z[-1]]])
+    dV = r.dx * r.dy * 0.5 * (zh - zl)
+    T3 = y[3 * N:4 * N].reshape(r.Nx, r.Ny, r.Nz)[:-1, :-1, :]
+    cut = P.cut_nodes()[:-1, :-1, None]
+    above = np.arange(r.Nz)[None, None, :] >= cut
+    rho = r.T_inf * r.rho_inf / T3
+    mass = np.sum(np.where(above, rho * dV[None, None, :], 0.0))
+    energy = np.sum(np.where(above, rho * r.c_p * T3 * dV[None, None, :], 0.0))
+    NzY = r.Nz_Y_max
+    Y3 = y[4 * N:].reshape(r.Nx, r.Ny, NzY)[:-1, :-1, :]
+    stored = np.arange(NzY)[None, None, :] < P.nz_y()[:-1, :-1, None]
+    fuel = np.sum(np.where(stored, Y3 * dV[None, None, :NzY], 0.0))
+    return mass, energy, fuel
+
+
 def test_diagnostics_match_numpy(params_from_text):
+    """Every FP64 diagnostic against a numpy restatement: extrema and NaN count
+    exactly, mass, energy and fuel to 1e-12 of their size (the summation
+    order differs), and the fuel consumed over three steps to 1e-12 of the
+    initial fuel."""
     g = load_golden("hill_rk4")
     P = params_from_text(g["params"])
     r = P.rec
@@ -107,21 +136,31 @@ def test_diagnostics_match_numpy(params_from_text):
     y0 = g["y0"]
     with _solver(P) as s:
         s.upload(y0, g["p0"])
-        d = s.diagnostics()
+        d0 = s.diagnostics()
+        s.step(3)
+        d3 = s.diagnostics()
+        y3, _ = s.download()
     u, v, w, T = (y0[q * N:(q + 1) * N] for q in range(4))
-    assert d["max_abs_u"] == np.max(np.abs(u)) and d["max_abs_w"] == np.max(np.abs(w))
-    assert d["T_min"] == np.min(T) and d["T_max"] == np.max(T)
+    assert d0["max_abs_u"] == np.max(np.abs(u)) and d0["max_abs_v"] == np.max(np.abs(v))
+    assert d0["max_abs_w"] == np.max(np.abs(w))
+    assert d0["T_min"] == np.min(T) and d0["T_max"] == np.max(T)
+    stored = (np.arange(r.Nz_Y_max)[None, None, :] < P.nz_y()[:, :, None]).reshape(-1)
+    assert d0["Y_min"] == np.min(y0[4 * N:][stored]) and d0["Y_max"] == np.max(y0[4 * N:][stored])
     z = P.z()
-    zl = np.concatenate([[z[0]], z[:-1]])
-    zh = np.concatenate([z[1:], [z[-1]]])
-    dV = r.dx * r.dy * 0.5 * (zh - zl)
-    T3 = T.reshape(r.Nx, r.Ny, r.Nz)[:-1, :-1, :]
-    cut = P.cut_nodes()[:-1, :-1, None]
-    above = np.arange(r.Nz)[None, None, :] >= cut
-    rho = r.T_inf * r.rho_inf / T3
-    mass = np.sum(np.where(above, rho * dV[None, None, :], 0.0))
-    assert abs(d["mass"] - mass) <= 1e-12 * mass
-    assert d["nan_count"] == 0 and d["cfl"] > 0
+    cfl = r.dt * (np.max(np.abs(u)) / r.dx + np.max(np.abs(v)) / r.dy + np.max(np.abs(w)) / r.dz)
+    assert abs(d0["cfl"] - cfl) <= 1e-14 * cfl
+    for d, y in ((d0, y0), (d3, y3)):
+        mass, energy, fuel = _numpy_integrals(P, y)
+        assert abs(d["mass"] - mass) <= 1e-12 * mass
+        assert abs(d["energy"] - energy) <= 1e-12 * energy
+        assert abs(d["fuel"] - fuel) <= 1e-12 * fuel
+        assert d["nan_count"] == 0
+    fuel0 = _numpy_integrals(P, y0)[2]
+    fuel3 = _numpy_integrals(P, y3)[2]
+    assert fuel0 - fuel3 > 0, "the ignition consumes fuel within three steps"
+    assert abs(d0["fuel_consumed"]) <= 1e-13 * fuel0
+    assert abs(d3["fuel_consumed"] - (fuel0 - fuel3)) <= 1e-12 * fuel0
+    assert z.size == r.Nz
 
 
 def test_full_size_flat_one_step_matches_oracle():
@@ -162,3 +201,20 @@ def test_pressure_fft_lengths_match_oracle(nx, ny, params_from_text):
         p, _ = s.pressure(y0, y0, p0)
     scale = np.max(np.abs(po))
     assert np.max(np.abs(p - po)) <= 1e-11 * scale
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-11), ("fp32", 1e-5)])
+def test_tallest_column_one_step_matches_oracle(prec, tol, params_from_text):
+    """The longest tridiagonal system wf_create accepts (Nz - 1 = 511) and the
+    widest projection block (512 threads): one step of a 9 x 9 x 512 flat case
+    against the oracle."""
+    from wildfires_b200 import configs
+    case = configs.flat(Nx=9, Ny=9, Nz=512, Nt=1, jitter=0.2, seed=5)
+    P = params_from_text(configs.param_text(case.params))
+    y0, p0 = case.fields(P)
+    yo, po = O.steps(P, y0, p0, 1)
+    with _solver(P, prec) as s:
+        s.upload(y0, p0)
+        s.step(1)
+        y, p = s.download()
+    _assert_fields(P, y, yo, tol, "9x9x512 step (%s)" % prec)

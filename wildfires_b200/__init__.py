@@ -54,6 +54,11 @@ class Params:
         r = self.rec
         return np.ctypeslib.as_array(r.Nz_Y, shape=(r.Nx * r.Ny,)).copy().reshape(r.Nx, r.Ny)
 
+    def topo(self):
+        """Terrain height, Nx x Ny."""
+        r = self.rec
+        return np.ctypeslib.as_array(r.topography, shape=(r.Nx * r.Ny,)).copy().reshape(r.Nx, r.Ny)
+
     def cut_nodes(self):
         r = self.rec
         return np.ctypeslib.as_array(r.cut_nodes, shape=(r.Nx * r.Ny,)).copy().reshape(r.Nx, r.Ny)

@@ -28,6 +28,8 @@ EXPORTS = [
     "wf_closure_param_count", "wf_set_closure", "wf_closure_coefficients", "wf_mlp_loss_grad", "wf_mlp_train",
     "wf_timestep_reports", "wf_dump_async", "wf_dump_wait", "wf_save_domain", "wf_save_topography",
     "wf_initial_conditions", "wf_stage_tile", "wf_set_stage_tile",
+    "wf_set_stream", "wf_phi_device", "wf_rk_device", "wf_pressure_device",
+    "wf_closure_predict", "wf_set_closure_wait_limit",
 ]
 
 
@@ -118,6 +120,12 @@ def lib():
         "wf_initial_conditions": (C.c_int, [vp]),
         "wf_stage_tile": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "wf_set_stage_tile": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
+        "wf_set_stream": (C.c_int, [vp, vp]),
+        "wf_phi_device": (C.c_int, [vp, vp, vp]),
+        "wf_rk_device": (C.c_int, [vp, vp, vp]),
+        "wf_pressure_device": (C.c_int, [vp, vp, vp, vp]),
+        "wf_closure_predict": (C.c_int, [fp, fp, C.c_size_t, fp]),
+        "wf_set_closure_wait_limit": (C.c_int, [vp, C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -226,10 +226,18 @@ def train(X, y, steps=3000, batch=8192, lr=1e-3, seed=0):
 
 
 def predict(th, X):
-    """CPU forward pass (float64) of the network on unnormalised features."""
-    sys.path.insert(0, os.path.join(os.path.dirname(HERE), "oracle"))
-    import mlp_oracle
-    return mlp_oracle.forward(th[:NPARAM].astype(np.float64), X * th[NPARAM:])[0]
+    """The network's coefficient for rows of unnormalised features X (n x 12),
+    evaluated by the solver's own BF16 tensor-core inference kernel on the
+    current GPU (wf_closure_predict)."""
+    import ctypes as C
+    from ._abi import check, lib
+    th32 = np.ascontiguousarray(th, dtype=np.float32)
+    X32 = np.ascontiguousarray(X, dtype=np.float32).reshape(-1, NIN)
+    out = np.empty(len(X32), dtype=np.float32)
+    fp = C.POINTER(C.c_float)
+    check(lib().wf_closure_predict(th32.ctypes.data_as(fp), X32.ctypes.data_as(fp), len(X32), out.ctypes.data_as(fp)),
+          "wf_closure_predict")
+    return out.astype(np.float64)
 
 
 # ---- evaluation -----------------------------------------------------------------

@@ -81,8 +81,7 @@ def _grid(P):
 
 
 def _topo_array(P):
-    r = P.rec
-    return np.ctypeslib.as_array(r.topography, shape=(r.Nx * r.Ny,)).copy().reshape(r.Nx, r.Ny)
+    return P.topo()
 
 
 def _pack(P, u, v, w, T, Y):

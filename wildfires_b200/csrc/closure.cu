@@ -126,9 +126,13 @@ __device__ void cell_features(const R *__restrict__ X, const Geom &g, double dx,
 // thread issues tcgen05.mma (M = 128, N = 64, FP32 accumulation in TMEM) for
 // layer 1 (K = 16) and, after the epilogue has written GELU(h1) back as the
 // next A operand, four for layer 2 (K = 64); each warp reads its 32 TMEM lanes
-// (= its 32 cells) with tcgen05.ld.  Every mbarrier wait is bounded: on timeout
-// the kernel raises *err, skips the rest and still frees its TMEM.
+// (= its 32 cells) with tcgen05.ld.  Every mbarrier wait is bounded (wait_limit
+// polls): on timeout the kernel raises *err, skips the rest, gives the MMA group
+// in flight kDrainLimit polls to finish and still frees its TMEM.
+// FEAT = false: the features of every cell of the state X (coef[cell]);
+// FEAT = true: n rows of 12 raw features from feat (coef[row]).
 constexpr int kTcThreads = 128, kTcCols = 128;
+constexpr int kDrainLimit = 1 << 22;
 constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 constexpr size_t kTcA1 = 0, kTcA2 = kTcA1 + 128 * 16 * 2, kTcB1 = kTcA2 + 128 * 64 * 2, kTcB2 = kTcB1 + 64 * 16 * 2;
 constexpr size_t kTcF = kTcB2 + 64 * 64 * 2;                       // fp32: b1, b2, W3, b3, scales
@@ -162,9 +166,9 @@ __device__ __forceinline__ void tc_commit(uint32_t bar)
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
-__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity)
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity, int limit)
 {
-    for (int it = 0; it < (1 << 22); it++) {
+    for (int it = 0; it < limit; it++) {
         uint32_t done;
         asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                      "selp.u32 %0, 1, 0, p;\n\t}\n"
@@ -198,10 +202,11 @@ __device__ __forceinline__ void tc_ld64(uint32_t taddr, float (&v)[64])
     for (int q = 0; q < 64; q++) v[q] = __uint_as_float(r[q]);
 }
 
-template <class R>
+template <class R, bool FEAT>
 __global__ void __launch_bounds__(kTcThreads, 1) k_closure_coef_tc(const R *__restrict__ X, Geom g, double dx,
-                                                                   double dy, const float *__restrict__ theta,
-                                                                   R *__restrict__ coef, int *err)
+                                                                   double dy, const float *__restrict__ feat, size_t nfeat,
+                                                                   const float *__restrict__ theta,
+                                                                   R *__restrict__ coef, int *err, int wait_limit)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint32_t s_taddr;
@@ -243,14 +248,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_closure_coef_tc(const R *__re
     const uint32_t taddr = s_taddr;
     const uint32_t lane_base = taddr + ((uint32_t)(32 * warp) << 16);
     const uint64_t dB1 = tc_desc(sbase + (uint32_t)kTcB1, 128, 256);
-    const size_t N = (size_t)g.N;
+    const size_t N = FEAT ? nfeat : (size_t)g.N;
     const size_t ntiles = (N + 127) / 128;
     uint32_t phase = 0;
     bool ok = true;
     for (size_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const size_t cell = tile * 128 + tid;
         float f[NIN];
-        if (cell < N) {
+        if (cell < N && FEAT) {
+#pragma unroll
+            for (int q = 0; q < NIN; q++) f[q] = feat[cell * NIN + q];
+        } else if (cell < N) {
             const int k = (int)(cell % g.Nz), j = (int)((cell / g.Nz) % g.Ny), i = (int)(cell / ((size_t)g.Nz * g.Ny));
             cell_features(X, g, dx, dy, i, j, k, f);
         } else {
@@ -278,7 +286,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_closure_coef_tc(const R *__re
             tc_mma(taddr, tc_desc(sbase + (uint32_t)kTcA1, 128, 256), dB1, 0u);
             tc_commit(bar);
         }
-        ok = __syncthreads_and(tc_wait(bar, phase) ? 1 : 0);
+        ok = __syncthreads_and(tc_wait(bar, phase, wait_limit) ? 1 : 0);
         phase ^= 1u;
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -305,7 +313,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_closure_coef_tc(const R *__re
                        tc_desc(sbase + (uint32_t)kTcB2 + 256u * s, 128, 1024), s > 0 ? 1u : 0u);
             tc_commit(bar);
         }
-        ok = __syncthreads_and(tc_wait(bar, phase) ? 1 : 0);
+        ok = __syncthreads_and(tc_wait(bar, phase, wait_limit) ? 1 : 0);
         phase ^= 1u;
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -320,7 +328,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_closure_coef_tc(const R *__re
     }
     if (!ok) {
         // give the MMA group in flight a bounded chance to finish before TMEM is freed
-        tc_wait(bar, phase ^ 1u);
+        tc_wait(bar, phase ^ 1u, kDrainLimit);
         if (tid == 0 && err) atomicExch(err, 1);
     }
     __syncthreads();
@@ -419,26 +427,50 @@ __global__ void k_adam(float *theta, float *m, float *v, const float *g, int np,
 
 int closure_param_count() { return NTOTAL; }
 
-template <class R>
-cudaError_t launch_closure_coef_tc(const R *X, const Geom &g, double dx, double dy, const float *theta, R *coef,
-                                   int *err, cudaStream_t s)
+template <class R, bool FEAT> cudaError_t closure_tc_attr()
 {
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_closure_coef_tc<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(k_closure_coef_tc<R, FEAT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)kSmemTc);
         if (e) return e;
         attr = true;
     }
-    const size_t tiles = ((size_t)g.N + 127) / 128;
-    const size_t blocks = tiles < 148 * 4 ? tiles : 148 * 4;
-    k_closure_coef_tc<R><<<(unsigned)blocks, kTcThreads, kSmemTc, s>>>(X, g, dx, dy, theta, coef, err);
+    return cudaSuccess;
+}
+
+unsigned closure_tc_blocks(size_t n)
+{
+    const size_t tiles = (n + 127) / 128;
+    return (unsigned)(tiles < 148 * 4 ? tiles : 148 * 4);
+}
+
+template <class R>
+cudaError_t launch_closure_coef_tc(const R *X, const Geom &g, double dx, double dy, const float *theta, R *coef,
+                                   int *err, cudaStream_t s, int wait_limit)
+{
+    cudaError_t e = closure_tc_attr<R, false>();
+    if (e) return e;
+    k_closure_coef_tc<R, false><<<closure_tc_blocks((size_t)g.N), kTcThreads, kSmemTc, s>>>(
+        X, g, dx, dy, nullptr, 0, theta, coef, err, wait_limit);
     return cudaGetLastError();
 }
 template cudaError_t launch_closure_coef_tc<float>(const float *, const Geom &, double, double, const float *, float *,
-                                                   int *, cudaStream_t);
+                                                   int *, cudaStream_t, int);
 template cudaError_t launch_closure_coef_tc<double>(const double *, const Geom &, double, double, const float *,
-                                                    double *, int *, cudaStream_t);
+                                                    double *, int *, cudaStream_t, int);
+
+cudaError_t launch_closure_predict(const float *theta, const float *feat, size_t n, float *out, int *err,
+                                   cudaStream_t s, int wait_limit)
+{
+    cudaError_t e = closure_tc_attr<float, true>();
+    if (e) return e;
+    Geom g;
+    memset(&g, 0, sizeof(g));
+    k_closure_coef_tc<float, true><<<closure_tc_blocks(n), kTcThreads, kSmemTc, s>>>(nullptr, g, 1.0, 1.0, feat, n,
+                                                                                      theta, out, err, wait_limit);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_mlp_grad(const float *theta, const float *xs, const float *ys, const int *idx, int n, float *grad,
                             double *loss, cudaStream_t s)

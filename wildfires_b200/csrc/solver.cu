@@ -121,7 +121,9 @@ struct wf_ctx {
     int method = 2;        // 0 Euler, 1 RK2, 2 RK4
     int nstages = 4;
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;   // the stream work is enqueued on: own, or the caller's (wf_set_stream)
+    cudaStream_t own = nullptr;      // the context's own stream; graphs are captured on it
+    bool member = false;             // owned by an ensemble (its stream is the ensemble's to fork and join)
     int Nx, Ny, Nz, NzY, N, NY;
     size_t S;              // packed state size (elements)
     size_t esz;            // element size of the stencil state
@@ -160,6 +162,7 @@ struct wf_ctx {
     void *coef = nullptr;    // [N] learned coefficient (stencil precision)
     float *d_theta = nullptr;
     int *d_closure_err = nullptr;   // raised by the closure kernel on a timed-out tensor-core wait
+    int closure_wait = kClosureWaitLimit;   // polls of each tensor-core completion wait
     double *d_rep = nullptr;        // checkpoint report scratch
     Dumper *dump = nullptr;         // asynchronous dumps (created by the first wf_dump_async)
     int tile = 0;                   // tile shape of the fused stage pass (index)
@@ -395,6 +398,7 @@ template <class R> StageArgs<R> stage_args(wf_ctx *c, const void *X, const void 
     a.coef = c->closure ? (R *)c->coef : nullptr;
     a.theta = c->d_theta;
     a.closure_err = c->d_closure_err;
+    a.closure_wait = c->closure_wait;
     a.bcfix = c->d_bcfix;
     a.nbcfix = c->nbcfix;
     a.tile = c->tile;
@@ -513,10 +517,11 @@ template <class R> wf_status enqueue_pressure(wf_ctx *c, const void *y1, const v
     for (auto &pl : c->ploop)
         if (pl.ge && pl.y1 == y1 && pl.yn == yn) ge = pl.ge;
     if (!ge) {
+        // captured on the context's own stream, launched on the current one
         cudaGraph_t gph = nullptr;
-        WF_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        wf_status st = capture_pressure_loop<R>(c, a, s);
-        cudaError_t e = cudaStreamEndCapture(s, &gph);
+        WF_TRY_CUDA(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
+        wf_status st = capture_pressure_loop<R>(c, a, c->own);
+        cudaError_t e = cudaStreamEndCapture(c->own, &gph);
         if (st) {
             if (gph) cudaGraphDestroy(gph);
             return st;
@@ -774,11 +779,12 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
 
     wf_status st = WF_OK;
     auto fail = [&](wf_status s) { wf_destroy(c); return s; };
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) {
         set_error("wf_create: stream creation failed");
         delete c;
         return WF_ERR_CUDA;
     }
+    c->stream = c->own;
     const size_t sb = c->S * c->esz;
     if ((st = dev_alloc(c, &c->ybuf[0], sb)) || (st = dev_alloc(c, &c->ybuf[1], sb))) return fail(st);
     if (c->nstages > 1) {
@@ -868,7 +874,7 @@ wf_status wf_destroy(wf_ctx *c)
         if (pl.ge) cudaGraphExecDestroy(pl.ge);
     for (auto &b : c->bufs) cudaFree(b.p);
     if (c->aux) cudaStreamDestroy(c->aux);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->own) cudaStreamDestroy(c->own);
     delete c;
     return WF_OK;
 }
@@ -1028,10 +1034,16 @@ wf_status wf_step(wf_ctx *c, int nsteps)
         if (step_is_static(c, n1)) {
             cudaGraphExec_t &ge = c->graph[c->cur];
             if (!ge) {
+                // captured on the context's own stream (a caller's stream may be
+                // one that cannot be captured, such as the legacy default stream)
+                // and launched on the current one
                 cudaGraph_t gph = nullptr;
-                WF_TRY_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+                const cudaStream_t user = c->stream;
+                c->stream = c->own;
+                WF_TRY_CUDA(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
                 wf_status st = enqueue_step_any(c, c->cur, n1);
-                cudaError_t e = cudaStreamEndCapture(c->stream, &gph);
+                cudaError_t e = cudaStreamEndCapture(c->own, &gph);
+                c->stream = user;
                 if (st) {
                     if (gph) cudaGraphDestroy(gph);
                     return st;
@@ -1059,7 +1071,12 @@ wf_status wf_synchronize(wf_ctx *c)
     if (c->closure && c->d_closure_err) {
         int herr = 0;
         WF_TRY_CUDA(cudaMemcpy(&herr, c->d_closure_err, sizeof(int), cudaMemcpyDeviceToHost));
-        if (herr) { set_error("wf_synchronize: a closure tensor-core completion wait timed out"); return WF_ERR_CUDA; }
+        if (herr) {
+            // reported once: the flag is cleared so that later calls start clean
+            WF_TRY_CUDA(cudaMemset(c->d_closure_err, 0, sizeof(int)));
+            set_error("wf_synchronize: a closure tensor-core completion wait timed out");
+            return WF_ERR_CUDA;
+        }
     }
     return WF_OK;
 }
@@ -1323,6 +1340,7 @@ wf_status wf_ensemble_create(const Parameters *members, int n_members, int preci
         wf_ctx *c = nullptr;
         wf_status st = wf_create(&members[i], precision, &c);
         if (st) return fail(st);
+        c->member = true;
         e->m.push_back(c);
         cudaEvent_t ev;
         if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
@@ -1444,11 +1462,13 @@ wf_status wf_closure_coefficients(wf_ctx *c, const double *y, double *coef)
     void *in = c->ybuf[1 - c->cur];
     wf_status st = put_state(c, in, y);
     if (st) return st;
+    WF_TRY_CUDA(cudaMemsetAsync(c->d_closure_err, 0, sizeof(int), c->stream));
     cudaError_t e = (c->prec == WF_FP64)
                         ? launch_closure_coef_tc<double>((const double *)in, c->geom, c->ph.dx, c->ph.dy, c->d_theta,
-                                                         (double *)c->coef, c->d_closure_err, c->stream)
+                                                         (double *)c->coef, c->d_closure_err, c->stream,
+                                                         c->closure_wait)
                         : launch_closure_coef_tc<float>((const float *)in, c->geom, c->ph.dx, c->ph.dy, c->d_theta,
-                                                        (float *)c->coef, c->d_closure_err, c->stream);
+                                                        (float *)c->coef, c->d_closure_err, c->stream, c->closure_wait);
     if (e) { set_error("wf_closure_coefficients: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
     int herr = 0;
     WF_TRY_CUDA(cudaMemcpyAsync(&herr, c->d_closure_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -1464,6 +1484,14 @@ wf_status wf_closure_coefficients(wf_ctx *c, const double *y, double *coef)
         for (int q = 0; q < c->N; q++) coef[q] = h[q];
     }
     drop_graphs(c);
+    return WF_OK;
+}
+
+wf_status wf_set_closure_wait_limit(wf_ctx *c, int polls)
+{
+    if (!c || polls < 0) { set_error("wf_set_closure_wait_limit: invalid argument"); return WF_ERR_ARG; }
+    drop_graphs(c);   // captured steps carry the limit
+    c->closure_wait = polls;
     return WF_OK;
 }
 
@@ -1490,6 +1518,29 @@ struct TrainBuffers {
 }  // namespace wfs
 
 extern "C" {
+
+wf_status wf_closure_predict(const float *params, const float *features, size_t n, float *out)
+{
+    if (!params || !features || !out || !n || n > (size_t)1 << 30) {
+        set_error("wf_closure_predict: invalid argument");
+        return WF_ERR_ARG;
+    }
+    const int np = closure_param_count();
+    TrainBuffers b;
+    float *dth = (float *)b.get(sizeof(float) * np), *dx = (float *)b.get(sizeof(float) * 12 * n);
+    float *dout = (float *)b.get(sizeof(float) * n);
+    int *derr = (int *)b.get(sizeof(int));
+    if (!dth || !dx || !dout || !derr) { set_error("wf_closure_predict: device allocation failed"); return WF_ERR_OOM; }
+    WF_TRY_CUDA(cudaMemcpy(dth, params, sizeof(float) * np, cudaMemcpyHostToDevice));
+    WF_TRY_CUDA(cudaMemcpy(dx, features, sizeof(float) * 12 * n, cudaMemcpyHostToDevice));
+    WF_TRY_CUDA(cudaMemset(derr, 0, sizeof(int)));
+    WF_TRY_CUDA(launch_closure_predict(dth, dx, n, dout, derr, 0));
+    int herr = 0;
+    WF_TRY_CUDA(cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) { set_error("wf_closure_predict: a tensor-core completion wait timed out"); return WF_ERR_CUDA; }
+    WF_TRY_CUDA(cudaMemcpy(out, dout, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    return WF_OK;
+}
 
 wf_status wf_mlp_loss_grad(const float *theta, const float *x, const float *y, size_t n, double *loss, float *grad)
 {
@@ -1569,6 +1620,119 @@ wf_status wf_pressure_report(const wf_ctx *c, double *error, int *max_iter)
 {
     if (!c) { set_error("wf_pressure_report: null context"); return WF_ERR_ARG; }
     return read_piter(const_cast<wf_ctx *>(c), nullptr, error, max_iter);
+}
+
+wf_status wf_set_stream(wf_ctx *c, void *stream)
+{
+    if (!c) { set_error("wf_set_stream: null context"); return WF_ERR_ARG; }
+    if (c->member) { set_error("wf_set_stream: an ensemble member runs on the ensemble's streams"); return WF_ERR_ARG; }
+    const cudaStream_t next = stream ? (cudaStream_t)stream : c->own;
+    if (next == c->stream) return WF_OK;
+    // work already enqueued on the previous stream comes first
+    cudaEvent_t ev = nullptr;
+    WF_TRY_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaError_t e = cudaEventRecord(ev, c->stream);
+    if (!e) e = cudaStreamWaitEvent(next, ev, 0);
+    cudaEventDestroy(ev);
+    if (e) { set_error("wf_set_stream: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
+    c->stream = next;
+    return WF_OK;
+}
+
+}  // extern "C"
+
+namespace wfs {
+
+// Fuel entries above each column's fuel top (k >= Nz_Y(i, j)) of a packed FP64
+// state on the device, set to zero (Phi never writes them).
+__global__ void k_zero_fuel_above(double *R, const int *__restrict__ nzy, int ncol, int NzY)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ncol * NzY) return;
+    const int col = t / NzY, k = t % NzY;
+    if (k >= nzy[col]) R[t] = 0.0;
+}
+
+// Packed FP64 device state -> stencil-precision device state, and back, on the
+// context's stream (no host copy).
+wf_status put_state_dev(wf_ctx *c, void *dst, const double *src)
+{
+    if (c->prec == WF_FP64) {
+        WF_TRY_CUDA(cudaMemcpyAsync(dst, src, c->S * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        return WF_OK;
+    }
+    k_to_prec<float><<<592, 256, 0, c->stream>>>((float *)dst, src, c->S);
+    WF_TRY_CUDA(cudaGetLastError());
+    return WF_OK;
+}
+
+wf_status get_state_dev(wf_ctx *c, double *dst, const void *src)
+{
+    if (c->prec == WF_FP64) {
+        WF_TRY_CUDA(cudaMemcpyAsync(dst, src, c->S * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        return WF_OK;
+    }
+    k_from_prec<float><<<592, 256, 0, c->stream>>>(dst, (const float *)src, c->S);
+    WF_TRY_CUDA(cudaGetLastError());
+    return WF_OK;
+}
+
+}  // namespace wfs
+
+extern "C" {
+
+wf_status wf_phi_device(wf_ctx *c, const double *R_old, double *R_new)
+{
+    const NvtxRange range("wf_phi_device");
+    if (!c || !R_old || !R_new) { set_error("wf_phi_device: null argument"); return WF_ERR_ARG; }
+    void *in = c->ybuf[1 - c->cur], *outb = c->Xa ? c->Xa : c->ybuf[c->cur];
+    wf_status st = put_state_dev(c, in, R_old);
+    if (st) return st;
+    const int saved = c->method;
+    c->method = 3;
+    cudaError_t e;
+    if (c->prec == WF_FP64) e = launch_stage<double>(stage_args<double>(c, in, in, outb, 1), c->stream);
+    else e = launch_stage<float>(stage_args<float>(c, in, in, outb, 1), c->stream);
+    c->method = saved;
+    if (e != cudaSuccess) { set_error("wf_phi_device: %s", cudaGetErrorString(e)); return WF_ERR_CUDA; }
+    if ((st = get_state_dev(c, R_new, outb))) return st;
+    const int ny = c->Nx * c->Ny * c->NzY;
+    if (ny > 0) {
+        k_zero_fuel_above<<<(ny + 255) / 256, 256, 0, c->stream>>>(R_new + (size_t)4 * c->N, c->geom.nzy,
+                                                                     c->Nx * c->Ny, c->NzY);
+        WF_TRY_CUDA(cudaGetLastError());
+    }
+    drop_graphs(c);
+    return WF_OK;
+}
+
+wf_status wf_rk_device(wf_ctx *c, const double *y_n, double *y_np1)
+{
+    if (!c || !y_n || !y_np1) { set_error("wf_rk_device: null argument"); return WF_ERR_ARG; }
+    void *yn = c->ybuf[1 - c->cur], *y1 = c->ybuf[c->cur];
+    wf_status st = put_state_dev(c, yn, y_n);
+    if (st) return st;
+    st = (c->prec == WF_FP64) ? enqueue_stages<double>(c, yn, y1) : enqueue_stages<float>(c, yn, y1);
+    if (st) return st;
+    if ((st = get_state_dev(c, y_np1, y1))) return st;
+    drop_graphs(c);
+    return WF_OK;
+}
+
+wf_status wf_pressure_device(wf_ctx *c, const double *y_np1, const double *y_n, double *pr)
+{
+    const NvtxRange range("wf_pressure_device");
+    if (!c || !y_np1 || !y_n || !pr) { set_error("wf_pressure_device: null argument"); return WF_ERR_ARG; }
+    void *b1 = c->ybuf[1 - c->cur], *bn = c->Xa ? c->Xa : c->ybuf[c->cur];
+    wf_status st = put_state_dev(c, b1, y_np1);
+    if (st) return st;
+    if ((st = put_state_dev(c, bn, y_n))) return st;
+    WF_TRY_CUDA(cudaMemcpyAsync(c->p, pr, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, c->stream));
+    st = (c->prec == WF_FP64) ? enqueue_pressure<double>(c, b1, bn) : enqueue_pressure<float>(c, b1, bn);
+    if (st) return st;
+    WF_TRY_CUDA(cudaMemcpyAsync(pr, c->p, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, c->stream));
+    drop_graphs(c);
+    return WF_OK;
 }
 
 wf_status wf_rk(wf_ctx *c, const double *y_n, double *y_np1)

@@ -883,7 +883,8 @@ template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t 
 {
     const int ncol = a.g.Nx * a.g.Ny;
     if (a.coef) {
-        cudaError_t e = launch_closure_coef_tc<R>(a.X, a.g, a.ph.dx, a.ph.dy, a.theta, a.coef, a.closure_err, s);
+        cudaError_t e = launch_closure_coef_tc<R>(a.X, a.g, a.ph.dx, a.ph.dy, a.theta, a.coef, a.closure_err, s,
+                                                  a.closure_wait);
         if (e) return e;
     }
     k_utau<R><<<(ncol + 127) / 128, 128, 0, s>>>(a);

@@ -121,6 +121,7 @@ struct StageArgs {
     R *coef;               // [N] coefficient of the stage input, written before the stage
     const float *theta;    // closure parameters on the device
     int *closure_err;      // set by the closure kernel when a tensor-core wait times out
+    int closure_wait;      // polls of each tensor-core completion wait
     const int *bcfix;      // columns whose cut node or top the fused pass leaves to k_stage_bc
     int nbcfix;
     int tile;              // tile shape of the fused pass (index into the compiled shapes)
@@ -128,9 +129,13 @@ struct StageArgs {
 
 // Learned closure (closure.cu).
 int closure_param_count();
+constexpr int kClosureWaitLimit = 1 << 22;   // polls of a tensor-core completion wait before it gives up
 template <class R>
 cudaError_t launch_closure_coef_tc(const R *X, const Geom &g, double dx, double dy, const float *theta, R *coef,
-                                   int *err, cudaStream_t s);
+                                   int *err, cudaStream_t s, int wait_limit = kClosureWaitLimit);
+// the network on n rows of 12 raw features (feat, device) -> out[n] (device)
+cudaError_t launch_closure_predict(const float *theta, const float *feat, size_t n, float *out, int *err,
+                                   cudaStream_t s, int wait_limit = kClosureWaitLimit);
 cudaError_t launch_mlp_grad(const float *theta, const float *xs, const float *ys, const int *idx, int n, float *grad,
                             double *loss, cudaStream_t s);
 cudaError_t launch_adam(float *theta, float *m, float *v, const float *g, int step, float lr, cudaStream_t s);
@@ -196,7 +201,8 @@ template <class R>
 cudaError_t launch_poisson_impl(const PoissonArgs<R> &a, const double *zt, cudaStream_t s, cudaEvent_t *ev = nullptr);
 template <class R> cudaError_t poisson_set_attributes();
 constexpr int kMaxFftLength = 2048;     // longest supported x or y transform
-constexpr int kMaxZUnknowns = 256;      // longest supported tridiagonal system (Nz-1)
+constexpr int kMaxZUnknowns = 511;      // longest tridiagonal system (Nz-1): the projection runs one
+                                        // thread per cell of a column, at most 512
 
 // Grid-wide FP64 reductions for the diagnostics and the pressure fixed point.
 template <class R>

@@ -42,7 +42,10 @@ void check_cuda(cudaError_t e, const char *where)
 }
 
 // The operator entries keep one FP64 context for the last parameter record
-// they saw (the reference passes the record by value on every call).
+// they saw (the reference passes the record by value on every call).  Its work
+// goes on the legacy default stream, where the reference launches its kernels,
+// so it is ordered with the caller's own default-stream work; the operators
+// take the caller's device buffers directly (no host copies).
 struct OperatorContext {
     wf_ctx *ctx = nullptr;
     Parameters key;
@@ -54,6 +57,7 @@ wf_ctx *context_for(const Parameters &P)
     if (g_op.ctx) wf_destroy(g_op.ctx);
     g_op.ctx = nullptr;
     check_status(wf_create(&P, WF_FP64, &g_op.ctx), "wf_create");
+    check_status(wf_set_stream(g_op.ctx, (void *)cudaStreamLegacy), "wf_set_stream");
     g_op.key = P;
     return g_op.ctx;
 }
@@ -75,24 +79,13 @@ void rk_with(const char *method, double *y_n, double *y_np1, Parameters paramete
     Parameters q = parameters;
     memset(q.method, 0, sizeof(q.method));
     strncpy(q.method, method, sizeof(q.method) - 1);
-    wf_ctx *c = context_for(q);
-    const size_t S = wf_state_size(&q);
-    std::vector<double> a, b(S);
-    to_host(a, y_n, S);
-    check_status(wf_rk(c, a.data(), b.data()), method);
-    to_device(y_np1, b);
+    check_status(wf_rk_device(context_for(q), y_n, y_np1), method);
 }
 
 void pressure_with(double *y_np1, double *y_n, double *p, const Parameters &q, double *error, int *max_iter)
 {
     wf_ctx *c = context_for(q);
-    const size_t S = wf_state_size(&q), N = (size_t)q.Nx * q.Ny * q.Nz;
-    std::vector<double> a, b, pp;
-    to_host(a, y_np1, S);
-    to_host(b, y_n, S);
-    to_host(pp, p, N);
-    check_status(wf_pressure(c, a.data(), b.data(), pp.data(), nullptr), "solve_pressure");
-    to_device(p, pp);
+    check_status(wf_pressure_device(c, y_np1, y_n, p), "solve_pressure");
     if (error || max_iter) check_status(wf_pressure_report(c, error, max_iter), "solve_pressure_iterative");
 }
 
@@ -118,12 +111,7 @@ void create_y_0(double *u, double *v, double *w, double *T, double *Y, double *y
 void Phi(double t, double *R_old, double *R_new, double *, double *, double *, int *, int *, Parameters parameters)
 {
     (void)t;   // the right-hand side has no explicit time dependence (pde.cu:139-787)
-    wf_ctx *c = context_for(parameters);
-    const size_t S = wf_state_size(&parameters);
-    std::vector<double> a, b(S);
-    to_host(a, R_old, S);
-    check_status(wf_phi(c, a.data(), b.data()), "Phi");
-    to_device(R_new, b);
+    check_status(wf_phi_device(context_for(parameters), R_old, R_new), "Phi");
 }
 
 void euler(double, double *y_n, double *y_np1, double *, double *, double *, double *, int *, int *, double, int,
