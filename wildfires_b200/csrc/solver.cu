@@ -167,6 +167,15 @@ struct wf_ctx {
     Dumper *dump = nullptr;         // asynchronous dumps (created by the first wf_dump_async)
     int tile = 0;                   // tile shape of the fused stage pass (index)
     bool tile_set = false;          // chosen by the tuner, WF_STAGE_TILE or wf_set_stage_tile
+    int *d_kerr = nullptr;          // raised by a stage kernel whose bounded tile wait gave up
+    // FP32: TMA tensor maps (CUtensorMap, 128 bytes) of the state buffers a stage
+    // reads, for the boxes of 16-column (map[0]) and 8-column (map[1]) tiles
+    struct TensorMaps {
+        const void *ptr = nullptr;
+        alignas(64) unsigned char map[2][128];
+        bool ok[2] = {false, false};
+    } tmaps[4];
+    int ntmaps = 0;
 };
 
 namespace wfs {
@@ -401,6 +410,11 @@ template <class R> StageArgs<R> stage_args(wf_ctx *c, const void *X, const void 
     a.closure_wait = c->closure_wait;
     a.bcfix = c->d_bcfix;
     a.nbcfix = c->nbcfix;
+    a.kerr = c->d_kerr;
+    a.tmap[0] = a.tmap[1] = nullptr;
+    for (int q = 0; q < c->ntmaps; q++)
+        if (c->tmaps[q].ptr == X)
+            for (int b = 0; b < 2; b++) a.tmap[b] = c->tmaps[q].ok[b] ? c->tmaps[q].map[b] : nullptr;
     a.tile = c->tile;
     const double dt = c->P.dt;
     if (c->method == 0) a.a_next = dt;
@@ -859,6 +873,31 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
     e = cudaMemsetAsync(c->p, 0, sizeof(double) * c->N, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { set_error("wf_create: %s", cudaGetErrorString(e)); return fail(WF_ERR_CUDA); }
+    if ((st = dev_alloc(c, (void **)&c->d_kerr, sizeof(int)))) return fail(st);
+    e = cudaMemset(c->d_kerr, 0, sizeof(int));
+    if (e != cudaSuccess) { set_error("wf_create: %s", cudaGetErrorString(e)); return fail(WF_ERR_CUDA); }
+    if (precision != WF_FP64 && !(getenv("WF_NO_TMA") && atoi(getenv("WF_NO_TMA")))) {
+        // tensor maps for the tile loads of the FP32 stage kernel, one per state
+        // buffer a stage can read; without them (column length not a multiple
+        // of 4, or no driver entry point) the tiles are loaded by cp.async
+        void *encode = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &encode, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            encode = nullptr;
+        cudaGetLastError();
+        const void *bufs[4] = {c->ybuf[0], c->ybuf[1], c->Xa, c->Xb};
+        for (int b = 0; b < 4 && encode; b++) {
+            if (!bufs[b]) continue;
+            auto &m = c->tmaps[c->ntmaps];
+            m.ok[0] = stage_tensor_map(m.map[0], (const float *)bufs[b], Nx, Ny, Nz, 8, 16, encode);
+            m.ok[1] = stage_tensor_map(m.map[1], (const float *)bufs[b], Nx, Ny, Nz, 8, 8, encode);
+            if (m.ok[0] || m.ok[1]) {
+                m.ptr = bufs[b];
+                c->ntmaps++;
+            }
+        }
+    }
     c->launches = launches_per_step(c);
     *out = c;
     return WF_OK;
@@ -1068,6 +1107,15 @@ wf_status wf_synchronize(wf_ctx *c)
 {
     if (!c) return WF_ERR_ARG;
     WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->d_kerr) {
+        int herr = 0;
+        WF_TRY_CUDA(cudaMemcpy(&herr, c->d_kerr, sizeof(int), cudaMemcpyDeviceToHost));
+        if (herr) {
+            WF_TRY_CUDA(cudaMemset(c->d_kerr, 0, sizeof(int)));
+            set_error("wf_synchronize: a stage kernel's wait for its tile load timed out");
+            return WF_ERR_CUDA;
+        }
+    }
     if (c->closure && c->d_closure_err) {
         int herr = 0;
         WF_TRY_CUDA(cudaMemcpy(&herr, c->d_closure_err, sizeof(int), cudaMemcpyDeviceToHost));

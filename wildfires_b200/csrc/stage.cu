@@ -16,181 +16,16 @@
 // pde.cu:58-97), so the fused pass evaluates interior stencils only.
 // Arithmetic follows the reference expression by expression; divisions by
 // grid constants are folded into precomputed weights (ZCoef, KRow).
+#include <cuda.h>
 #include <math.h>
+#include <stdint.h>
+#include <string.h>
 
-#include "wf_internal.h"
+#include "stage_common.cuh"
 
 namespace wf {
 
 namespace {
-
-__device__ __forceinline__ int wrap_p(int v, int n)
-{
-    // periodic index with period n = N-1 for v in [-2, 2n+1] (pde.cu:227-234)
-    if (v >= n) v -= n;
-    if (v >= n) v -= n;
-    if (v < 0) v += n;
-    return v;
-}
-
-template <class R> __device__ __forceinline__ R rmax(R a, R b) { return (a > b) ? a : b; }
-template <class R> __device__ __forceinline__ R rmin(R a, R b) { return (a < b) ? a : b; }
-
-// Square root, quotient and third.  The FP64 path keeps the reference's
-// correctly rounded operations; the FP32 stencil path uses the PTX
-// approximations (sqrt.approx.f32, div.approx.f32: about 1 ulp, no slow path),
-// well inside its 1e-5 error budget against FP64.
-__device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
-__device__ __forceinline__ float rsqrt_(float x)
-{
-    float r;
-    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
-__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
-__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
-__device__ __forceinline__ double third(double a) { return a / 3.0; }
-__device__ __forceinline__ float third(float a) { return a * (1.0f / 3.0f); }
-__device__ __forceinline__ double rexp(double x) { return exp(x); }
-__device__ __forceinline__ float rexp(float x) { return expf(x); }
-__device__ __forceinline__ double rpow(double x, double y) { return pow(x, y); }
-__device__ __forceinline__ float rpow(float x, float y) { return powf(x, y); }
-__device__ __forceinline__ double rfabs(double x) { return fabs(x); }
-__device__ __forceinline__ float rfabs(float x) { return fabsf(x); }
-
-// Packed FP32 pairs (sm_100 FFMA2 / FMUL2 / FADD2): the stencil arithmetic of
-// two fields in one instruction.  Each lane is rounded like the scalar form.
-__device__ __forceinline__ float2 bcast(float a) { return make_float2(a, a); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
-
-// Van Driest damping f_w = 1 - exp(-z+ / A_VD).  Below the cut-off the
-// exponential is smaller than half an ulp of 1 and the result is exactly 1.
-__device__ __forceinline__ double van_driest(double x) { return x < -37.5 ? 1.0 : 1.0 - exp(x); }
-__device__ __forceinline__ float van_driest(float x) { return x < -17.5f ? 1.0f : 1.0f - expf(x); }
-template <class R> struct VanDriestCut;
-template <> struct VanDriestCut<double> { static constexpr double v = 37.5; };
-template <> struct VanDriestCut<float> { static constexpr float v = 17.5f; };
-
-// Temperature source terms (pde.cu:664-711).
-template <class R> struct Thermo {
-    R T_RHS_tmp;  // conduction + radiation + reaction, before convection
-    R nu;         // molecular kinematic viscosity (Sutherland when enabled)
-    R mu;         // molecular dynamic viscosity
-    R Y;          // solid fuel fraction (0 above the fuel top)
-    R K_T;        // Arrhenius rate
-};
-
-template <class R>
-__device__ __forceinline__ Thermo<R> thermo(const PhysR<R> &p, int suth_mu, int suth_k, R T, R T_kp1, R Yc, int k,
-                                            int nzy, R Tx, R Ty, R Tz, R lap_T, R dz_k, R rho)
-{
-    Thermo<R> o;
-    R mu = p.mu, kT = p.kT, dk = R(0);
-    // Arrhenius rate A exp(-T_act/T) H(T - T_pc); exactly 0 below the phase change
-    o.K_T = (T > p.T_pc) ? p.A * rexp(-fdiv(p.T_act, T)) * R(1) : R(0);
-    R Y = R(0), T_gas = p.T_inf, T_solid = p.T_inf;
-    if (k <= nzy) {
-        if (k < nzy) Y = Yc;
-        else T_gas = T_kp1;
-        if (Y > R(0)) T_solid = T;
-        else T_gas = T;
-    }
-    if (suth_mu == 1) mu = R(1.716e-5) * rpow(T / R(273.15), R(1.5)) * (R(273.15) + R(110.4)) / (T + R(110.4));
-    if (suth_k == 1) {
-        kT = R(0.0241) * rpow(T / R(273.15), R(1.5)) * (R(273.15) + R(194)) / (T + R(194));
-        dk = R(0.0241) * (R(1.5) * rpow(T / R(273.15), R(0.5)) * (R(273.15) + R(194)) / (T + R(194)) -
-                          rpow(T / R(273.15), R(1.5)) * (R(273.15) + R(194)) / ((T + R(194)) * (T + R(194))));
-    }
-    o.nu = fdiv(mu, rho);
-    o.mu = mu;
-    R q = fdiv(p.H_C * Y * o.K_T, p.c_p);
-    if (p.alpha_s * p.sigma_s != R(0)) {
-        // h_c evaluated per cell (the reference compounds its copy per thread, pde.cu:698)
-        const R h_c = p.h_c * dz_k * rpow(rfabs(T_gas - T_solid) / dz_k, R(0.25));
-        q = q - h_c * p.alpha_s * p.sigma_s * (T_gas - T_solid) / (p.c_p * p.T_inf * p.rho_inf / T_gas);
-    }
-    o.T_RHS_tmp = fdiv(dk + p.c12 * (T * T) * (Tx * Tx + Ty * Ty + Tz * Tz) + (kT + p.c4 * (T * T * T)) * lap_T,
-                       rho * p.c_p) + q;
-    o.Y = Y;
-    return o;
-}
-
-// RK update of one value: returns the next-stage (or final) value, updates acc.
-template <class R>
-__device__ __forceinline__ R rk_update(int method, int stage, R kv, R yv, R &accv, R a_next)
-{
-    if (method == 3) return kv;                               // operator test: store k_s
-    if (method == 0) return yv + a_next * kv;                 // Euler (solver.cu:14-21)
-    if (method == 1) {                                        // RK2 (solver.cu:23-30, 65-74)
-        if (stage == 1) { accv = kv; return yv + a_next * kv; }
-        return yv + a_next * (accv + kv);
-    }
-    // RK4 (solver.cu:32-39, 76-93): acc = k1 + 2 k2 + 2 k3, then (acc + k4)
-    if (stage == 1) { accv = kv; return yv + a_next * kv; }
-    if (stage < 4) { accv = accv + R(2) * kv; return yv + a_next * kv; }
-    return yv + a_next * (accv + kv);
-}
-
-__device__ __forceinline__ bool stage_keeps_acc(int method, int stage)
-{
-    return (method == 1 && stage == 1) || (method == 2 && stage < 4);
-}
-__device__ __forceinline__ bool stage_reads_acc(int method, int stage)
-{
-    return (method == 1 && stage == 2) || (method == 2 && stage > 1);
-}
-
-// RK update of the value at offset o with k-value kv.
-template <class R>
-__device__ __forceinline__ void rk_cell(const StageArgs<R> &a, size_t o, R kv, bool rd, bool kp, R an)
-{
-    R accv = rd ? a.acc[o] : R(0);
-    a.Xout[o] = rk_update(a.method, a.stage, kv, a.yn[o], accv, an);
-    if (kp) a.acc[o] = accv;
-}
-
-// Whether the cut node kc and the two cells above it share a z-tile of KZ
-// planes (then the fused pass completes the cut node), and the same for the
-// top plane and the two below it.
-__host__ __device__ __forceinline__ bool bc_cut_in_tile(int kc, int KZ) { return kc / KZ == (kc + 2) / KZ; }
-__host__ __device__ __forceinline__ bool bc_top_in_tile(int Nz, int KZ) { return (Nz - 1) / KZ == (Nz - 3) / KZ; }
-
-// Cut node of a column (pde.cu:58-77): no-slip velocity, T and Y extrapolated
-// from the k-values of kc+1 and kc+2 held in the column's boundary slots.
-template <class R>
-__device__ __forceinline__ void bc_cut_node(const StageArgs<R> &a, int col, int kc, int nzy, bool rd, bool kp, R an)
-{
-    const R *bc = a.bc + (size_t)col * kBcSlots;
-    const size_t N = (size_t)a.g.N, cb = (size_t)col * a.g.Nz;
-    const double *z = a.g.z;
-    const R A = (R)(z[kc + 1] - z[kc]), B = (R)(z[kc + 2] - z[kc + 1]);
-    rk_cell(a, cb + kc, R(0), rd, kp, an);
-    rk_cell(a, N + cb + kc, R(0), rd, kp, an);
-    rk_cell(a, 2 * N + cb + kc, R(0), rd, kp, an);
-    rk_cell(a, 3 * N + cb + kc, fdiv((A + B) * (A + B) * bc[0] - A * A * bc[1], B * (R(2) * A + B)), rd, kp, an);
-    if (kc < nzy) {
-        const R Y1 = (kc + 1 < nzy) ? bc[2] : R(0), Y2 = (kc + 2 < nzy) ? bc[3] : R(0);
-        rk_cell(a, 4 * N + (size_t)col * a.g.NzY + kc, fdiv((A + B) * (A + B) * Y1 - A * A * Y2, B * (R(2) * A + B)),
-                rd, kp, an);
-    }
-}
-
-// Top plane of a column (pde.cu:79-86): second-order extrapolation from Nz-2, Nz-3.
-template <class R>
-__device__ __forceinline__ void bc_top(const StageArgs<R> &a, int col, bool rd, bool kp, R an)
-{
-    const R *bc = a.bc + (size_t)col * kBcSlots;
-    const int k = a.g.Nz - 1;
-    const size_t N = (size_t)a.g.N, cb = (size_t)col * a.g.Nz;
-    const double *z = a.g.z;
-    const R a1 = (R)(z[k] - z[k - 1]), a2 = (R)(z[k - 1] - z[k - 2]);
-    const R num = (a2 + a1) * (a2 + a1), den = a2 * (a2 + R(2) * a1), a1s = a1 * a1;
-#pragma unroll
-    for (int f = 0; f < 4; f++) rk_cell(a, (size_t)f * N + cb + k, fdiv(num * bc[4 + f] - a1s * bc[8 + f], den), rd, kp, an);
-}
 
 // ---------------------------------------------------------------------------
 // wall friction velocity of every column from its k = 0 plane
@@ -237,7 +72,10 @@ template <class R, int TI, int TJ, int KZ> struct Tile {
     static constexpr size_t O_UT = O_TOPO + up16(sizeof(double) * (size_t)NCOL);
     static constexpr size_t O_NZY = O_UT + up16(sizeof(R) * (size_t)NCOL);
     static constexpr size_t O_CUT = O_NZY + up16(sizeof(int) * (size_t)NCOL);
-    static constexpr size_t BUF = O_CUT + up16(sizeof(int) * (size_t)NCOL);
+    static constexpr size_t O_MISC = O_CUT + up16(sizeof(int) * (size_t)NCOL);   // mbarrier, flags
+    // the SGS buffer doubles as the staging area of the TMA box (512-byte aligned: 64-byte swizzle)
+    static constexpr size_t BUF = (O_MISC + 32 + 1023) / 1024 * 1024;
+    static constexpr size_t BOX = sizeof(float) * 4 * (size_t)SI * SJ * 16;   // one box, FP32 path
     static constexpr size_t bytes() { return BUF + up16(sizeof(R) * 8 * (size_t)GR); }
     R *st;         // [4][SR]  u, v, w, T
     R *kr;         // [GK][KROW] z-stencil rows for k0-1 .. k0+KZ
@@ -285,7 +123,7 @@ template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile(
 // Issue the copies of one tile's inputs into buffer t (one commit group).
 // Periodic in x and y (period N-1), zero outside 0..Nz-1 in z.
 template <class R, class TL, int NT>
-__device__ __forceinline__ void issue_tile(const StageArgs<R> &a, TL &t, int i0, int j0, int k0)
+__device__ __forceinline__ void issue_tile(const StageArgs<R> &a, TL &t, int i0, int j0, int k0, bool state)
 {
     const Geom &g = a.g;
     const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz, N = g.N;
@@ -305,7 +143,9 @@ __device__ __forceinline__ void issue_tile(const StageArgs<R> &a, TL &t, int i0,
         const bool ok = gk >= 0 && gk < Nz;
         cp_async<sizeof(R)>(t.kr + c, a.krow + (ok ? (size_t)gk * KROW + c % KROW : 0), ok);
     }
-    if constexpr (TL::PAIRED && TL::SK * TL::SJ <= NT) {
+    if (!state) {
+        // the stage input arrives as a TMA box (see k_stage_fused)
+    } else if constexpr (TL::PAIRED && TL::SK * TL::SJ <= NT) {
         // FP32 tile: thread (k, j) of the SK x SJ cross-section walks the SI
         // planes in i, so the k/j arithmetic and the j wrap happen once per
         // thread (lanes k fastest: global reads stay coalesced along k).  With
@@ -343,6 +183,48 @@ __device__ __forceinline__ void issue_tile(const StageArgs<R> &a, TL &t, int i0,
     cp_async_commit();
 }
 
+// Bounded wait on an mbarrier phase (false when the limit ran out).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int limit)
+{
+    for (int it = 0; it < limit; it++) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(done)
+                     : "r"(bar), "r"(parity)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+constexpr int kTmaWaitLimit = 1 << 20;   // polls before a tile load is given up (about a second)
+
+// FP32 tile from the TMA box: the box holds u, v, w, T (outermost) x SI x SJ
+// columns x 16 planes (k0-4 .. k0+11), one 64-byte row per column with the
+// 64-byte swizzle (16-byte chunk c of row r at chunk c ^ ((r >> 1) & 3)), so
+// the four chunk loads of consecutive columns hit distinct banks.  One thread
+// per (pair, column) writes the column's planes k0-2 .. k0+9 as (u, v) or
+// (w, T) pairs into the tile.
+template <class TL, int NT>
+__device__ __forceinline__ void repack_box(TL &t, const unsigned char *stg)
+{
+    for (int c = threadIdx.x; c < 2 * TL::SI * TL::SJ; c += NT) {
+        const int jj = c % TL::SJ, r = c / TL::SJ, ii = r % TL::SI, pr = r / TL::SI;
+        const int ra = ((2 * pr) * TL::SI + ii) * TL::SJ + jj, rb = ra + TL::SI * TL::SJ;
+        float va[16], vb[16];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const float4 x = *reinterpret_cast<const float4 *>(stg + ra * 64 + ((q ^ ((ra >> 1) & 3)) << 4));
+            const float4 y = *reinterpret_cast<const float4 *>(stg + rb * 64 + ((q ^ ((rb >> 1) & 3)) << 4));
+            va[4 * q] = x.x; va[4 * q + 1] = x.y; va[4 * q + 2] = x.z; va[4 * q + 3] = x.w;
+            vb[4 * q] = y.x; vb[4 * q + 1] = y.y; vb[4 * q + 2] = y.z; vb[4 * q + 3] = y.w;
+        }
+        float2 *dst = reinterpret_cast<float2 *>(t.st) + pr * TL::SR + ii * TL::SK * TL::SJ + jj;
+#pragma unroll
+        for (int kk = 0; kk < TL::SK; kk++) dst[kk * TL::SJ] = make_float2(va[kk + 2], vb[kk + 2]);
+    }
+}
+
 // upwind derivative from 5 weights (zero weights leave the sum unchanged)
 template <class R> __device__ __forceinline__ R dz5(const R *w, R m2, R m1, R c, R p1, R p2)
 {
@@ -361,30 +243,67 @@ template <class R> __device__ __forceinline__ R dz5(const R *w, R m2, R m1, R c,
 //      RK update.  Cells the boundary rules overwrite (k <= cut node, top) are
 //      left to k_stage_bc; the values it needs are stored in a.bc.
 template <class R, int TI, int TJ, int KZ, int NT>
-__global__ void __launch_bounds__(NT, sizeof(R) != 4 ? 1 : NT > 256 ? 2 : (TI * TJ <= 64 ? 3 : 2)) k_stage_fused(const StageArgs<R> a, int ntk, int ntj, int nti)
+__global__ void __launch_bounds__(NT, sizeof(R) != 4 ? 1 : NT > 256 ? 2 : (TI * TJ <= 64 ? 3 : 2))
+    k_stage_fused(const StageArgs<R> a, const __grid_constant__ CUtensorMap tmap, int use_tma, int ntk, int ntj, int nti)
 {
     using TL = Tile<R, TI, TJ, KZ>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *sgs = reinterpret_cast<R *>(smem_raw + TL::BUF);
+    R *s_vd = reinterpret_cast<R *>(smem_raw + TL::O_MISC);
+    int *s_fail = reinterpret_cast<int *>(smem_raw + TL::O_MISC + 8);
+    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(smem_raw + TL::O_MISC + 16);
     const Geom &g = a.g;
     const PhysR<R> &p = a.pr;
     const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz, N = g.N;
     const R *__restrict__ X = a.X;
     const int ntiles = ntk * ntj * nti;
-    int tile = blockIdx.x;
+    const int tile = blockIdx.x;   // one tile per block
     if (tile >= ntiles) return;
     {
-        TL t0;
-        t0.bind(smem_raw, sgs);
-        issue_tile<R, TL, NT>(a, t0, (tile / (ntk * ntj)) * TI, ((tile / ntk) % ntj) * TJ, (tile % ntk) * KZ);
-    }
-    for (int it = 0; tile < ntiles; tile += gridDim.x, it++) {
         TL t;
         t.bind(smem_raw, sgs);
         const int k0 = (tile % ntk) * KZ, j0 = ((tile / ntk) % ntj) * TJ, i0 = (tile / (ntk * ntj)) * TI;
-        cp_async_commit();       // empty group keeps the wait below uniform
-        cp_async_wait<1>();      // this tile's group has landed
+        // FP32 tiles whose halo stays inside the stored planes 0..N-2 (no periodic
+        // wrap) arrive as one TMA box of u, v, w, T; the others by cp.async
+        bool tma = false;
+        if constexpr (TL::PAIRED)
+            tma = use_tma && i0 >= 2 && i0 + TI + 1 <= Nx - 2 && j0 >= 2 && j0 + TJ + 1 <= Ny - 2 &&
+                  (((uint32_t)__cvta_generic_to_shared(sgs)) & 511u) == 0;
+        if (threadIdx.x == 0) {
+            *s_fail = 0;
+            if (tma) {
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+                asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            }
+        }
+        __syncthreads();   // barrier initialised before anyone waits on it
+        if (tma && threadIdx.x == 0) {
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"((uint32_t)TL::BOX)
+                         : "memory");
+            asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+                         "[%0], [%1, {%2, %3, %4, %5}], [%6];"
+                         :
+                         : "r"((uint32_t)__cvta_generic_to_shared(sgs)), "l"(reinterpret_cast<uint64_t>(&tmap)),
+                           "r"(k0 - 4), "r"(j0 - 2), "r"(i0 - 2), "r"(0), "r"(bar)
+                         : "memory");
+        }
+        issue_tile<R, TL, NT>(a, t, i0, j0, k0, !tma);
+        cp_async_wait<0>();
+        if (tma) {
+            if (!mbar_wait(bar, 0, kTmaWaitLimit)) *s_fail = 1;
+            else repack_box<TL, NT>(t, reinterpret_cast<const unsigned char *>(sgs));
+        }
         __syncthreads();
+        if (*s_fail) {
+            // the box did not arrive in time: flag it, give the copy a bounded
+            // chance to land (it writes this block's shared memory), leave the tile
+            if (threadIdx.x == 0) {
+                if (a.kerr) atomicExch(a.kerr, 1);
+                mbar_wait(bar, 0, kTmaWaitLimit);
+            }
+            __syncthreads();
+            return;
+        }
 
         const int smu = a.ph.sutherland_viscosity, sk = a.ph.sutherland_conductivity;
         // FP32 path without Sutherland laws or convective exchange: the
@@ -393,7 +312,7 @@ __global__ void __launch_bounds__(NT, sizeof(R) != 4 ? 1 : NT > 256 ? 2 : (TI * 
 
         // Lower bound over the tile of z_ibm u_tau / A_vd: when it exceeds
         // the cut-off times nu, every Van Driest factor of the tile is exactly 1.
-        __shared__ R s_vd_bound;
+        R &s_vd_bound = *s_vd;
         if (threadIdx.x < 32) {
             const R zlow = (k0 > 0) ? t.K(-1, RZ) : R(0);
             R hmax = R(-1e30), umin = R(1e30);
@@ -789,12 +708,7 @@ __global__ void __launch_bounds__(NT, sizeof(R) != 4 ? 1 : NT > 256 ? 2 : (TI * 
             if (kc >= k0 && kc < k0 + KZ && bc_cut_in_tile(kc, KZ)) bc_cut_node(a, col, kc, nzy, rd, kp, an);
             if (Nz - 1 >= k0 && Nz - 1 < k0 + KZ && bc_top_in_tile(Nz, KZ)) bc_top(a, col, rd, kp, an);
         }
-        __syncthreads();         // buffer and SGS inputs free for the next tiles
-        // a grid smaller than the tile count walks on (the launch gives one tile per block)
-        const int nxt = tile + gridDim.x;
-        if (nxt < ntiles) issue_tile<R, TL, NT>(a, t, (nxt / (ntk * ntj)) * TI, ((nxt / ntk) % ntj) * TJ, (nxt % ntk) * KZ);
     }
-    cp_async_wait<0>();
 }
 
 
@@ -893,7 +807,12 @@ template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t 
         using SH = decltype(sh);
         const int ntk = (a.g.Nz + SH::KZ - 1) / SH::KZ, ntj = (a.g.Ny + SH::TJ - 1) / SH::TJ;
         const int nti = (a.g.Nx + SH::TI - 1) / SH::TI;
-        k_stage_fused<R, SH::TI, SH::TJ, SH::KZ, SH::NT><<<ntk * ntj * nti, SH::NT, SH::smem(), s>>>(a, ntk, ntj, nti);
+        CUtensorMap m;
+        const void *src = (sizeof(R) == 4) ? a.tmap[SH::TJ == 16 ? 0 : 1] : nullptr;
+        if (src) memcpy(&m, src, sizeof(m));
+        else memset(&m, 0, sizeof(m));
+        k_stage_fused<R, SH::TI, SH::TJ, SH::KZ, SH::NT><<<ntk * ntj * nti, SH::NT, SH::smem(), s>>>(a, m, src ? 1 : 0,
+                                                                                                    ntk, ntj, nti);
         return cudaSuccess;
     });
     if (e) return e;
@@ -904,6 +823,23 @@ template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t 
 }
 
 int stage_tile_planes(int precision) { (void)precision; return 8; }
+
+bool stage_tensor_map(void *out, const float *X, int Nx, int Ny, int Nz, int TI, int TJ, void *encode_fn)
+{
+    if (!encode_fn || Nz % 4 != 0 || (reinterpret_cast<uintptr_t>(X) & 15) != 0) return false;
+    using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    const cuuint64_t dims[4] = {(cuuint64_t)Nz, (cuuint64_t)Ny, (cuuint64_t)Nx, 4};
+    const cuuint64_t strides[3] = {(cuuint64_t)Nz * 4, (cuuint64_t)Ny * Nz * 4, (cuuint64_t)Nx * Ny * Nz * 4};
+    const cuuint32_t box[4] = {16, (cuuint32_t)(TJ + 4), (cuuint32_t)(TI + 4), 4};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = reinterpret_cast<Encode>(encode_fn)(
+        reinterpret_cast<CUtensorMap *>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float *>(X), dims, strides,
+        box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
 int stage_tile_count(int precision) { return precision == 0 ? StageShapes<double>::count : StageShapes<float>::count; }
 void stage_tile_shape(int precision, int idx, int *ti, int *tj, int *nt)
 {

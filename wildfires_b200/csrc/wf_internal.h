@@ -125,6 +125,10 @@ struct StageArgs {
     const int *bcfix;      // columns whose cut node or top the fused pass leaves to k_stage_bc
     int nbcfix;
     int tile;              // tile shape of the fused pass (index into the compiled shapes)
+    // FP32: host copies of the TMA tensor maps (CUtensorMap) of X for the tile
+    // boxes of 16-column and 8-column tiles, or nullptr (tiles loaded by cp.async)
+    const void *tmap[2];
+    int *kerr;             // set by a stage kernel whose bounded wait for its tile gave up
 };
 
 // Learned closure (closure.cu).
@@ -145,6 +149,11 @@ cudaError_t launch_adam(float *theta, float *m, float *v, const float *g, int st
 template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t s, cudaEvent_t *ev = nullptr);
 template <class R> cudaError_t stage_set_attributes();
 int stage_tile_planes(int precision);   // z planes of a fused-stage tile
+// TMA tensor map (CUtensorMap) of a packed FP32 state for the FP32 tile box of
+// a TI x TJ tile (dims k, j, i, field = Nz, Ny, Nx, 4; box 16 x TJ+4 x TI+4 x 4,
+// 64-byte swizzle); false when the grid cannot be described (column length not a
+// multiple of 4) or the driver call fails.  encode_fn: cuTensorMapEncodeTiled.
+bool stage_tensor_map(void *out, const float *X, int Nx, int Ny, int Nz, int TI, int TJ, void *encode_fn);
 // Tile shapes compiled for the fused pass (all with the same z planes, so the
 // boundary-column list does not depend on the choice): count and TI x TJ.
 int stage_tile_count(int precision);
