@@ -93,6 +93,22 @@ void wf_free_parameters(Parameters *p);
  * packed-state size when Nz_Y_max changes. */
 wf_status wf_set_topography(Parameters *p, const double *topo);
 
+/* The immersed-boundary tables of the record's current topography (cut nodes,
+ * Nz_Y, Nz_Y_max, z_ibm; ibm_parameters, ibm.cu:57-95) computed on the current
+ * CUDA device and written back into the record's host arrays, bit-identical to
+ * wf_set_topography's host computation.  The host arrays stay the record
+ * callers may edit afterwards. */
+wf_status wf_ibm_parameters_device(Parameters *p);
+
+/* Replace the terrain by n Gaussian hills, hills[4 q .. 4 q + 3] = centre x,
+ * centre y, height, width: topography(x, y) = sum_q height exp(-(dx^2 + dy^2)
+ * / (2 width^2)), dx and dy the periodic distances to the centre (periods
+ * x_max - x_min and y_max - y_min), summed in the order given; evaluated on
+ * the current CUDA device with the immersed-boundary tables, both written back
+ * into the record.  The seeded multi-hill terrain of the benchmark workloads;
+ * the reference's terrains are flat and one hill (simple_hill, ibm.cu:13-28). */
+wf_status wf_set_topography_hills(Parameters *p, int n, const double *hills);
+
 /* Number of FP64 values in a packed state vector: 4*Nx*Ny*Nz + Nx*Ny*Nz_Y_max. */
 size_t wf_state_size(const Parameters *p);
 

@@ -190,6 +190,8 @@ def test_every_entry_point_rejects_null_arguments():
         "wf_pressure_device": ((None, None, None, None), ARG),
         "wf_closure_predict": ((None, None, 0, None), ARG),
         "wf_set_closure_wait_limit": ((None, 0), ARG),
+        "wf_ibm_parameters_device": ((None,), ARG),
+        "wf_set_topography_hills": ((None, 0, None), ARG),
     }
     for name, (args, expect) in calls.items():
         assert getattr(L, name)(*args) == expect, name

@@ -69,6 +69,20 @@ class Params:
         assert t.size == r.Nx * r.Ny
         check(lib().wf_set_topography(C.byref(r), _ptr(t)), "wf_set_topography")
 
+    def set_topography_hills(self, hills):
+        """Terrain of Gaussian hills [(cx, cy, height, width), ...] and its
+        immersed-boundary tables, computed on the current GPU."""
+        h = np.ascontiguousarray(np.asarray(hills, dtype=np.float64).reshape(-1))
+        check(lib().wf_set_topography_hills(C.byref(self.rec), len(h) // 4, _ptr(h)), "wf_set_topography_hills")
+
+    def ibm_on_device(self):
+        """Recompute the immersed-boundary tables of the current terrain on the GPU."""
+        check(lib().wf_ibm_parameters_device(C.byref(self.rec)), "wf_ibm_parameters_device")
+
+    def z_ibm(self):
+        r = self.rec
+        return np.ctypeslib.as_array(r.z_ibm, shape=(r.Nx * r.Ny * r.Nz,)).copy()
+
     def free(self):
         if self._owned:
             lib().wf_free_parameters(C.byref(self.rec))

@@ -30,6 +30,7 @@ EXPORTS = [
     "wf_initial_conditions", "wf_stage_tile", "wf_set_stage_tile",
     "wf_set_stream", "wf_phi_device", "wf_rk_device", "wf_pressure_device",
     "wf_closure_predict", "wf_set_closure_wait_limit",
+    "wf_ibm_parameters_device", "wf_set_topography_hills",
 ]
 
 
@@ -126,6 +127,8 @@ def lib():
         "wf_pressure_device": (C.c_int, [vp, vp, vp, vp]),
         "wf_closure_predict": (C.c_int, [fp, fp, C.c_size_t, fp]),
         "wf_set_closure_wait_limit": (C.c_int, [vp, C.c_int]),
+        "wf_ibm_parameters_device": (C.c_int, [P]),
+        "wf_set_topography_hills": (C.c_int, [P, C.c_int, dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -58,11 +58,14 @@ def base_params(Nx, Ny, Nz, Nt, x_max, y_max, z_max, t_max, **kw):
 class Case:
     """A parameter dict, an optional terrain override and an initial-state builder."""
 
-    def __init__(self, name, params, fields, topography=None):
+    def __init__(self, name, params, fields, topography=None, hills=None):
         self.name = name
         self.params = params
         self._fields = fields
         self._topo = topography
+        # Gaussian hills of the terrain, (centre x, centre y, height, width) each:
+        # the same terrain on the device by wf_set_topography_hills
+        self.hills = hills
 
     def topography(self, P):
         return None if self._topo is None else self._topo(P)
@@ -230,7 +233,7 @@ def hills8(Nx=512, Ny=512, Nz=128, Nt=1000, dt=0.003, seed=1234, L=800.0, H=60.0
         rng = np.random.default_rng(seed + 1)
         return _finish(P, u, v, w, T, Y, rng, jitter)
 
-    return Case("hills8", params, fields, topography)
+    return Case("hills8", params, fields, topography, hills)
 
 
 # ---- ensemble members (uneven grids, varied wind, terrain, ignition, fuel) ----------
@@ -286,7 +289,7 @@ def scenario(Nx, Ny, Nz=64, Nt=300, dt=0.005, seed=0, dx=1.5625, z_max=19.6875, 
         rng = np.random.default_rng(seed + 1)
         return _finish(P, u, v, w, T, Y, rng, jitter)
 
-    return Case("scenario", params, fields, topography)
+    return Case("scenario", params, fields, topography, hills if hills else None)
 
 
 def ensemble(n=64, seed=2024, sizes=ENSEMBLE_SIZES, **kw):
