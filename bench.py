@@ -523,20 +523,38 @@ def run_ensemble(args):
         if clk:
             clk.start()
             time.sleep(0.3)
+        # ensemble steps: CUDA events on the stream the step graphs are launched on
+        master = torch.cuda.ExternalStream(ens.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
         barrier()
-        t0 = time.perf_counter()
         w0 = time.time()
+        t0 = time.perf_counter()
+        e0.record(master)
         ens.step(args.steps)
+        e1.record(master)
         ens.synchronize()
-        t_ens = max_over_ranks(time.perf_counter() - t0)
+        wall_ens = time.perf_counter() - t0
         w1 = time.time()
+        t_ens = max_over_ranks(e0.elapsed_time(e1) * 1e-3)
         barrier()
+        # the same members one after another: each step event-timed on its own
+        # stream (device time of the member's step graph) and, separately, the
+        # wall clock of the whole serial loop (a launch and a wait per member step)
+        gpu_ser = 0.0
         t0 = time.perf_counter()
         for _ in range(args.steps):
             for m in ens.members:
+                st = torch.cuda.ExternalStream(m.stream())
+                a0 = torch.cuda.Event(enable_timing=True)
+                a1 = torch.cuda.Event(enable_timing=True)
+                a0.record(st)
                 m.step(1)
+                a1.record(st)
                 m.synchronize()
-        t_ser = max_over_ranks(time.perf_counter() - t0)
+                gpu_ser += a0.elapsed_time(a1) * 1e-3
+        wall_ser = max_over_ranks(time.perf_counter() - t0)
+        t_ser = max_over_ranks(gpu_ser)
         clocks = clk.stop((w0, w1)) if clk else None
     cells = cells_local
     if world > 1:
@@ -557,9 +575,13 @@ def run_ensemble(args):
                       "members": len(members), "cells": cells,
                       "parallelism": "members partitioned over %d ranks, no collective while stepping" % world},
            "serial": {"value": round(v_ser, 2), "ms_per_step": round(t_ser / args.steps * 1e3, 3),
-                      "how": "each member: one graph launch per step, then a wait, members one after another"},
+                      "wall_ms_per_step": round(wall_ser / args.steps * 1e3, 3),
+                      "how": "each member: one graph launch per step, then a wait, members one after another; "
+                             "ms_per_step sums the members' event-timed step graphs (device time, no gaps), "
+                             "wall_ms_per_step is the host clock of the loop"},
            "speedup_over_serial": round(t_ser / t_ens, 3),
-           "timing": "host wall clock around a device synchronisation, max over ranks", "clocks": clocks}
+           "speedup_over_serial_wall": round(wall_ser / wall_ens, 3),
+           "timing": "CUDA events on the launching streams, max over ranks", "clocks": clocks}
     print(json.dumps(out), flush=True)
     return out
 

@@ -263,6 +263,9 @@ typedef struct wf_ensemble wf_ensemble;
 wf_status wf_ensemble_create(const Parameters *members, int n_members, int precision, wf_ensemble **out);
 wf_status wf_ensemble_destroy(wf_ensemble *e);
 int wf_ensemble_size(const wf_ensemble *e);
+/* The CUDA stream (cudaStream_t) an ensemble step is launched on: work
+ * recorded on it after wf_ensemble_step follows every member's step. */
+void *wf_ensemble_stream(wf_ensemble *e);
 /* Member i as a context: upload, download and diagnose it with the wf_ctx
  * calls; owned by the ensemble (do not destroy it). */
 wf_ctx *wf_ensemble_member(wf_ensemble *e, int i);
@@ -352,6 +355,13 @@ const char *wf_phase_name(int q);
  * lock.  Nothing in the array needs to start at zero: each call writes every
  * element it reads before reading it. */
 wf_status wf_pressure_noalloc(const Parameters *p, const double *y_np1, double *pr, void *stream);
+
+/* Failure injection for tests of the error paths: after `after` more device
+ * allocations by contexts (wf_create, wf_set_closure, dumps) succeed, the
+ * next one is refused with WF_ERR_OOM as if the device were full; then
+ * injection switches itself off.  Negative: off.  No counterpart in the
+ * reference (it asserts on CUDA errors, utils.cuh:124-130). */
+void wf_inject_allocation_failure(int after);
 
 const char *wf_status_string(wf_status s);
 const char *wf_last_error(void);

@@ -192,6 +192,7 @@ def test_every_entry_point_rejects_null_arguments():
         "wf_set_closure_wait_limit": ((None, 0), ARG),
         "wf_ibm_parameters_device": ((None,), ARG),
         "wf_set_topography_hills": ((None, 0, None), ARG),
+        "wf_ensemble_stream": ((None,), None),
     }
     for name, (args, expect) in calls.items():
         assert getattr(L, name)(*args) == expect, name
@@ -200,7 +201,8 @@ def test_every_entry_point_rejects_null_arguments():
     assert L.wf_phase_name(0) is not None and L.wf_status_string(ARG)
     # every declared entry point that takes a pointer is in the table above
     takes_pointer = {n for n in _abi.EXPORTS if n not in ("wf_status_string", "wf_last_error", "wf_phase_name",
-                                                          "wf_closure_param_count", "wf_free_parameters")}
+                                                          "wf_closure_param_count", "wf_free_parameters",
+                                                          "wf_inject_allocation_failure")}
     assert takes_pointer == set(calls), takes_pointer ^ set(calls)
 
 

@@ -311,6 +311,10 @@ class Ensemble:
     def step(self, n=1):
         check(lib().wf_ensemble_step(self._h, int(n)), "wf_ensemble_step")
 
+    def stream(self):
+        """The cudaStream_t (as an int) ensemble steps are launched on."""
+        return lib().wf_ensemble_stream(self._h) or 0
+
     def synchronize(self):
         check(lib().wf_ensemble_synchronize(self._h), "wf_ensemble_synchronize")
 

@@ -30,7 +30,8 @@ EXPORTS = [
     "wf_initial_conditions", "wf_stage_tile", "wf_set_stage_tile",
     "wf_set_stream", "wf_phi_device", "wf_rk_device", "wf_pressure_device",
     "wf_closure_predict", "wf_set_closure_wait_limit",
-    "wf_ibm_parameters_device", "wf_set_topography_hills",
+    "wf_ibm_parameters_device", "wf_set_topography_hills", "wf_ensemble_stream",
+    "wf_inject_allocation_failure",
 ]
 
 
@@ -129,6 +130,8 @@ def lib():
         "wf_set_closure_wait_limit": (C.c_int, [vp, C.c_int]),
         "wf_ibm_parameters_device": (C.c_int, [P]),
         "wf_set_topography_hills": (C.c_int, [P, C.c_int, dp]),
+        "wf_ensemble_stream": (vp, [vp]),
+        "wf_inject_allocation_failure": (None, [C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -13,6 +13,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -197,9 +198,18 @@ int launches_per_step(const wf_ctx *c)
     return c->nstages * per_stage + pressure + 1;
 }
 
+// Failure injection (wf_inject_allocation_failure): the number of context
+// allocations that still succeed before one is refused; negative: off.
+std::atomic<int> g_alloc_budget{-1};
+
 wf_status dev_alloc(wf_ctx *c, void **out, size_t bytes)
 {
     void *p = nullptr;
+    if (g_alloc_budget.load() >= 0 && g_alloc_budget.fetch_sub(1) == 0) {
+        g_alloc_budget.store(-1);
+        set_error("device allocation of %zu bytes failed: refused by failure injection", bytes);
+        return WF_ERR_OOM;
+    }
     cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
     if (e != cudaSuccess) {
         set_error("device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
@@ -1415,6 +1425,10 @@ wf_status wf_ensemble_destroy(wf_ensemble *e)
 }
 
 int wf_ensemble_size(const wf_ensemble *e) { return e ? (int)e->m.size() : 0; }
+
+void *wf_ensemble_stream(wf_ensemble *e) { return e ? (void *)e->master : nullptr; }
+
+void wf_inject_allocation_failure(int after) { g_alloc_budget.store(after < 0 ? -1 : after); }
 
 wf_ctx *wf_ensemble_member(wf_ensemble *e, int i)
 {
