@@ -106,19 +106,27 @@ __device__ __forceinline__ Thermo<R> thermo(const PhysR<R> &p, int suth_mu, int 
 }
 
 // RK update of one value: returns the next-stage (or final) value, updates acc.
+//   operator test (method 3): k_s itself;
+//   Euler (solver.cu:14-21): y_n + a k;
+//   RK2 (solver.cu:23-30, 65-74): acc = k1, y_n + a k1; then y_n + a (acc + k2);
+//   RK4 (solver.cu:32-39, 76-93): acc = k1, then acc + 2 k2, acc + 2 k3 with
+//   y_n + a k_s; last y_n + a (acc + k4).
+// Written as three fused multiply-adds with coefficients of the method and
+// stage (uniform over the launch, so computed once), without branches per
+// value: t = k + cA acc, out = a t + cY y_n, acc' = cK k + cB acc.  Each is the
+// rounding of the contracted expression above (1 and 0 coefficients are exact).
 template <class R>
 __device__ __forceinline__ R rk_update(int method, int stage, R kv, R yv, R &accv, R a_next)
 {
-    if (method == 3) return kv;                               // operator test: store k_s
-    if (method == 0) return yv + a_next * kv;                 // Euler (solver.cu:14-21)
-    if (method == 1) {                                        // RK2 (solver.cu:23-30, 65-74)
-        if (stage == 1) { accv = kv; return yv + a_next * kv; }
-        return yv + a_next * (accv + kv);
-    }
-    // RK4 (solver.cu:32-39, 76-93): acc = k1 + 2 k2 + 2 k3, then (acc + k4)
-    if (stage == 1) { accv = kv; return yv + a_next * kv; }
-    if (stage < 4) { accv = accv + R(2) * kv; return yv + a_next * kv; }
-    return yv + a_next * (accv + kv);
+    const bool kstore = method == 3;
+    const bool last = (method == 1 && stage == 2) || (method == 2 && stage == 4);
+    const bool first = (method == 1 || method == 2) && stage == 1;
+    const R cA = last ? R(1) : R(0), cY = kstore ? R(0) : R(1), an = kstore ? R(1) : a_next;
+    const R cB = first ? R(0) : R(1), cK = (method == 2 && stage > 1 && stage < 4) ? R(2) : R(1);
+    const R t = fma(cA, accv, kv);
+    const R out = fma(an, t, cY * yv);
+    accv = fma(cK, kv, cB * accv);
+    return out;
 }
 
 __device__ __forceinline__ bool stage_keeps_acc(int method, int stage)
