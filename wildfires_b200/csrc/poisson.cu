@@ -19,6 +19,7 @@
 #include <math.h>
 
 #include "fft.cuh"
+#include "fft_pr.cuh"
 #include "wf_internal.h"
 
 namespace wf {
@@ -50,12 +51,66 @@ constexpr int kRadixFft = 8;
 template <int L, int RB> constexpr int kRad = (L >= 12) ? 16 : RB;
 template <int L, int RB> __device__ __forceinline__ int padl(int i) { return fft::pad<kRad<L, RB>>(i); }
 
+// z weights of the divergence at plane k: the one-sided weights f0, f1, f2 of
+// planes 0, 1, 2 at k = 0 and the centred weight c = 1/(dz_{k-1} + dz_k) above
+// (the reference's differences of pressure.cu:37-95 with the division folded
+// into a weight, the values of the zc table's ZF0..ZF2 and ZC rows).
+struct DivZ {
+    double f0, f1, f2, c;
+};
+__device__ __forceinline__ DivZ div_weights(const double *z, int k)
+{
+    DivZ w{0.0, 0.0, 0.0, 0.0};
+    if (k == 0) {
+        const double A = z[1] - z[0], B = z[2] - z[1];
+        w.f0 = -(2 * A + B) / (A * (A + B));
+        w.f1 = (A + B) / (A * B);
+        w.f2 = -A / (B * (A + B));
+    } else {
+        w.c = 1.0 / ((z[k] - z[k - 1]) + (z[k + 1] - z[k]));
+    }
+    return w;
+}
+
+// Divergence of the intermediate velocity at (i, j, k), k < Nz-1, as the
+// reference forms it (pressure.cu:37-95): periodic centred differences in x
+// and y, a one-sided second-order difference at k = 0; idx = 1/dx, idy = 1/dy.
+template <class R>
+__device__ __forceinline__ double velocity_divergence(const PoissonArgs<R> &a, int i, int j, int k, double idx,
+                                                      double idy, const DivZ &w)
+{
+    const Geom &g = a.g;
+    const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz, N = g.N;
+    const int im1 = (i == 0) ? Nx - 2 : i - 1, ip1 = (i + 1 == Nx - 1) ? 0 : i + 1;
+    const int jm1 = (j == 0) ? Ny - 2 : j - 1, jp1 = (j + 1 == Ny - 1) ? 0 : j + 1;
+    const R *U = a.y1;
+    const size_t c = ((size_t)i * Ny + j) * Nz + k;
+    const size_t cxm = ((size_t)im1 * Ny + j) * Nz + k, cxp = ((size_t)ip1 * Ny + j) * Nz + k;
+    const size_t cym = ((size_t)i * Ny + jm1) * Nz + k, cyp = ((size_t)i * Ny + jp1) * Nz + k;
+    const double u = U[c], v = U[(size_t)N + c];
+    const double u_im1 = U[cxm], u_ip1 = U[cxp];
+    const double v_jm1 = U[(size_t)N + cym], v_jp1 = U[(size_t)N + cyp];
+    const R *W = U + 2 * (size_t)N;
+    double wz;
+    if (k == 0) {
+        wz = w.f0 * (double)W[c] + w.f1 * (double)W[c + 1] + w.f2 * (double)W[c + 2];
+    } else {
+        wz = ((double)W[c + 1] - (double)W[c - 1]) * w.c;
+    }
+    const double ux = (0.5 * (u_ip1 + u) - 0.5 * (u + u_im1)) * idx;
+    const double vy = (0.5 * (v_jp1 + v) - 0.5 * (v + v_jm1)) * idy;
+    return ux + vy + wz;
+}
+
 // Poisson source at (i, j, k), k < Nz-1 (pressure.cu:37-95 and 150-321).
 template <class R>
 __device__ double poisson_source(const PoissonArgs<R> &a, int i, int j, int k)
 {
     const Geom &g = a.g;
     const Phys &ph = a.ph;
+    const double div = velocity_divergence(a, i, j, k, 1.0 / ph.dx, 1.0 / ph.dy, div_weights(g.z, k));
+    if (ph.variable_density == 0) return ph.rho_inf * div / ph.dt;
+    // variable density: f = rho_n (div u* - D_T)/dt + grad(rho).grad(p)/rho
     const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz, N = g.N;
     const int im1 = (i == 0) ? Nx - 2 : i - 1, ip1 = (i + 1 == Nx - 1) ? 0 : i + 1;
     const int jm1 = (j == 0) ? Ny - 2 : j - 1, jp1 = (j + 1 == Ny - 1) ? 0 : j + 1;
@@ -64,28 +119,15 @@ __device__ double poisson_source(const PoissonArgs<R> &a, int i, int j, int k)
     const size_t cxm = ((size_t)im1 * Ny + j) * Nz + k, cxp = ((size_t)ip1 * Ny + j) * Nz + k;
     const size_t cym = ((size_t)i * Ny + jm1) * Nz + k, cyp = ((size_t)i * Ny + jp1) * Nz + k;
     const double *z = g.z;
-    const double u = U[c], v = U[(size_t)N + c];
-    const double u_im1 = U[cxm], u_ip1 = U[cxp];
-    const double v_jm1 = U[(size_t)N + cym], v_jp1 = U[(size_t)N + cyp];
-    const R *W = U + 2 * (size_t)N;
-    double wz;
     double dzk_f = 0, dzkp1_f = 0, dzkp2_f = 0, dzkm1_c = 0, dzk_c = 0;
     if (k == 0) {
         dzk_f = z[1] - z[0];
         dzkp1_f = z[2] - z[1];
         dzkp2_f = z[3] - z[2];
-        const double A = dzk_f, B = dzkp1_f;
-        wz = -(2 * A + B) * (double)W[c] / (A * (A + B)) + (A + B) * (double)W[c + 1] / (A * B) -
-             A * (double)W[c + 2] / (B * (A + B));
     } else {
         dzkm1_c = z[k] - z[k - 1];
         dzk_c = z[k + 1] - z[k];
-        wz = ((double)W[c + 1] - (double)W[c - 1]) / (dzk_c + dzkm1_c);
     }
-    const double ux = (0.5 * (u_ip1 + u) - 0.5 * (u + u_im1)) / ph.dx;
-    const double vy = (0.5 * (v_jp1 + v) - 0.5 * (v + v_jm1)) / ph.dy;
-    if (ph.variable_density == 0) return ph.rho_inf * (ux + vy + wz) / ph.dt;
-    // variable density: f = rho_n (div u* - D_T)/dt + grad(rho).grad(p)/rho
     const R *T1 = U + 3 * (size_t)N;
     const R *Tn = a.yn + 3 * (size_t)N;
     const double *p = a.p;
@@ -142,7 +184,7 @@ __device__ double poisson_source(const PoissonArgs<R> &a, int i, int j, int k)
                      h_c * ph.alpha_s * ph.sigma_s * (T_gas - T_solid) / (ph.c_p * Ti * ri / T_gas);
     const double divT = (dk + 12 * kSigmaSB * ph.delta * pow(T, 2) * (Tx * Tx + Ty * Ty + Tz * Tz) +
                          (kT + 4 * kSigmaSB * ph.delta * pow(T, 3)) * lap_T) / (Ti * ri * ph.c_p) + q / T;
-    return rho * (ux + vy + wz - divT) / ph.dt + (rhox * px + rhoy * py + rhoz * pz) / rho;
+    return rho * (div - divT) / ph.dt + (rhox * px + rhoy * py + rhoz * pz) / rho;
 }
 
 // Length-n DFT of the line (buf, jj): one power-of-two FFT when n = M, else
@@ -191,16 +233,53 @@ __device__ __forceinline__ void line_dft(const FftDesc &d, double2 *buf, int jj,
         });
 }
 
+// Line engines.  A kernel stages LB lines of stride LS in shared memory
+// (element idx of a line at pos(idx)) and transforms each with run<INV>, which
+// every thread of the block calls with its line(tid) and lane(tid).
+//   EngS: power-of-two Stockham, or Bluestein around it; threads of a line
+//         interleave (line = tid % LB) and synchronise the block.
+//   EngPR: prime-factor + Rader (fft_pr.cuh), one warp per line, no block
+//         barrier inside.
+template <int L, int RB>
+struct EngS {
+    using SH = fft::Shape<L, kRad<L, RB>>;
+    static constexpr bool kPR = false;
+    static constexpr int kL = L;
+    static constexpr int LB = SH::LB, LS = SH::LS;
+    static constexpr size_t smem_bytes = SH::smem_bytes;
+    __device__ __forceinline__ static int line(int tid) { return tid % LB; }
+    __device__ __forceinline__ static int lane(int tid) { return tid / LB; }
+    __device__ __forceinline__ static int pos(int i) { return padl<L, RB>(i); }
+    template <bool INV, class Pre, class Post>
+    __device__ __forceinline__ static void run(const FftDesc &d, double2 *buf, int jj, Pre pre, Post post)
+    {
+        line_dft<L, INV, RB>(d, buf, jj, pre, post);
+    }
+};
+template <class Plan>
+struct EngPR {
+    static constexpr bool kPR = true;
+    static constexpr int LB = Plan::LB, LS = Plan::LS;
+    static constexpr size_t smem_bytes = Plan::smem_bytes;
+    __device__ __forceinline__ static int line(int tid) { return tid >> 5; }
+    __device__ __forceinline__ static int lane(int tid) { return tid & 31; }
+    __device__ __forceinline__ static int pos(int i) { return i; }
+    template <bool INV, class Pre, class Post>
+    __device__ __forceinline__ static void run(const FftDesc &d, double2 *buf, int jj, Pre pre, Post post)
+    {
+        Plan::template run<INV>(fft::PrTables{d.prb, d.prmap, d.pr_e1}, buf, jj, pre, post);
+    }
+};
+
 // P1: source + top plane, forward FFT in y of packed slice pairs.  Block
 // (pair group, i): LB complex lines, line q packs slices 2(pair0+q) (real
 // part) and 2(pair0+q)+1 (imaginary part); slice nk is the top-plane pressure.
 // The pair group is the fast grid index, so the blocks resident at one time
 // read whole z-columns of the same x-plane of the state.
-template <int L, class R>
+template <class E, class R>
 __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_rhs_ffty(const PoissonArgs<R> a)
 {
-    using SH = fft::Shape<L, kRad<L, kRadixRhs>>;
-    constexpr int LB = SH::LB, LS = SH::LS;
+    constexpr int LB = E::LB, LS = E::LS;
     extern __shared__ double2 smem[];
     const Geom &g = a.g;
     const int n0 = g.Nx - 1, n1 = g.Ny - 1, nk = g.Nz - 1, h1 = a.h1;
@@ -208,20 +287,49 @@ __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_rhs_ffty(const Poisson
     const int pair0 = blockIdx.x * LB;
     const int nslices = nk + 1;                      // f slices + top-plane pressure
     double *Ad = reinterpret_cast<double *>(smem);
-    for (int t = threadIdx.x; t < n1 * 2 * LB; t += 256) {
-        const int jj = t / (2 * LB), q = t - jj * (2 * LB);
-        const int kk = 2 * pair0 + q;
-        double val = 0.0;
-        if (kk < nk) val = poisson_source(a, i, jj, kk);
-        else if (kk == nk) val = a.p[((size_t)i * g.Ny + jj) * g.Nz + (g.Nz - 1)];
-        Ad[2 * ((q >> 1) * LS + padl<L, kRadixRhs>(jj)) + (q & 1)] = val;
+    const int total = n1 * 2 * LB;
+    if (a.ph.variable_density == 0) {
+        // the source is the scaled divergence: SU points per thread at a
+        // time, so that their loads are in flight together
+        constexpr int SU = 4;
+        const double idx = 1.0 / a.ph.dx, idy = 1.0 / a.ph.dy, scale = a.ph.rho_inf / a.ph.dt;
+        __shared__ DivZ s_w[2 * LB];   // z weights of the block's slices
+        if (threadIdx.x < 2 * LB && 2 * pair0 + threadIdx.x < nk) s_w[threadIdx.x] = div_weights(g.z, 2 * pair0 + threadIdx.x);
+        __syncthreads();
+        for (int t0 = threadIdx.x; t0 < total; t0 += 256 * SU) {
+            double val[SU];
+#pragma unroll
+            for (int r = 0; r < SU; r++) {
+                const int t = t0 + 256 * r;
+                const int jj = t / (2 * LB), q = t - jj * (2 * LB);
+                const int kk = 2 * pair0 + q;
+                val[r] = 0.0;
+                if (t < total && kk < nk) val[r] = scale * velocity_divergence(a, i, jj, kk, idx, idy, s_w[q]);
+                else if (t < total && kk == nk) val[r] = a.p[((size_t)i * g.Ny + jj) * g.Nz + (g.Nz - 1)];
+            }
+#pragma unroll
+            for (int r = 0; r < SU; r++) {
+                const int t = t0 + 256 * r;
+                const int jj = t / (2 * LB), q = t - jj * (2 * LB);
+                if (t < total) Ad[2 * ((q >> 1) * LS + E::pos(jj)) + (q & 1)] = val[r];
+            }
+        }
+    } else {
+        for (int t = threadIdx.x; t < total; t += 256) {
+            const int jj = t / (2 * LB), q = t - jj * (2 * LB);
+            const int kk = 2 * pair0 + q;
+            double val = 0.0;
+            if (kk < nk) val = poisson_source(a, i, jj, kk);
+            else if (kk == nk) val = a.p[((size_t)i * g.Ny + jj) * g.Nz + (g.Nz - 1)];
+            Ad[2 * ((q >> 1) * LS + E::pos(jj)) + (q & 1)] = val;
+        }
     }
     __syncthreads();
     {
-        const int q = threadIdx.x % LB, jj = threadIdx.x / LB;
+        const int q = E::line(threadIdx.x), jj = E::lane(threadIdx.x);
         double2 *buf = smem + q * LS;
-        line_dft<L, false, kRadixRhs>(
-            a.fy, buf, jj, [&](int idx) { return buf[padl<L, kRadixRhs>(idx)]; }, [&](int idx, double2 v) { buf[padl<L, kRadixRhs>(idx)] = v; });
+        E::template run<false>(
+            a.fy, buf, jj, [&](int idx) { return buf[E::pos(idx)]; }, [&](int idx, double2 v) { buf[E::pos(idx)] = v; });
     }
     __syncthreads();
     // split each packed transform into the two half spectra
@@ -229,8 +337,8 @@ __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_rhs_ffty(const Poisson
     for (int t = threadIdx.x; t < kp * h1; t += 256) {
         const int line = t / h1, s = t - line * h1;
         const double2 *Rb = smem + line * LS;
-        const double2 Zs = Rb[padl<L, kRadixRhs>(s)];
-        const double2 Zc = cconj(Rb[padl<L, kRadixRhs>(s == 0 ? 0 : n1 - s)]);
+        const double2 Zs = Rb[E::pos(s)];
+        const double2 Zc = cconj(Rb[E::pos(s == 0 ? 0 : n1 - s)]);
         const double2 Fa = make_double2(0.5 * (Zs.x + Zc.x), 0.5 * (Zs.y + Zc.y));
         const double2 Fb = make_double2(0.5 * (Zs.y - Zc.y), -0.5 * (Zs.x - Zc.x));
         const int kk0 = 2 * (pair0 + line);
@@ -296,6 +404,40 @@ __global__ void __launch_bounds__(256, kFftMinBlocks)
         __syncthreads();      // buffer free before the fetch two items ahead
     }
     cp_async_wait<0>();
+}
+
+// P2/P4 with the prime-factor + Rader engine: block (s group, kk) copies LB
+// lines (consecutive s, one warp each) into shared memory, each warp
+// transforms its line with no block barrier, and the block writes the lines
+// back.  Both copies move 128 contiguous bytes per 8 threads (LB = 8 lines of
+// 16-byte values); LS = 1 (mod 8) keeps the shared-memory side conflict-free.
+template <class E, bool INV>
+__global__ void __launch_bounds__(256, 2) k_p_fftx_pr(double2 *__restrict__ G, const FftDesc fx, int n0, int h1)
+{
+    constexpr int LB = E::LB, LS = E::LS;
+    static_assert(LB == 8, "copies assume 8 lines of 16-byte values per 128 bytes");
+    extern __shared__ double2 smem[];
+    const int s0 = blockIdx.x * LB;
+    const int nl = min(LB, h1 - s0);
+    double2 *g = G + (size_t)blockIdx.y * n0 * h1 + s0;
+    for (int e = threadIdx.x; e < LB * n0; e += 256) {
+        const int l = e % LB, idx = e / LB;
+        if (l < nl) cp_async16(smem + l * LS + idx, g + (size_t)idx * h1 + l, true);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    const int q = E::line(threadIdx.x);
+    if (q < nl) {
+        double2 *buf = smem + q * LS;
+        E::template run<INV>(
+            fx, buf, E::lane(threadIdx.x), [&](int idx) { return buf[idx]; }, [&](int idx, double2 v) { buf[idx] = v; });
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < LB * n0; e += 256) {
+        const int l = e % LB, idx = e / LB;
+        if (l < nl) g[(size_t)idx * h1 + l] = smem[l * LS + idx];
+    }
 }
 
 // P3: tridiagonal solve in z per (r, s) (pressure.cu:356-390, 473-504, 418-443).
@@ -396,11 +538,10 @@ __global__ void __launch_bounds__(128, 8) k_p_tridiag(double2 *__restrict__ G, c
 
 // P5: inverse FFT in y of packed slice pairs, normalisation, write p and the
 // periodic duplicate planes (pressure.cu:392-416, deterministic here).
-template <int L, class R>
+template <class E, class R>
 __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_iffty_out(const PoissonArgs<R> a)
 {
-    using SH = fft::Shape<L, kRad<L, kRadixFft>>;
-    constexpr int LB = SH::LB, LS = SH::LS;
+    constexpr int LB = E::LB, LS = E::LS;
     extern __shared__ double2 smem[];
     const Geom &g = a.g;
     const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz;
@@ -410,32 +551,49 @@ __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_iffty_out(const Poisso
     const int np = (nk + 1) / 2;
     const int kp = min(LB, np - pair0);
     const bool even = (n1 % 2) == 0;
-    for (int t = threadIdx.x; t < LB * n1; t += 256) {
-        const int line = t / n1, s = t - line * n1;
-        double2 val = make_double2(0.0, 0.0);
-        if (line < kp) {
+    // each stored half-spectrum value ss fills position ss and its mirror
+    // n1 - ss (conjugates) of the packed line; SU values per thread at a time
+    // so that their loads are in flight together
+    constexpr int SU = 4;
+    const int total = LB * h1;
+    for (int t0 = threadIdx.x; t0 < total; t0 += 256 * SU) {
+        double2 Fa[SU], Fb[SU];
+#pragma unroll
+        for (int r = 0; r < SU; r++) {
+            const int t = t0 + 256 * r;
+            const int line = t / h1, ss = t - line * h1;
             const int kk0 = 2 * (pair0 + line), kk1 = kk0 + 1;
-            const int ss = (s < h1) ? s : n1 - s;
-            double2 Fa = a.G[((size_t)kk0 * n0 + i) * h1 + ss];
-            double2 Fb = (kk1 < nk) ? a.G[((size_t)kk1 * n0 + i) * h1 + ss] : make_double2(0.0, 0.0);
-            if (ss == 0 || (even && ss == n1 / 2)) {
-                Fa.y = 0.0;
-                Fb.y = 0.0;
+            Fa[r] = Fb[r] = make_double2(0.0, 0.0);
+            if (t < total && line < kp) {
+                Fa[r] = a.G[((size_t)kk0 * n0 + i) * h1 + ss];
+                if (kk1 < nk) Fb[r] = a.G[((size_t)kk1 * n0 + i) * h1 + ss];
             }
-            if (s >= h1) {
-                Fa.y = -Fa.y;
-                Fb.y = -Fb.y;
-            }
-            val = make_double2(Fa.x - Fb.y, Fa.y + Fb.x);
         }
-        smem[line * LS + padl<L, kRadixFft>(s)] = val;
+#pragma unroll
+        for (int r = 0; r < SU; r++) {
+            const int t = t0 + 256 * r;
+            const int line = t / h1, ss = t - line * h1;
+            if (t < total) {
+                double2 fa = Fa[r], fb = Fb[r];
+                if (ss == 0 || (even && ss == n1 / 2)) {
+                    fa.y = 0.0;
+                    fb.y = 0.0;
+                }
+                smem[line * LS + E::pos(ss)] = make_double2(fa.x - fb.y, fa.y + fb.x);
+                if (ss >= 1 && ss <= n1 - h1) {
+                    fa.y = -fa.y;
+                    fb.y = -fb.y;
+                    smem[line * LS + E::pos(n1 - ss)] = make_double2(fa.x - fb.y, fa.y + fb.x);
+                }
+            }
+        }
     }
     __syncthreads();
     {
-        const int q = threadIdx.x % LB, jj = threadIdx.x / LB;
+        const int q = E::line(threadIdx.x), jj = E::lane(threadIdx.x);
         double2 *buf = smem + q * LS;
-        line_dft<L, true, kRadixFft>(
-            a.fy, buf, jj, [&](int idx) { return buf[padl<L, kRadixFft>(idx)]; }, [&](int idx, double2 v) { buf[padl<L, kRadixFft>(idx)] = v; });
+        E::template run<true>(
+            a.fy, buf, jj, [&](int idx) { return buf[E::pos(idx)]; }, [&](int idx, double2 v) { buf[E::pos(idx)] = v; });
     }
     __syncthreads();
     const double norm = (double)n0 * (double)n1;
@@ -445,7 +603,7 @@ __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_iffty_out(const Poisso
         const int jj = t / ns, q = t - jj * ns;
         const int kk = 2 * pair0 + q;
         if (kk >= nk) continue;
-        const double2 zv = smem[(q >> 1) * LS + padl<L, kRadixFft>(jj)];
+        const double2 zv = smem[(q >> 1) * LS + E::pos(jj)];
         const double val = ((q & 1) ? zv.y : zv.x) / norm;
         p[((size_t)i * Ny + jj) * Nz + kk] = val;
         if (jj == 0) p[((size_t)i * Ny + (Ny - 1)) * Nz + kk] = val;
@@ -464,76 +622,122 @@ __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_iffty_out(const Poisso
     }
 }
 
-// ---- launch: one kernel instantiation per inner FFT length ----------------
+// ---- launch: one kernel instantiation per line engine ----------------------
 constexpr int kMinL = 2, kMaxL = 12;
 
-template <class Op, class... A>
-cudaError_t by_length(int L, A &...args)
+// Prime-factor + Rader plans compiled in: n = N1 * P, P - 1 = F1 * F2.
+using PlanPr511 = fft::PrPlan<7, 73, 8, 9>;
+
+// Engine of a descriptor: a Rader plan when the descriptor carries one (its
+// length is then one of the plans above), else the power-of-two engine of
+// inner length 2^L with largest radix RB.
+template <class Op, int RB, class... A>
+cudaError_t by_engine(const FftDesc &d, A &...args)
 {
-    switch (L) {
-    case 2: return Op::template go<2>(args...);
-    case 3: return Op::template go<3>(args...);
-    case 4: return Op::template go<4>(args...);
-    case 5: return Op::template go<5>(args...);
-    case 6: return Op::template go<6>(args...);
-    case 7: return Op::template go<7>(args...);
-    case 8: return Op::template go<8>(args...);
-    case 9: return Op::template go<9>(args...);
-    case 10: return Op::template go<10>(args...);
-    case 11: return Op::template go<11>(args...);
-    case 12: return Op::template go<12>(args...);
+    if (d.pr) {
+        switch (d.n) {
+        case PlanPr511::n: return Op::template go<EngPR<PlanPr511>>(args...);
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (d.L) {
+    case 2: return Op::template go<EngS<2, RB>>(args...);
+    case 3: return Op::template go<EngS<3, RB>>(args...);
+    case 4: return Op::template go<EngS<4, RB>>(args...);
+    case 5: return Op::template go<EngS<5, RB>>(args...);
+    case 6: return Op::template go<EngS<6, RB>>(args...);
+    case 7: return Op::template go<EngS<7, RB>>(args...);
+    case 8: return Op::template go<EngS<8, RB>>(args...);
+    case 9: return Op::template go<EngS<9, RB>>(args...);
+    case 10: return Op::template go<EngS<10, RB>>(args...);
+    case 11: return Op::template go<EngS<11, RB>>(args...);
+    case 12: return Op::template go<EngS<12, RB>>(args...);
     default: return cudaErrorInvalidValue;
     }
 }
 
 template <class R>
 struct LaunchP1 {
-    template <int L> static cudaError_t go(const PoissonArgs<R> &a, cudaStream_t &s)
+    template <class E> static cudaError_t go(const PoissonArgs<R> &a, cudaStream_t &s)
     {
-        using SH = fft::Shape<L, kRad<L, kRadixRhs>>;
         const int np = (a.g.Nz - 1 + 2) / 2;
-        k_p_rhs_ffty<L, R><<<dim3((np + SH::LB - 1) / SH::LB, a.g.Nx - 1), 256, SH::smem_bytes, s>>>(a);
+        k_p_rhs_ffty<E, R><<<dim3((np + E::LB - 1) / E::LB, a.g.Nx - 1), 256, E::smem_bytes, s>>>(a);
         return cudaSuccess;
     }
 };
 template <class R>
 struct LaunchP5 {
-    template <int L> static cudaError_t go(const PoissonArgs<R> &a, cudaStream_t &s)
+    template <class E> static cudaError_t go(const PoissonArgs<R> &a, cudaStream_t &s)
     {
-        using SH = fft::Shape<L, kRad<L, kRadixFft>>;
         const int np = (a.g.Nz - 1 + 1) / 2;
-        k_p_iffty_out<L, R><<<dim3(a.g.Nx - 1, (np + SH::LB - 1) / SH::LB), 256, SH::smem_bytes, s>>>(a);
+        k_p_iffty_out<E, R><<<dim3(a.g.Nx - 1, (np + E::LB - 1) / E::LB), 256, E::smem_bytes, s>>>(a);
         return cudaSuccess;
     }
 };
 template <bool INV>
 struct LaunchFx {
-    template <int L> static cudaError_t go(double2 *const &G, const FftDesc &fx, const int &nslices, const int &n0,
+    template <class E> static cudaError_t go(double2 *const &G, const FftDesc &fx, const int &nslices, const int &n0,
                                            const int &h1, cudaStream_t &s)
     {
-        using SH = fft::Shape<L, kRad<L, kRadixFft>>;
-        const int nitems = nslices * ((h1 + SH::LB - 1) / SH::LB);
-        const int blocks = min(nitems, kFftMinBlocks * g_poisson_sms);
-        k_p_fftx<L, INV><<<blocks, 256, 2 * SH::smem_bytes, s>>>(G, fx, n0, h1, nslices);
+        if constexpr (E::kPR) {
+            k_p_fftx_pr<E, INV><<<dim3((h1 + E::LB - 1) / E::LB, nslices), 256, E::smem_bytes, s>>>(G, fx, n0, h1);
+        } else {
+            constexpr int L = E::kL;
+            const int nitems = nslices * ((h1 + E::LB - 1) / E::LB);
+            const int blocks = min(nitems, kFftMinBlocks * g_poisson_sms);
+            k_p_fftx<L, INV><<<blocks, 256, 2 * E::smem_bytes, s>>>(G, fx, n0, h1, nslices);
+        }
         return cudaSuccess;
     }
 };
 
+template <class R, class E, class EF>
+cudaError_t set_engine_attributes()
+{
+    const int b1 = (int)E::smem_bytes, b = (int)EF::smem_bytes;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_p_rhs_ffty<E, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, b1))) return e;
+    if ((e = cudaFuncSetAttribute(k_p_iffty_out<EF, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    return cudaSuccess;
+}
 template <class R, int L>
 cudaError_t set_attributes_for()
 {
-    const int b1 = (int)fft::Shape<L, kRad<L, kRadixRhs>>::smem_bytes;
-    const int b = (int)fft::Shape<L, kRad<L, kRadixFft>>::smem_bytes;
+    using E = EngS<L, kRadixRhs>;
+    using EF = EngS<L, kRadixFft>;
+    const int bx = 2 * (int)EF::smem_bytes;   // the persistent x kernel holds two item buffers
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_p_rhs_ffty<L, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, b1))) return e;
-    if ((e = cudaFuncSetAttribute(k_p_iffty_out<L, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
-    if ((e = cudaFuncSetAttribute(k_p_fftx<L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * b))) return e;
-    if ((e = cudaFuncSetAttribute(k_p_fftx<L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * b))) return e;
+    if ((e = set_engine_attributes<R, E, EF>())) return e;
+    if ((e = cudaFuncSetAttribute(k_p_fftx<L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bx))) return e;
+    if ((e = cudaFuncSetAttribute(k_p_fftx<L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bx))) return e;
     if constexpr (L < kMaxL) return set_attributes_for<R, L + 1>();
+    return cudaSuccess;
+}
+template <class R, class Plan>
+cudaError_t set_pr_attributes()
+{
+    using E = EngPR<Plan>;
+    const int b = (int)E::smem_bytes;
+    cudaError_t e;
+    if ((e = set_engine_attributes<R, E, E>())) return e;
+    if ((e = cudaFuncSetAttribute(k_p_fftx_pr<E, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
+    if ((e = cudaFuncSetAttribute(k_p_fftx_pr<E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
     return cudaSuccess;
 }
 
 }  // namespace
+
+bool poisson_pr_plan(int n, int f[4])
+{
+    if (n == PlanPr511::n) {
+        f[0] = PlanPr511::N1;
+        f[1] = PlanPr511::P;
+        f[2] = PlanPr511::F1;
+        f[3] = PlanPr511::F2;
+        return true;
+    }
+    return false;
+}
 
 template <class R> cudaError_t poisson_set_attributes()
 {
@@ -541,6 +745,7 @@ template <class R> cudaError_t poisson_set_attributes()
     cudaError_t e = cudaGetDevice(&dev);
     if (!e) e = cudaDeviceGetAttribute(&g_poisson_sms, cudaDevAttrMultiProcessorCount, dev);
     if (!e) e = set_attributes_for<R, kMinL>();
+    if (!e) e = set_pr_attributes<R, PlanPr511>();
     return e;
 }
 template cudaError_t poisson_set_attributes<double>();
@@ -551,19 +756,19 @@ cudaError_t launch_poisson_impl(const PoissonArgs<R> &a, const double *zt, cudaS
 {
     int n0 = a.g.Nx - 1, nk = a.g.Nz - 1, h1 = a.h1;
     cudaError_t e;
-    if ((e = by_length<LaunchP1<R>>(a.fy.L, a, s))) return e;
+    if ((e = by_engine<LaunchP1<R>, kRadixRhs>(a.fy, a, s))) return e;
     if (ev) cudaEventRecord(ev[0], s);
     int ns = nk + 1;
     double2 *G = a.G;
-    if ((e = by_length<LaunchFx<false>>(a.fx.L, G, a.fx, ns, n0, h1, s))) return e;
+    if ((e = by_engine<LaunchFx<false>, kRadixFft>(a.fx, G, a.fx, ns, n0, h1, s))) return e;
     if (ev) cudaEventRecord(ev[1], s);
     if (nk > kSeg * kMaxSeg) return cudaErrorInvalidValue;
     k_p_tridiag<<<dim3(n0, (h1 + 127) / 128), 128, 0, s>>>(a.G, a.kx2, a.ky2, zt, n0, h1, nk);
     if (ev) cudaEventRecord(ev[2], s);
     ns = nk;
-    if ((e = by_length<LaunchFx<true>>(a.fx.L, G, a.fx, ns, n0, h1, s))) return e;
+    if ((e = by_engine<LaunchFx<true>, kRadixFft>(a.fx, G, a.fx, ns, n0, h1, s))) return e;
     if (ev) cudaEventRecord(ev[3], s);
-    if ((e = by_length<LaunchP5<R>>(a.fy.L, a, s))) return e;
+    if ((e = by_engine<LaunchP5<R>, kRadixFft>(a.fy, a, s))) return e;
     if (ev) cudaEventRecord(ev[4], s);
     return cudaGetLastError();
 }

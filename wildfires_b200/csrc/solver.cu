@@ -44,14 +44,95 @@ const long double kPiL = 3.141592653589793238462643383279502884L;
 
 struct HostFft {
     FftDesc d;
-    std::vector<double2> tw, chirp, filt;
+    std::vector<double2> tw, chirp, filt, prb;
+    std::vector<int> prmap;
 };
+
+long long pow_mod(long long b, long long e, long long m)
+{
+    long long r = 1 % m;
+    b %= m;
+    for (; e > 0; e >>= 1) {
+        if (e & 1) r = r * b % m;
+        b = b * b % m;
+    }
+    return r;
+}
+// inverse of a modulo m (gcd(a, m) = 1, m small)
+int inv_mod(int a, int m)
+{
+    for (int t = 0; t < m; t++)
+        if ((long long)a * t % m == 1 % m) return t;
+    return 0;
+}
+// smallest primitive root of the prime P
+int primitive_root(int P)
+{
+    std::vector<int> fac;
+    for (int r = 2, x = P - 1; x > 1; r++)
+        if (x % r == 0) {
+            fac.push_back(r);
+            while (x % r == 0) x /= r;
+        }
+    for (int g = 2; g < P; g++) {
+        bool ok = true;
+        for (int r : fac) ok = ok && pow_mod(g, (P - 1) / r, P) != 1;
+        if (ok) return g;
+    }
+    return 0;
+}
+
+// Tables of the prime-factor + Rader engine for n = N1 P, P - 1 = F1 F2
+// (layout in fft_pr.cuh); the filter in long double (setup only).
+void plan_pr(HostFft &h, const int f[4])
+{
+    const int n = h.d.n, N1 = f[0], P = f[1], F1 = f[2], F2 = f[3], Q = P - 1;
+    const int g = primitive_root(P), gi = (int)pow_mod(g, P - 2, P);
+    const int e2 = (int)((long long)N1 * inv_mod(N1 % P, P) % n);
+    h.d.pr_e1 = (N1 > 1) ? (int)((long long)P * inv_mod(P % N1, N1) % n) : 0;
+    h.prmap.assign(P + Q, 0);
+    for (int q1 = 0; q1 < F1; q1++)
+        for (int q2 = 0; q2 < F2; q2++) {
+            const int q = (F2 * q1 + F1 * q2) % Q;
+            h.prmap[1 + F2 * q1 + q2] = (int)pow_mod(g, q, P);
+            h.prmap[P + F2 * q1 + q2] = (int)((long long)e2 * pow_mod(gi, q, P) % n);
+        }
+    // B'[j] = (1/Q) sum_t exp(-2 pi i gi^t / P) exp(-2 pi i j t / Q)
+    std::vector<long double> br(Q), bi(Q);
+    for (int t = 0; t < Q; t++) {
+        const long double a = -2.0L * kPiL * (long double)pow_mod(gi, t, P) / (long double)P;
+        br[t] = cosl(a);
+        bi[t] = sinl(a);
+    }
+    const int c1 = F2 * inv_mod(F2 % F1, F1), c2 = (F2 > 1) ? F1 * inv_mod(F1 % F2, F2) : 0;
+    h.prb.resize(Q);
+    for (int j1 = 0; j1 < F1; j1++)
+        for (int j2 = 0; j2 < F2; j2++) {
+            const int j = (j1 * c1 + j2 * c2) % Q;
+            long double sr = 0, si = 0;
+            for (int t = 0; t < Q; t++) {
+                const long double a = -2.0L * kPiL * (long double)(((long long)j * t) % Q) / (long double)Q;
+                const long double c = cosl(a), sn = sinl(a);
+                sr += br[t] * c - bi[t] * sn;
+                si += br[t] * sn + bi[t] * c;
+            }
+            h.prb[j1 * F2 + j2] = make_double2((double)(sr / Q), (double)(si / Q));
+        }
+    h.d.pr = 1;
+}
 
 HostFft plan_fft(int n)
 {
     HostFft h;
     memset(&h.d, 0, sizeof(h.d));
     h.d.n = n;
+    // WF_FFT_RADER=0 keeps such lengths on Bluestein (for comparisons)
+    const char *rader = getenv("WF_FFT_RADER");
+    int f[4];
+    if (!(rader && rader[0] == '0') && poisson_pr_plan(n, f)) {
+        plan_pr(h, f);
+        return h;
+    }
     if ((n & (n - 1)) == 0) {
         h.d.m = n;
     } else {
@@ -232,6 +313,15 @@ template <class T> wf_status upload(wf_ctx *c, T **dst, const T *src, size_t n)
 wf_status upload_fft(wf_ctx *c, const HostFft &h, FftDesc &d)
 {
     d = h.d;
+    if (h.d.pr) {
+        double2 *rb = nullptr;
+        int *map = nullptr;
+        wf_status s = upload(c, &rb, h.prb.data(), h.prb.size());
+        if (!s) s = upload(c, &map, h.prmap.data(), h.prmap.size());
+        d.prb = rb;
+        d.prmap = map;
+        return s;
+    }
     double2 *tw = nullptr, *ch = nullptr, *fl = nullptr;
     wf_status s = upload(c, &tw, h.tw.data(), h.tw.size());
     if (s) return s;

@@ -189,7 +189,14 @@ struct FftDesc {
     const double2 *tw;      // exp(-2 pi i j / m), j < m
     const double2 *chirp;   // Bluestein: exp(-i pi j^2 / n), j < n
     const double2 *filt;    // Bluestein: FFT_m of the conjugate chirp filter
+    int pr;                 // 1: prime-factor + Rader plan of length n (fft_pr.cuh); tw, chirp, filt unused
+    const double2 *prb;     // Rader: DFT of the root-power filter / (P-1), (j1, j2) order
+    const int *prmap;       // Rader: input slot map [P] and output index map [P-1]
+    int pr_e1;              // Rader: CRT weight of the N1 residue
 };
+// Prime-factor + Rader plan compiled for length n: f = {N1, P, F1, F2} with
+// n = N1 P, P prime, P - 1 = F1 F2.  False for every other length.
+bool poisson_pr_plan(int n, int f[4]);
 
 template <class R>
 struct PoissonArgs {
