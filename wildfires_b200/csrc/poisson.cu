@@ -625,8 +625,21 @@ __global__ void __launch_bounds__(256, kFftMinBlocks) k_p_iffty_out(const Poisso
 // ---- launch: one kernel instantiation per line engine ----------------------
 constexpr int kMinL = 2, kMaxL = 12;
 
-// Prime-factor + Rader plans compiled in: n = N1 * P, P - 1 = F1 * F2.
-using PlanPr511 = fft::PrPlan<7, 73, 8, 9>;
+// Prime-factor + Rader plans compiled in: n = N1 * P, P - 1 = F1 * F2.  The
+// x and y lengths of the workloads: 511 (512-point grids), 255 (256), 159
+// (160) and 95 (96); 127 and 191 are prime with P - 1 = 2 * 63 and 2 * 95,
+// beyond these two-factor plans, and stay on Bluestein.
+template <class... Pl> struct PlanList {};
+using PrPlans = PlanList<fft::PrPlan<7, 73, 8, 9>, fft::PrPlan<15, 17, 16, 1>, fft::PrPlan<3, 53, 4, 13>,
+                         fft::PrPlan<5, 19, 2, 9>>;
+
+template <class Op, class... Pl, class... A>
+cudaError_t by_plan(PlanList<Pl...>, int n, A &...args)
+{
+    cudaError_t e = cudaErrorInvalidValue;
+    (void)((n == Pl::n ? (e = Op::template go<EngPR<Pl>>(args...), true) : false) || ...);
+    return e;
+}
 
 // Engine of a descriptor: a Rader plan when the descriptor carries one (its
 // length is then one of the plans above), else the power-of-two engine of
@@ -634,12 +647,7 @@ using PlanPr511 = fft::PrPlan<7, 73, 8, 9>;
 template <class Op, int RB, class... A>
 cudaError_t by_engine(const FftDesc &d, A &...args)
 {
-    if (d.pr) {
-        switch (d.n) {
-        case PlanPr511::n: return Op::template go<EngPR<PlanPr511>>(args...);
-        default: return cudaErrorInvalidValue;
-        }
-    }
+    if (d.pr) return by_plan<Op>(PrPlans{}, d.n, args...);
     switch (d.L) {
     case 2: return Op::template go<EngS<2, RB>>(args...);
     case 3: return Op::template go<EngS<3, RB>>(args...);
@@ -724,20 +732,22 @@ cudaError_t set_pr_attributes()
     if ((e = cudaFuncSetAttribute(k_p_fftx_pr<E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b))) return e;
     return cudaSuccess;
 }
+template <class R, class... Pl>
+cudaError_t set_pr_attributes_all(PlanList<Pl...>)
+{
+    cudaError_t e = cudaSuccess;
+    (void)(((e = set_pr_attributes<R, Pl>()) != cudaSuccess) || ...);
+    return e;
+}
+template <class... Pl>
+bool pr_plan_of(PlanList<Pl...>, int n, int f[4])
+{
+    return ((n == Pl::n ? (f[0] = Pl::N1, f[1] = Pl::P, f[2] = Pl::F1, f[3] = Pl::F2, true) : false) || ...);
+}
 
 }  // namespace
 
-bool poisson_pr_plan(int n, int f[4])
-{
-    if (n == PlanPr511::n) {
-        f[0] = PlanPr511::N1;
-        f[1] = PlanPr511::P;
-        f[2] = PlanPr511::F1;
-        f[3] = PlanPr511::F2;
-        return true;
-    }
-    return false;
-}
+bool poisson_pr_plan(int n, int f[4]) { return pr_plan_of(PrPlans{}, n, f); }
 
 template <class R> cudaError_t poisson_set_attributes()
 {
@@ -745,7 +755,7 @@ template <class R> cudaError_t poisson_set_attributes()
     cudaError_t e = cudaGetDevice(&dev);
     if (!e) e = cudaDeviceGetAttribute(&g_poisson_sms, cudaDevAttrMultiProcessorCount, dev);
     if (!e) e = set_attributes_for<R, kMinL>();
-    if (!e) e = set_pr_attributes<R, PlanPr511>();
+    if (!e) e = set_pr_attributes_all<R>(PrPlans{});
     return e;
 }
 template cudaError_t poisson_set_attributes<double>();
