@@ -258,6 +258,10 @@ struct wf_ctx {
         bool ok[2] = {false, false};
     } tmaps[4];
     int ntmaps = 0;
+    // FP32: maps of y_n (either step buffer) and acc for the boxes of a tile's own
+    // cells, with which the stage kernel prefetches its RK operands into L2
+    TensorMaps cmaps[3];
+    int ncmaps = 0;
 };
 
 namespace wfs {
@@ -515,6 +519,12 @@ template <class R> StageArgs<R> stage_args(wf_ctx *c, const void *X, const void 
     for (int q = 0; q < c->ntmaps; q++)
         if (c->tmaps[q].ptr == X)
             for (int b = 0; b < 2; b++) a.tmap[b] = c->tmaps[q].ok[b] ? c->tmaps[q].map[b] : nullptr;
+    for (int b = 0; b < 2; b++) a.pmap_yn[b] = a.pmap_acc[b] = nullptr;
+    for (int q = 0; q < c->ncmaps; q++)
+        for (int b = 0; b < 2; b++) {
+            if (c->cmaps[q].ptr == yn) a.pmap_yn[b] = c->cmaps[q].ok[b] ? c->cmaps[q].map[b] : nullptr;
+            if (c->cmaps[q].ptr == c->acc) a.pmap_acc[b] = c->cmaps[q].ok[b] ? c->cmaps[q].map[b] : nullptr;
+        }
     a.tile = c->tile;
     const double dt = c->P.dt;
     if (c->method == 0) a.a_next = dt;
@@ -995,6 +1005,19 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
             if (m.ok[0] || m.ok[1]) {
                 m.ptr = bufs[b];
                 c->ntmaps++;
+            }
+        }
+        // the RK operands' cell boxes (WF_NO_PREFETCH=1: none, for comparisons)
+        const void *cbufs[3] = {c->ybuf[0], c->ybuf[1], c->acc};
+        const bool no_pf = getenv("WF_NO_PREFETCH") && atoi(getenv("WF_NO_PREFETCH"));
+        for (int b = 0; b < 3 && encode && !no_pf; b++) {
+            if (!cbufs[b]) continue;
+            auto &m = c->cmaps[c->ncmaps];
+            m.ok[0] = stage_cell_map(m.map[0], (const float *)cbufs[b], Nx, Ny, Nz, 8, 16, encode);
+            m.ok[1] = stage_cell_map(m.map[1], (const float *)cbufs[b], Nx, Ny, Nz, 8, 8, encode);
+            if (m.ok[0] || m.ok[1]) {
+                m.ptr = cbufs[b];
+                c->ncmaps++;
             }
         }
     }

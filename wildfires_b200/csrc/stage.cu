@@ -244,7 +244,8 @@ template <class R> __device__ __forceinline__ R dz5(const R *w, R m2, R m1, R c,
 //      left to k_stage_bc; the values it needs are stored in a.bc.
 template <class R, int TI, int TJ, int KZ, int NT>
 __global__ void __launch_bounds__(NT, sizeof(R) != 4 ? 1 : NT > 256 ? 2 : (TI * TJ <= 64 ? 3 : 2))
-    k_stage_fused(const StageArgs<R> a, const __grid_constant__ CUtensorMap tmap, int use_tma, int ntk, int ntj, int nti)
+    k_stage_fused(const StageArgs<R> a, const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap pyn,
+                  const __grid_constant__ CUtensorMap pacc, int use_tma, int use_pf, int ntk, int ntj, int nti)
 {
     using TL = Tile<R, TI, TJ, KZ>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -286,6 +287,21 @@ __global__ void __launch_bounds__(NT, sizeof(R) != 4 ? 1 : NT > 256 ? 2 : (TI * 
                          : "r"((uint32_t)__cvta_generic_to_shared(sgs)), "l"(reinterpret_cast<uint64_t>(&tmap)),
                            "r"(k0 - 4), "r"(j0 - 2), "r"(i0 - 2), "r"(0), "r"(bar)
                          : "memory");
+        }
+        // RK operands of the tile's cells (yn, and acc when this stage reads it)
+        // into L2 while the tile loads and phase 2 runs: phase 3 then finds
+        // them there instead of waiting on DRAM.  A prefetch has no completion
+        // to wait for and ignores coordinates outside the buffer.
+        if (use_pf && threadIdx.x == 32) {
+            asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];"
+                         :
+                         : "l"(reinterpret_cast<uint64_t>(&pyn)), "r"(k0), "r"(j0), "r"(i0), "r"(0)
+                         : "memory");
+            if (stage_reads_acc(a.method, a.stage))
+                asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];"
+                             :
+                             : "l"(reinterpret_cast<uint64_t>(&pacc)), "r"(k0), "r"(j0), "r"(i0), "r"(0)
+                             : "memory");
         }
         issue_tile<R, TL, NT>(a, t, i0, j0, k0, !tma);
         cp_async_wait<0>();
@@ -807,12 +823,22 @@ template <class R> cudaError_t launch_stage(const StageArgs<R> &a, cudaStream_t 
         using SH = decltype(sh);
         const int ntk = (a.g.Nz + SH::KZ - 1) / SH::KZ, ntj = (a.g.Ny + SH::TJ - 1) / SH::TJ;
         const int nti = (a.g.Nx + SH::TI - 1) / SH::TI;
-        CUtensorMap m;
-        const void *src = (sizeof(R) == 4) ? a.tmap[SH::TJ == 16 ? 0 : 1] : nullptr;
+        const int w = SH::TJ == 16 ? 0 : 1;
+        CUtensorMap m, myn, macc;
+        const void *src = (sizeof(R) == 4) ? a.tmap[w] : nullptr;
+        const void *pyn = (sizeof(R) == 4) ? a.pmap_yn[w] : nullptr, *pacc = (sizeof(R) == 4) ? a.pmap_acc[w] : nullptr;
         if (src) memcpy(&m, src, sizeof(m));
         else memset(&m, 0, sizeof(m));
-        k_stage_fused<R, SH::TI, SH::TJ, SH::KZ, SH::NT><<<ntk * ntj * nti, SH::NT, SH::smem(), s>>>(a, m, src ? 1 : 0,
-                                                                                                    ntk, ntj, nti);
+        const bool pf = pyn && pacc;
+        if (pf) {
+            memcpy(&myn, pyn, sizeof(myn));
+            memcpy(&macc, pacc, sizeof(macc));
+        } else {
+            memset(&myn, 0, sizeof(myn));
+            memset(&macc, 0, sizeof(macc));
+        }
+        k_stage_fused<R, SH::TI, SH::TJ, SH::KZ, SH::NT><<<ntk * ntj * nti, SH::NT, SH::smem(), s>>>(
+            a, m, myn, macc, src ? 1 : 0, pf ? 1 : 0, ntk, ntj, nti);
         return cudaSuccess;
     });
     if (e) return e;
@@ -837,6 +863,22 @@ bool stage_tensor_map(void *out, const float *X, int Nx, int Ny, int Nz, int TI,
     const CUresult r = reinterpret_cast<Encode>(encode_fn)(
         reinterpret_cast<CUtensorMap *>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float *>(X), dims, strides,
         box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+bool stage_cell_map(void *out, const float *X, int Nx, int Ny, int Nz, int TI, int TJ, void *encode_fn)
+{
+    if (!encode_fn || Nz % 4 != 0 || (reinterpret_cast<uintptr_t>(X) & 15) != 0) return false;
+    using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    const cuuint64_t dims[4] = {(cuuint64_t)Nz, (cuuint64_t)Ny, (cuuint64_t)Nx, 4};
+    const cuuint64_t strides[3] = {(cuuint64_t)Nz * 4, (cuuint64_t)Ny * Nz * 4, (cuuint64_t)Nx * Ny * Nz * 4};
+    const cuuint32_t box[4] = {8, (cuuint32_t)TJ, (cuuint32_t)TI, 4};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = reinterpret_cast<Encode>(encode_fn)(
+        reinterpret_cast<CUtensorMap *>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float *>(X), dims, strides,
+        box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }

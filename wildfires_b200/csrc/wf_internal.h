@@ -128,6 +128,10 @@ struct StageArgs {
     // FP32: host copies of the TMA tensor maps (CUtensorMap) of X for the tile
     // boxes of 16-column and 8-column tiles, or nullptr (tiles loaded by cp.async)
     const void *tmap[2];
+    // FP32: host copies of the tensor maps of yn and acc for the boxes of the tile's
+    // own cells (16- and 8-column tiles), or nullptr: the stage kernel prefetches
+    // its RK operands into L2 with them while it loads and evaluates its tile
+    const void *pmap_yn[2], *pmap_acc[2];
     int *kerr;             // set by a stage kernel whose bounded wait for its tile gave up
 };
 
@@ -154,6 +158,8 @@ int stage_tile_planes(int precision);   // z planes of a fused-stage tile
 // 64-byte swizzle); false when the grid cannot be described (column length not a
 // multiple of 4) or the driver call fails.  encode_fn: cuTensorMapEncodeTiled.
 bool stage_tensor_map(void *out, const float *X, int Nx, int Ny, int Nz, int TI, int TJ, void *encode_fn);
+// map of the same buffer for boxes of a tile's own cells (8 planes x TJ x TI x 4 fields)
+bool stage_cell_map(void *out, const float *X, int Nx, int Ny, int Nz, int TI, int TJ, void *encode_fn);
 // Tile shapes compiled for the fused pass (all with the same z planes, so the
 // boundary-column list does not depend on the choice): count and TI x TJ.
 int stage_tile_count(int precision);
