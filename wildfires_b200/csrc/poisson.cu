@@ -244,6 +244,7 @@ template <int L, int RB>
 struct EngS {
     using SH = fft::Shape<L, kRad<L, RB>>;
     static constexpr bool kPR = false;
+    static constexpr int kMinBlocks = kFftMinBlocks;
     static constexpr int kL = L;
     static constexpr int LB = SH::LB, LS = SH::LS;
     static constexpr size_t smem_bytes = SH::smem_bytes;
@@ -259,6 +260,10 @@ struct EngS {
 template <class Plan>
 struct EngPR {
     static constexpr bool kPR = true;
+    // y kernels: three blocks per SM (80 registers, a few hundred bytes spilled)
+    // measured faster than two at 128 registers (source 0.465 -> 0.396 ms,
+    // inverse 0.268 -> 0.246 ms at 512x512x128); the x kernel keeps two
+    static constexpr int kMinBlocks = 3;
     static constexpr int LB = Plan::LB, LS = Plan::LS;
     static constexpr size_t smem_bytes = Plan::smem_bytes;
     __device__ __forceinline__ static int line(int tid) { return tid >> 5; }
@@ -277,7 +282,7 @@ struct EngPR {
 // The pair group is the fast grid index, so the blocks resident at one time
 // read whole z-columns of the same x-plane of the state.
 template <class E, class R>
-__global__ void __launch_bounds__(256, kFftMinBlocks) k_p_rhs_ffty(const PoissonArgs<R> a)
+__global__ void __launch_bounds__(256, E::kMinBlocks) k_p_rhs_ffty(const PoissonArgs<R> a)
 {
     constexpr int LB = E::LB, LS = E::LS;
     extern __shared__ double2 smem[];
@@ -539,7 +544,7 @@ __global__ void __launch_bounds__(128, 8) k_p_tridiag(double2 *__restrict__ G, c
 // P5: inverse FFT in y of packed slice pairs, normalisation, write p and the
 // periodic duplicate planes (pressure.cu:392-416, deterministic here).
 template <class E, class R>
-__global__ void __launch_bounds__(256, kFftMinBlocks) k_p_iffty_out(const PoissonArgs<R> a)
+__global__ void __launch_bounds__(256, E::kMinBlocks) k_p_iffty_out(const PoissonArgs<R> a)
 {
     constexpr int LB = E::LB, LS = E::LS;
     extern __shared__ double2 smem[];
