@@ -4,8 +4,9 @@
 // power-of-two FFT reaches only through Bluestein's chirp-z identity (two
 // FFTs of 1024 points per line).
 //
-// Plan: N1 odd (1 allowed), P an odd prime not dividing N1, P - 1 = F1 * F2
-// with F1 a power of two (2 ... 16) and F2 odd (1 allowed).
+// Plan: N1 odd (1 allowed), P an odd prime not dividing N1, P - 1 = F1 * F2 * F3
+// with F1 a power of two (2 ... 16) and F2, F3 odd and coprime (F3 = 1 allowed,
+// then F2 = 1 allowed).
 //
 //   Good-Thomas: x[(P n1 + N1 n2) mod n] -> X[k], k = k1 (mod N1), k = k2 (mod P):
 //     Y[k1][n2] = sum_n1 W_N1^(n1 k1) x[P n1 + N1 n2]       (pass A, DFT_N1)
@@ -16,25 +17,27 @@
 //   the cyclic convolution of length P - 1 taken as
 //     c = IDFT_unnorm(DFT(u) * B'),  B' = DFT(b) / (P - 1),
 //   with a[0] added to the DC term before the inverse transform.  DFT and
-//   IDFT of length P - 1 are Good-Thomas again over (F1, F2):
-//     q = (F2 q1 + F1 q2) mod (P-1) on input, j = CRT(j1 mod F1, j2 mod F2).
+//   IDFT of length Q = P - 1 are Good-Thomas again over the factors of Q,
+//   written here (F1, M, L): (F1, 1, F2) for two factors, (F1, F2, F3) for
+//   three.  Input q = (Q/F1 q1 + Q/M qM + Q/L qL) mod Q, output index by CRT.
 //
 // Passes (each unit's values in registers, one __syncwarp between passes):
-//   A   P units (one per n2):        DFT_N1, write the Rader layout
-//   B1  N1*F2 units (k1, q2):        DFT_F1 over q1, in place
-//   B2  N1*F1 units (k1, j1):        DFT_F2 over q2, * B', IDFT_F2, in place
-//   B3  N1*F2 units (k1, m2):        IDFT_F1 over j1 -> X[k1][g^-m], post
+//   A   P units (one per n2):            DFT_N1, write the Rader layout
+//   B1  N1*M*L units (k1, qM, qL):       DFT_F1 over q1, in place
+//   B2a N1*F1*L units (k1, j1, qL):      DFT_M over qM, in place (M > 1)
+//   B2  N1*F1*M units (k1, j1, jM):      DFT_L over qL, * B', IDFT_L, in place
+//   B2b N1*F1*L units (k1, j1, mL):      IDFT_M over jM, in place (M > 1)
+//   B3  N1*M*L units (k1, mM, mL):       IDFT_F1 over j1 -> X[k1][g^-m], post
 //
 // Rader layout of sub-line k1 (stride SS): slot 0 holds a[0] (then X[k1][0]),
-// slot 1 + F2 q1 + q2 holds u at q = (F2 q1 + F1 q2) mod (P-1).  Within B1 and
-// B3 a warp's consecutive lanes read consecutive slots; in B2 they read slots
-// F2 apart (F2 odd); SS = F2 (mod 8) keeps the sub-line boundaries conflict
-// free too.
+// slot 1 + (q1 M + qM) L + qL holds u at q.  Within B1, B2a, B2b and B3 a
+// warp's consecutive lanes read consecutive slots; in B2 they read slots L apart
+// (L odd); SS = M L (mod 8) keeps the sub-line boundaries conflict free too.
 //
-// Tables (device, per length): rb[j1 F2 + j2] = B'[CRT(j1, j2)];
-// map[u] = n2 held by Rader slot u (u < P); map[P + m1 F2 + m2] =
-// (e2 * g^-m) mod n, m = (F2 m1 + F1 m2) mod (P-1), e2 = N1 (N1^-1 mod P); and
-// e1 = P (P^-1 mod N1) mod n, the CRT weight of k1.
+// Tables (device, per length): rb[(j1 M + jM) L + jL] = B'[CRT(j1, jM, jL)];
+// map[u] = n2 held by Rader slot u (u < P); map[P + (m1 M + mM) L + mL] =
+// (e2 * g^-m) mod n, m the output index of (m1, mM, mL), e2 = N1 (N1^-1 mod P);
+// and e1 = P (P^-1 mod N1) mod n, the CRT weight of k1.
 //
 // Trigonometric constants of the odd DFTs are compile-time values of a Taylor
 // series about pi/2 (16 terms, |phi| <= pi/2: error a few units in the last
@@ -153,25 +156,30 @@ struct PrTables {
     int e1;
 };
 
-template <int N1_, int P_, int F1_, int F2_>
+template <int N1_, int P_, int F1_, int F2_, int F3_ = 1>
 struct PrPlan {
-    static constexpr int N1 = N1_, P = P_, F1 = F1_, F2 = F2_;
+    static constexpr int N1 = N1_, P = P_, F1 = F1_, F2 = F2_, F3 = F3_;
     static constexpr int n = N1 * P;
-    static_assert(N1 % 2 == 1 && P % 2 == 1 && F2 % 2 == 1, "odd factors");
+    static constexpr int M = (F3 > 1) ? F2 : 1, L = (F3 > 1) ? F3 : F2;   // middle, innermost factor
+    static_assert(N1 % 2 == 1 && P % 2 == 1 && F2 % 2 == 1 && F3 % 2 == 1, "odd factors");
     static_assert(F1 == 2 || F1 == 4 || F1 == 8 || F1 == 16, "power-of-two factor");
-    static_assert(F1 * F2 == P - 1, "Rader length");
+    static_assert(F1 * F2 * F3 == P - 1, "Rader length");
     static_assert(N1 == 1 || N1 % P != 0, "coprime factors");
-    // sub-line stride: >= P, = F2 (mod 8)
-    static constexpr int SS = P + (((F2 - P) % 8) + 8) % 8;
+    static constexpr int gcd(int a, int b) { return b == 0 ? a : gcd(b, a % b); }
+    static_assert(F3 == 1 || (F2 > 1 && gcd(F2, F3) == 1), "coprime odd factors");
+    // sub-line stride: >= P, = M L (mod 8)
+    static constexpr int SS = P + (((M * L - P) % 8) + 8) % 8;
     static constexpr int LB = 8;                              // lines (warps) per 256-thread block
     static constexpr int LS0 = (n > N1 * SS) ? n : N1 * SS;
     static constexpr int LS = LS0 + ((1 - LS0 % 8) + 8) % 8;   // line stride = 1 (mod 8)
     static constexpr size_t smem_bytes = (size_t)LB * LS * 16;
     static constexpr int RA = (P + 31) / 32;                  // rounds of pass A
-    static constexpr int UB = N1 * F2;                        // units of B1 and B3
+    static constexpr int UB = N1 * M * L;                     // units of B1 and B3
     static constexpr int RB = (UB + 31) / 32;
-    static constexpr int UC = N1 * F1;                        // units of B2
+    static constexpr int UC = N1 * F1 * M;                    // units of B2
     static constexpr int RC = (UC + 31) / 32;
+    static constexpr int UD = N1 * F1 * L;                    // units of B2a, B2b
+    static constexpr int RD = (UD + 31) / 32;
 
     // Forward DFT (INV: exp(+2 pi i jk/n), unnormalised) of the line at buf,
     // by the 32 lanes of one warp.  pre(idx) supplies x[idx] (idx < n) and is
@@ -209,51 +217,87 @@ struct PrPlan {
             }
             __syncwarp();
         }
-        // pass B1: DFT_F1 over q1
+        // pass B1: DFT_F1 over q1 (slot stride M L)
 #pragma unroll
         for (int r = 0; r < RB; r++) {
             const int u = lane + 32 * r;
             if (u < UB) {
-                const int k1 = u / F2, q2 = u - k1 * F2;
-                double2 *b = buf + k1 * SS + 1 + q2;
+                const int k1 = u / (M * L), w = u - k1 * (M * L);
+                double2 *b = buf + k1 * SS + 1 + w;
                 double2 v[F1];
 #pragma unroll
-                for (int q1 = 0; q1 < F1; q1++) v[q1] = b[F2 * q1];
+                for (int q1 = 0; q1 < F1; q1++) v[q1] = b[M * L * q1];
                 dft_pow2<F1>(v);
 #pragma unroll
-                for (int j1 = 0; j1 < F1; j1++) b[F2 * j1] = v[j1];
+                for (int j1 = 0; j1 < F1; j1++) b[M * L * j1] = v[j1];
             }
         }
         __syncwarp();
-        // pass B2: DFT_F2 over q2, pointwise product with B', IDFT_F2
+        // pass B2a: DFT_M over qM (slot stride L)
+        if constexpr (M > 1) {
+#pragma unroll
+            for (int r = 0; r < RD; r++) {
+                const int u = lane + 32 * r;
+                if (u < UD) {
+                    const int k1 = u / (F1 * L), w = u - k1 * (F1 * L), j1 = w / L, qL = w - j1 * L;
+                    double2 *b = buf + k1 * SS + 1 + j1 * M * L + qL;
+                    double2 v[M];
+#pragma unroll
+                    for (int q = 0; q < M; q++) v[q] = b[L * q];
+                    dft_odd<M>(v);
+#pragma unroll
+                    for (int q = 0; q < M; q++) b[L * q] = v[q];
+                }
+            }
+            __syncwarp();
+        }
+        // pass B2: DFT_L over qL, pointwise product with B', IDFT_L
 #pragma unroll
         for (int r = 0; r < RC; r++) {
             const int u = lane + 32 * r;
             if (u < UC) {
-                const int k1 = u / F1, j1 = u - k1 * F1;
-                double2 *b = buf + k1 * SS + 1 + F2 * j1;
-                double2 v[F2];
+                const int k1 = u / (F1 * M), jj = u - k1 * (F1 * M);   // jj = j1 M + jM
+                double2 *b = buf + k1 * SS + 1 + L * jj;
+                double2 v[L];
 #pragma unroll
-                for (int q2 = 0; q2 < F2; q2++) v[q2] = b[q2];
-                dft_odd<F2>(v);
+                for (int q = 0; q < L; q++) v[q] = b[q];
+                dft_odd<L>(v);
                 double2 a0 = make_double2(0.0, 0.0);
-                if (j1 == 0) {
+                if (jj == 0) {
                     a0 = buf[k1 * SS];
                     buf[k1 * SS] = cadd(a0, v[0]);   // X[k1][0]
                 }
-                const double2 *w = t.rb + j1 * F2;
+                const double2 *w = t.rb + L * jj;
 #pragma unroll
-                for (int j2 = 0; j2 < F2; j2++) v[j2] = cmul(v[j2], __ldg(w + j2));
+                for (int q = 0; q < L; q++) v[q] = cmul(v[q], __ldg(w + q));
                 v[0] = cadd(v[0], a0);
                 // IDFT = conj(DFT(conj(.)))
 #pragma unroll
-                for (int j2 = 0; j2 < F2; j2++) v[j2].y = -v[j2].y;
-                dft_odd<F2>(v);
+                for (int q = 0; q < L; q++) v[q].y = -v[q].y;
+                dft_odd<L>(v);
 #pragma unroll
-                for (int m2 = 0; m2 < F2; m2++) b[m2] = make_double2(v[m2].x, -v[m2].y);
+                for (int q = 0; q < L; q++) b[q] = make_double2(v[q].x, -v[q].y);
             }
         }
         __syncwarp();
+        // pass B2b: IDFT_M over jM
+        if constexpr (M > 1) {
+#pragma unroll
+            for (int r = 0; r < RD; r++) {
+                const int u = lane + 32 * r;
+                if (u < UD) {
+                    const int k1 = u / (F1 * L), w = u - k1 * (F1 * L), j1 = w / L, mL = w - j1 * L;
+                    double2 *b = buf + k1 * SS + 1 + j1 * M * L + mL;
+                    double2 v[M];
+#pragma unroll
+                    for (int q = 0; q < M; q++) v[q] = make_double2(b[L * q].x, -b[L * q].y);
+                    dft_odd<M>(v);
+#pragma unroll
+                    for (int q = 0; q < M; q++) b[L * q] = make_double2(v[q].x, -v[q].y);
+                }
+            }
+            __syncwarp();
+        }
         // pass B3: IDFT_F1 over j1, outputs
         {
             double2 v[RB][F1], x0[RB];
@@ -261,11 +305,11 @@ struct PrPlan {
             for (int r = 0; r < RB; r++) {
                 const int u = lane + 32 * r;
                 if (u < UB) {
-                    const int k1 = u / F2, m2 = u - k1 * F2;
-                    const double2 *b = buf + k1 * SS + 1 + m2;
+                    const int k1 = u / (M * L), w = u - k1 * (M * L);
+                    const double2 *b = buf + k1 * SS + 1 + w;
 #pragma unroll
-                    for (int j1 = 0; j1 < F1; j1++) v[r][j1] = b[F2 * j1];
-                    if (m2 == 0) x0[r] = buf[k1 * SS];
+                    for (int j1 = 0; j1 < F1; j1++) v[r][j1] = b[M * L * j1];
+                    if (w == 0) x0[r] = buf[k1 * SS];
                 }
             }
             __syncwarp();
@@ -273,21 +317,21 @@ struct PrPlan {
             for (int r = 0; r < RB; r++) {
                 const int u = lane + 32 * r;
                 if (u < UB) {
-                    const int k1 = u / F2, m2 = u - k1 * F2;
+                    const int k1 = u / (M * L), w = u - k1 * (M * L);
                     const int kb = (k1 * t.e1) % n;
 #pragma unroll
                     for (int j1 = 0; j1 < F1; j1++) v[r][j1].y = -v[r][j1].y;
                     dft_pow2<F1>(v[r]);
-                    const int *km = t.map + P + m2;
+                    const int *km = t.map + P + w;
 #pragma unroll
                     for (int m1 = 0; m1 < F1; m1++) {
-                        int idx = kb + __ldg(km + F2 * m1);
+                        int idx = kb + __ldg(km + M * L * m1);
                         if (idx >= n) idx -= n;
                         // conj of the IDFT trick, and of the inverse transform
                         const double2 x = v[r][m1];
                         post(idx, INV ? x : make_double2(x.x, -x.y));
                     }
-                    if (m2 == 0) {
+                    if (w == 0) {
                         const double2 x = x0[r];
                         post(kb, INV ? make_double2(x.x, -x.y) : x);
                     }

@@ -630,13 +630,12 @@ __global__ void __launch_bounds__(256, E::kMinBlocks) k_p_iffty_out(const Poisso
 // ---- launch: one kernel instantiation per line engine ----------------------
 constexpr int kMinL = 2, kMaxL = 12;
 
-// Prime-factor + Rader plans compiled in: n = N1 * P, P - 1 = F1 * F2.  The
-// x and y lengths of the workloads: 511 (512-point grids), 255 (256), 159
-// (160) and 95 (96); 127 and 191 are prime with P - 1 = 2 * 63 and 2 * 95,
-// beyond these two-factor plans, and stay on Bluestein.
+// Prime-factor + Rader plans compiled in: n = N1 * P, P - 1 = F1 * F2 * F3.
+// The x and y lengths of the workloads: 511 (512-point grids), 255 (256), 191
+// (192), 159 (160), 127 (128) and 95 (96).
 template <class... Pl> struct PlanList {};
-using PrPlans = PlanList<fft::PrPlan<7, 73, 8, 9>, fft::PrPlan<15, 17, 16, 1>, fft::PrPlan<3, 53, 4, 13>,
-                         fft::PrPlan<5, 19, 2, 9>>;
+using PrPlans = PlanList<fft::PrPlan<7, 73, 8, 9>, fft::PrPlan<15, 17, 16, 1>, fft::PrPlan<1, 191, 2, 5, 19>,
+                         fft::PrPlan<3, 53, 4, 13>, fft::PrPlan<1, 127, 2, 7, 9>, fft::PrPlan<5, 19, 2, 9>>;
 
 template <class Op, class... Pl, class... A>
 cudaError_t by_plan(PlanList<Pl...>, int n, A &...args)
@@ -745,14 +744,15 @@ cudaError_t set_pr_attributes_all(PlanList<Pl...>)
     return e;
 }
 template <class... Pl>
-bool pr_plan_of(PlanList<Pl...>, int n, int f[4])
+bool pr_plan_of(PlanList<Pl...>, int n, int f[5])
 {
-    return ((n == Pl::n ? (f[0] = Pl::N1, f[1] = Pl::P, f[2] = Pl::F1, f[3] = Pl::F2, true) : false) || ...);
+    return ((n == Pl::n ? (f[0] = Pl::N1, f[1] = Pl::P, f[2] = Pl::F1, f[3] = Pl::F2, f[4] = Pl::F3, true) : false) ||
+            ...);
 }
 
 }  // namespace
 
-bool poisson_pr_plan(int n, int f[4]) { return pr_plan_of(PrPlans{}, n, f); }
+bool poisson_pr_plan(int n, int f[5]) { return pr_plan_of(PrPlans{}, n, f); }
 
 template <class R> cudaError_t poisson_set_attributes()
 {

@@ -82,42 +82,49 @@ int primitive_root(int P)
     return 0;
 }
 
-// Tables of the prime-factor + Rader engine for n = N1 P, P - 1 = F1 F2
-// (layout in fft_pr.cuh); the filter in long double (setup only).
-void plan_pr(HostFft &h, const int f[4])
+// Tables of the prime-factor + Rader engine for n = N1 P, P - 1 = F1 F2 F3
+// (layout in fft_pr.cuh, with the factors of P - 1 as (F1, M, L): (F1, 1, F2)
+// for two, (F1, F2, F3) for three); the filter in long double (setup only).
+void plan_pr(HostFft &h, const int f[5])
 {
-    const int n = h.d.n, N1 = f[0], P = f[1], F1 = f[2], F2 = f[3], Q = P - 1;
+    const int n = h.d.n, N1 = f[0], P = f[1], F1 = f[2], Q = P - 1;
+    const int M = (f[4] > 1) ? f[3] : 1, L = (f[4] > 1) ? f[4] : f[3];
     const int g = primitive_root(P), gi = (int)pow_mod(g, P - 2, P);
     const int e2 = (int)((long long)N1 * inv_mod(N1 % P, P) % n);
     h.d.pr_e1 = (N1 > 1) ? (int)((long long)P * inv_mod(P % N1, N1) % n) : 0;
     h.prmap.assign(P + Q, 0);
     for (int q1 = 0; q1 < F1; q1++)
-        for (int q2 = 0; q2 < F2; q2++) {
-            const int q = (F2 * q1 + F1 * q2) % Q;
-            h.prmap[1 + F2 * q1 + q2] = (int)pow_mod(g, q, P);
-            h.prmap[P + F2 * q1 + q2] = (int)((long long)e2 * pow_mod(gi, q, P) % n);
-        }
-    // B'[j] = (1/Q) sum_t exp(-2 pi i gi^t / P) exp(-2 pi i j t / Q)
+        for (int qm = 0; qm < M; qm++)
+            for (int ql = 0; ql < L; ql++) {
+                const int q = (int)(((long long)(Q / F1) * q1 + (long long)(Q / M) * qm + (long long)(Q / L) * ql) % Q);
+                const int slot = (q1 * M + qm) * L + ql;
+                h.prmap[1 + slot] = (int)pow_mod(g, q, P);
+                h.prmap[P + slot] = (int)((long long)e2 * pow_mod(gi, q, P) % n);
+            }
+    // B'[j] = (1/Q) sum_t exp(-2 pi i gi^t / P) exp(-2 pi i j t / Q), stored at
+    // (j1, jM, jL) with j = CRT(j1 mod F1, jM mod M, jL mod L)
     std::vector<long double> br(Q), bi(Q);
     for (int t = 0; t < Q; t++) {
         const long double a = -2.0L * kPiL * (long double)pow_mod(gi, t, P) / (long double)P;
         br[t] = cosl(a);
         bi[t] = sinl(a);
     }
-    const int c1 = F2 * inv_mod(F2 % F1, F1), c2 = (F2 > 1) ? F1 * inv_mod(F1 % F2, F2) : 0;
+    auto crt_weight = [&](int F) { return F > 1 ? (Q / F) * inv_mod((Q / F) % F, F) : 0; };
+    const int c1 = crt_weight(F1), cm = crt_weight(M), cl = crt_weight(L);
     h.prb.resize(Q);
     for (int j1 = 0; j1 < F1; j1++)
-        for (int j2 = 0; j2 < F2; j2++) {
-            const int j = (j1 * c1 + j2 * c2) % Q;
-            long double sr = 0, si = 0;
-            for (int t = 0; t < Q; t++) {
-                const long double a = -2.0L * kPiL * (long double)(((long long)j * t) % Q) / (long double)Q;
-                const long double c = cosl(a), sn = sinl(a);
-                sr += br[t] * c - bi[t] * sn;
-                si += br[t] * sn + bi[t] * c;
+        for (int jm = 0; jm < M; jm++)
+            for (int jl = 0; jl < L; jl++) {
+                const int j = (int)(((long long)j1 * c1 + (long long)jm * cm + (long long)jl * cl) % Q);
+                long double sr = 0, si = 0;
+                for (int t = 0; t < Q; t++) {
+                    const long double a = -2.0L * kPiL * (long double)(((long long)j * t) % Q) / (long double)Q;
+                    const long double c = cosl(a), sn = sinl(a);
+                    sr += br[t] * c - bi[t] * sn;
+                    si += br[t] * sn + bi[t] * c;
+                }
+                h.prb[(j1 * M + jm) * L + jl] = make_double2((double)(sr / Q), (double)(si / Q));
             }
-            h.prb[j1 * F2 + j2] = make_double2((double)(sr / Q), (double)(si / Q));
-        }
     h.d.pr = 1;
 }
 
@@ -128,7 +135,7 @@ HostFft plan_fft(int n)
     h.d.n = n;
     // WF_FFT_RADER=0 keeps such lengths on Bluestein (for comparisons)
     const char *rader = getenv("WF_FFT_RADER");
-    int f[4];
+    int f[5];
     if (!(rader && rader[0] == '0') && poisson_pr_plan(n, f)) {
         plan_pr(h, f);
         return h;

@@ -200,9 +200,9 @@ struct FftDesc {
     const int *prmap;       // Rader: input slot map [P] and output index map [P-1]
     int pr_e1;              // Rader: CRT weight of the N1 residue
 };
-// Prime-factor + Rader plan compiled for length n: f = {N1, P, F1, F2} with
-// n = N1 P, P prime, P - 1 = F1 F2.  False for every other length.
-bool poisson_pr_plan(int n, int f[4]);
+// Prime-factor + Rader plan compiled for length n: f = {N1, P, F1, F2, F3} with
+// n = N1 P, P prime, P - 1 = F1 F2 F3.  False for every other length.
+bool poisson_pr_plan(int n, int f[5]);
 
 template <class R>
 struct PoissonArgs {
