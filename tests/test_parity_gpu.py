@@ -203,6 +203,25 @@ def test_pressure_fft_lengths_match_oracle(nx, ny, params_from_text):
     assert np.max(np.abs(p - po)) <= 1e-11 * scale
 
 
+@pytest.mark.parametrize("nx,ny", [(512, 128), (192, 96), (256, 160)])
+def test_rader_and_bluestein_engines_agree(nx, ny, params_from_text, monkeypatch):
+    """The prime-factor + Rader transforms (511 = 7 x 73, 127 and 191 with a
+    three-factor inner transform, 255, 159, 95) against the same lengths by
+    Bluestein (WF_FFT_RADER=0) through the pressure solve: the two engines
+    round differently, so they agree to rounding, not bit for bit."""
+    from wildfires_b200 import configs
+    case = configs.flat(Nx=nx, Ny=ny, Nz=8, Nt=1, jitter=0.3, seed=nx * ny)
+    P = params_from_text(configs.param_text(case.params))
+    y0, p0 = case.fields(P)
+    with _solver(P) as s:
+        p_pr, _ = s.pressure(y0, y0, p0)
+    monkeypatch.setenv("WF_FFT_RADER", "0")
+    with _solver(P) as s:
+        p_bl, _ = s.pressure(y0, y0, p0)
+    scale = np.max(np.abs(p_bl))
+    assert np.max(np.abs(p_pr - p_bl)) <= 1e-12 * scale
+
+
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-11), ("fp32", 1e-5)])
 def test_tallest_column_one_step_matches_oracle(prec, tol, params_from_text):
     """The longest tridiagonal system wf_create accepts (Nz - 1 = 511) and the
