@@ -243,9 +243,7 @@ __device__ __forceinline__ void line_dft(const FftDesc &d, double2 *buf, int jj,
 template <int L, int RB>
 struct EngS {
     using SH = fft::Shape<L, kRad<L, RB>>;
-    static constexpr bool kPR = false;
     static constexpr int kMinBlocks = kFftMinBlocks;
-    static constexpr int kL = L;
     static constexpr int LB = SH::LB, LS = SH::LS;
     static constexpr size_t smem_bytes = SH::smem_bytes;
     __device__ __forceinline__ static int line(int tid) { return tid % LB; }
@@ -259,7 +257,6 @@ struct EngS {
 };
 template <class Plan>
 struct EngPR {
-    static constexpr bool kPR = true;
     // y kernels: three blocks per SM (80 registers, a few hundred bytes spilled)
     // measured faster than two at 128 registers (source 0.465 -> 0.396 ms,
     // inverse 0.268 -> 0.246 ms at 512x512x128); the x kernel keeps two
@@ -275,6 +272,12 @@ struct EngPR {
         Plan::template run<INV>(fft::PrTables{d.prb, d.prmap, d.pr_e1}, buf, jj, pre, post);
     }
 };
+
+// which engine a kernel instantiation got, and the power-of-two engine's log2 length
+template <class E> constexpr bool kIsPR = false;
+template <class Plan> constexpr bool kIsPR<EngPR<Plan>> = true;
+template <class E> constexpr int kLog2 = 0;
+template <int L, int RB> constexpr int kLog2<EngS<L, RB>> = L;
 
 // P1: source + top plane, forward FFT in y of packed slice pairs.  Block
 // (pair group, i): LB complex lines, line q packs slices 2(pair0+q) (real
@@ -691,10 +694,10 @@ struct LaunchFx {
     template <class E> static cudaError_t go(double2 *const &G, const FftDesc &fx, const int &nslices, const int &n0,
                                            const int &h1, cudaStream_t &s)
     {
-        if constexpr (E::kPR) {
+        if constexpr (kIsPR<E>) {
             k_p_fftx_pr<E, INV><<<dim3((h1 + E::LB - 1) / E::LB, nslices), 256, E::smem_bytes, s>>>(G, fx, n0, h1);
         } else {
-            constexpr int L = E::kL;
+            constexpr int L = kLog2<E>;
             const int nitems = nslices * ((h1 + E::LB - 1) / E::LB);
             const int blocks = min(nitems, kFftMinBlocks * g_poisson_sms);
             k_p_fftx<L, INV><<<blocks, 256, 2 * E::smem_bytes, s>>>(G, fx, n0, h1, nslices);
