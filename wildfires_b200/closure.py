@@ -129,7 +129,7 @@ def targets(uf, vf, wf, dxc, dyc, zc):
 
 
 # ---- cases ----------------------------------------------------------------------
-def study_case(Nc=(33, 33, 9), fine=False, seed=0, Nt=120, dt=0.002, L=100.0, H=20.0, gust=1.0, Y_h=0.1):
+def study_case(Nc=(33, 33, 9), fine=False, seed=0, Nt=120, dt=0.002, L=100.0, H=20.0, gust=1.0, Y_h=0.1, **kw):
     """The closure study family: flat terrain, log wind with seeded velocity
     fluctuations (`gust` m/s, on the fine grid's scale so that the coarse grid
     does not resolve them), one hot spot; the fine grid has 4x the intervals
@@ -142,7 +142,7 @@ def study_case(Nc=(33, 33, 9), fine=False, seed=0, Nt=120, dt=0.002, L=100.0, H=
     from . import configs
     N = tuple(FACTOR * (n - 1) + 1 for n in Nc) if fine else Nc
     rng = np.random.default_rng(seed)
-    params = configs.base_params(N[0], N[1], N[2], Nt, L, L, H, Nt * dt, Y_h=Y_h)
+    params = configs.base_params(N[0], N[1], N[2], Nt, L, L, H, Nt * dt, Y_h=Y_h, **kw)
     u_r = rng.uniform(3, 6)
     xc, yc = rng.uniform(0.2, 0.4) * L, rng.uniform(0.35, 0.65) * L
 
@@ -163,7 +163,7 @@ def study_case(Nc=(33, 33, 9), fine=False, seed=0, Nt=120, dt=0.002, L=100.0, H=
     def fields(P):
         if fine:
             return configs._finish(P, *fine_fields(P), None, 0.0)
-        Pf, _, _ = configs.materialize(study_case(Nc, True, seed, Nt, dt, L, H, gust, Y_h))
+        Pf, _, _ = configs.materialize(study_case(Nc, True, seed, Nt, dt, L, H, gust, Y_h, **kw))
         u, v, w, T, Y = (box_filter(q) for q in fine_fields(Pf))
         return configs._finish(P, u, v, w, T, np.ones_like(u), None, 0.0)
 
