@@ -140,6 +140,16 @@ wf_status wf_destroy(wf_ctx *ctx);
 
 /* Upload a packed FP64 host state and p (the time level becomes 0). */
 wf_status wf_upload_state(wf_ctx *ctx, const double *y, const double *pr);
+
+/* The same upload, returning once the state is on the device while p's copy
+ * continues on a stream of its own: the next wf_step waits for it only before
+ * its pressure solve (which reads p's top plane), so the copy overlaps the RK
+ * stages; every other call that reads or writes p (download, dumps, pressure
+ * operators, wf_device_state, wf_synchronize) first waits for it.  The host
+ * buffer pr must stay unchanged until the following step has completed or one
+ * of those calls has returned.  Counterpart of the reference's host-to-device
+ * copies before solve_PDE (main.cu:71-72), which block. */
+wf_status wf_upload_state_async(wf_ctx *ctx, const double *y, const double *pr);
 /* Download the current packed state and p as FP64. */
 wf_status wf_download_state(wf_ctx *ctx, double *y, double *pr);
 

@@ -152,6 +152,7 @@ def test_every_entry_point_rejects_null_arguments():
         "wf_create": ((None, 0, None), ARG),
         "wf_destroy": ((None,), 0),
         "wf_upload_state": ((None, None, None), ARG),
+        "wf_upload_state_async": ((None, None, None), ARG),
         "wf_download_state": ((None, None, None), ARG),
         "wf_step": ((None, 1), ARG),
         "wf_synchronize": ((None,), ARG),

@@ -203,6 +203,37 @@ def test_pressure_fft_lengths_match_oracle(nx, ny, params_from_text):
     assert np.max(np.abs(p - po)) <= 1e-11 * scale
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_async_upload_steps_like_the_blocking_one(prec, params_from_text):
+    """wf_upload_state_async (p's copy overlapping the RK stages) followed by
+    steps and a download gives the same bits as wf_upload_state, also when the
+    host buffer of p is overwritten right after the download and uploaded
+    again (the step must have waited for the first copy)."""
+    import ctypes as C
+    from wildfires_b200 import configs
+    from wildfires_b200._abi import check, lib
+    case = configs.hill(Nx=65, Ny=65, Nz=32, Nt=4, L=120.0, H=20.0, jitter=0.1, seed=3)
+    P = params_from_text(configs.param_text(case.params))
+    y0, p0 = case.fields(P)
+    import torch
+    dp = C.POINTER(C.c_double)
+    out = {}
+    for name in ("wf_upload_state", "wf_upload_state_async"):
+        with _solver(P, prec) as s:
+            # pinned host buffers: the copies are truly asynchronous
+            y = torch.empty(len(y0), dtype=torch.float64, pin_memory=True).numpy()
+            p = torch.empty(len(p0), dtype=torch.float64, pin_memory=True).numpy()
+            y[:] = y0
+            p[:] = p0
+            for _ in range(2):
+                check(getattr(lib(), name)(s._h, y.ctypes.data_as(dp), p.ctypes.data_as(dp)), name)
+                s.step(2)
+                check(lib().wf_download_state(s._h, y.ctypes.data_as(dp), p.ctypes.data_as(dp)), "download")
+            out[name] = (y.copy(), p.copy())
+    assert np.array_equal(out["wf_upload_state"][0], out["wf_upload_state_async"][0])
+    assert np.array_equal(out["wf_upload_state"][1], out["wf_upload_state_async"][1])
+
+
 @pytest.mark.parametrize("nx,ny", [(512, 128), (192, 96), (256, 160)])
 def test_rader_and_bluestein_engines_agree(nx, ny, params_from_text, monkeypatch):
     """The prime-factor + Rader transforms (511 = 7 x 73, 127 and 191 with a

@@ -18,7 +18,7 @@ WF_NPHASES = 9
 #: every symbol include/wildfires_b200.h declares
 EXPORTS = [
     "wf_read_parameters", "wf_free_parameters", "wf_set_topography", "wf_state_size",
-    "wf_load_fields", "wf_save_fields", "wf_create", "wf_destroy", "wf_upload_state",
+    "wf_load_fields", "wf_save_fields", "wf_create", "wf_destroy", "wf_upload_state", "wf_upload_state_async",
     "wf_download_state", "wf_step", "wf_synchronize", "wf_time", "wf_diagnostics",
     "wf_device_state", "wf_stream", "wf_phi", "wf_pressure", "wf_launches_per_step",
     "wf_status_string", "wf_last_error", "wf_profile_phases", "wf_phase_name",
@@ -86,6 +86,7 @@ def lib():
         "wf_create": (C.c_int, [P, C.c_int, C.POINTER(vp)]),
         "wf_destroy": (C.c_int, [vp]),
         "wf_upload_state": (C.c_int, [vp, dp, dp]),
+        "wf_upload_state_async": (C.c_int, [vp, dp, dp]),
         "wf_download_state": (C.c_int, [vp, dp, dp]),
         "wf_step": (C.c_int, [vp, C.c_int]),
         "wf_synchronize": (C.c_int, [vp]),

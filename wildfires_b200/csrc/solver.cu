@@ -257,6 +257,12 @@ struct wf_ctx {
     int tile = 0;                   // tile shape of the fused stage pass (index)
     bool tile_set = false;          // chosen by the tuner, WF_STAGE_TILE or wf_set_stage_tile
     int *d_kerr = nullptr;          // raised by a stage kernel whose bounded tile wait gave up
+    // wf_upload_state_async: p is copied on `up` after the state's copy (event
+    // ev_y) and completes ev_p; the step waits for ev_p just before its pressure
+    // solve, every other user of p first makes the context stream wait for it
+    cudaStream_t up = nullptr;
+    cudaEvent_t ev_y = nullptr, ev_p = nullptr;
+    bool p_pending = false;
     // FP32: TMA tensor maps (CUtensorMap, 128 bytes) of the state buffers a stage
     // reads, for the boxes of 16-column (map[0]) and 8-column (map[1]) tiles
     struct TensorMaps {
@@ -275,6 +281,17 @@ namespace wfs {
 
 wf_status finish_upload(wf_ctx *c);
 wf_status tune_tiles(wf_ctx *c);
+
+// Order the context stream after a pressure copy of wf_upload_state_async that
+// may still be in flight (callers that read or write p other than the step).
+wf_status settle_p(wf_ctx *c)
+{
+    if (c->p_pending) {
+        WF_TRY_CUDA(cudaStreamWaitEvent(c->stream, c->ev_p, 0));
+        c->p_pending = false;
+    }
+    return WF_OK;
+}
 
 // Kernel launches of one step: per stage the optional closure inference,
 // k_utau, k_stage_fused and, when some column needs it, k_stage_bc; five
@@ -693,6 +710,15 @@ template <class R> wf_status enqueue_step(wf_ctx *c, int cur, int n1)
     void *yn = c->ybuf[cur], *y1 = c->ybuf[1 - cur];
     wf_status st = enqueue_stages<R>(c, yn, y1);
     if (st) return st;
+    // the pressure solve reads p's top plane: wait for an asynchronous upload of
+    // p here, so that its copy overlaps the RK stages (a wait node when captured;
+    // an event never recorded, or long complete, makes it a no-op)
+    {
+        cudaStreamCaptureStatus cs;
+        WF_TRY_CUDA(cudaStreamIsCapturing(c->stream, &cs));
+        WF_TRY_CUDA(cudaStreamWaitEvent(c->stream, c->ev_p,
+                                        cs == cudaStreamCaptureStatusActive ? cudaEventWaitExternal : 0));
+    }
     if ((st = enqueue_pressure<R>(c, y1, yn))) return st;
     ProjectArgs<R> pa;
     memset(&pa, 0, sizeof(pa));
@@ -932,7 +958,10 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
         set_error("wf_create: clearing the pressure-loop record failed");
         return fail(WF_ERR_CUDA);
     }
-    if (cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->up, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_y, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_p, cudaEventDisableTiming) != cudaSuccess) {
         set_error("wf_create: stream creation failed");
         return fail(WF_ERR_CUDA);
     }
@@ -1042,6 +1071,10 @@ wf_status wf_destroy(wf_ctx *c)
     for (auto &pl : c->ploop)
         if (pl.ge) cudaGraphExecDestroy(pl.ge);
     for (auto &b : c->bufs) cudaFree(b.p);
+    if (c->up) cudaStreamSynchronize(c->up);
+    if (c->ev_y) cudaEventDestroy(c->ev_y);
+    if (c->ev_p) cudaEventDestroy(c->ev_p);
+    if (c->up) cudaStreamDestroy(c->up);
     if (c->aux) cudaStreamDestroy(c->aux);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
@@ -1052,17 +1085,37 @@ wf_status wf_upload_state(wf_ctx *c, const double *y, const double *pr)
 {
     const NvtxRange range("wf_upload_state");
     if (!c || !y || !pr) { set_error("wf_upload_state: null argument"); return WF_ERR_ARG; }
+    wf_status st = settle_p(c);
+    if (st) return st;
     c->cur = 0;
     c->n = 0;
-    wf_status st = put_state(c, c->ybuf[0], y);
-    if (st) return st;
+    if ((st = put_state(c, c->ybuf[0], y))) return st;
     WF_TRY_CUDA(cudaMemcpyAsync(c->p, pr, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
     return finish_upload(c);
+}
+
+wf_status wf_upload_state_async(wf_ctx *c, const double *y, const double *pr)
+{
+    const NvtxRange range("wf_upload_state_async");
+    if (!c || !y || !pr) { set_error("wf_upload_state_async: null argument"); return WF_ERR_ARG; }
+    wf_status st = settle_p(c);
+    if (st) return st;
+    c->cur = 0;
+    c->n = 0;
+    if ((st = put_state(c, c->ybuf[0], y))) return st;
+    // p after the state on the host link, on its own stream
+    WF_TRY_CUDA(cudaEventRecord(c->ev_y, c->stream));
+    WF_TRY_CUDA(cudaStreamWaitEvent(c->up, c->ev_y, 0));
+    WF_TRY_CUDA(cudaMemcpyAsync(c->p, pr, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->up));
+    WF_TRY_CUDA(cudaEventRecord(c->ev_p, c->up));
+    c->p_pending = true;
+    return finish_upload(c);   // waits for the state only
 }
 
 wf_status wf_initial_conditions(wf_ctx *c)
 {
     if (!c) { set_error("wf_initial_conditions: null context"); return WF_ERR_ARG; }
+    if (const wf_status st0 = settle_p(c)) return st0;
     const Parameters &P = c->P;
     IcArgs a;
     memset(&a, 0, sizeof(a));
@@ -1183,7 +1236,9 @@ wf_status wf_download_state(wf_ctx *c, double *y, double *pr)
 {
     const NvtxRange range("wf_download_state");
     if (!c || !y || !pr) { set_error("wf_download_state: null argument"); return WF_ERR_ARG; }
-    wf_status st = get_state(c, y, c->ybuf[c->cur]);
+    wf_status st = settle_p(c);
+    if (st) return st;
+    st = get_state(c, y, c->ybuf[c->cur]);
     if (st) return st;
     WF_TRY_CUDA(cudaMemcpyAsync(pr, c->p, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
     WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
@@ -1227,6 +1282,7 @@ wf_status wf_step(wf_ctx *c, int nsteps)
             wf_status st = enqueue_step_any(c, c->cur, n1);
             if (st) return st;
         }
+        c->p_pending = false;   // the step waited for an asynchronous copy of p
         c->cur = 1 - c->cur;
         c->n = n1;
     }
@@ -1236,6 +1292,7 @@ wf_status wf_step(wf_ctx *c, int nsteps)
 wf_status wf_synchronize(wf_ctx *c)
 {
     if (!c) return WF_ERR_ARG;
+    if (const wf_status st0 = settle_p(c)) return st0;
     WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
     if (c->d_kerr) {
         int herr = 0;
@@ -1329,6 +1386,7 @@ wf_status wf_dump_async(wf_ctx *c, const char *dir, int n)
 {
     const NvtxRange range("wf_dump_async");
     if (!c || !dir) { set_error("wf_dump_async: null argument"); return WF_ERR_ARG; }
+    if (const wf_status st0 = settle_p(c)) return st0;
     if (!c->dump) c->dump = dumper_create(c->device, c->P, c->S, (size_t)c->N);
     return dumper_enqueue(c->dump, c->stream, c->ybuf[c->cur], c->prec != WF_FP64, c->p, dir, n);
 }
@@ -1369,6 +1427,7 @@ wf_status wf_diagnostics(wf_ctx *c, wf_diag *out)
 wf_status wf_device_state(wf_ctx *c, void **y, double **pr)
 {
     if (!c) return WF_ERR_ARG;
+    if (const wf_status st0 = settle_p(c)) return st0;   // work enqueued on wf_stream sees p
     if (y) *y = c->ybuf[c->cur];
     if (pr) *pr = c->p;
     return WF_OK;
@@ -1383,6 +1442,7 @@ const char *wf_phase_name(int q) { return (q >= 0 && q < WF_NPHASES) ? kPhaseNam
 wf_status wf_profile_phases(wf_ctx *c, int nsteps, double *ms, int *launches)
 {
     if (!c || !ms || !launches || nsteps < 1) { set_error("wf_profile_phases: invalid argument"); return WF_ERR_ARG; }
+    if (const wf_status st0 = settle_p(c)) return st0;
     for (int q = 0; q < WF_NPHASES; q++) { ms[q] = 0.0; launches[q] = 0; }
     const int maxev = 2 + 3 * 4 + 5 * (c->P.pressure_solver_iter > 1 ? c->P.pressure_solver_iter : 1);
     std::vector<cudaEvent_t> ev(maxev);
@@ -1438,6 +1498,7 @@ wf_status wf_pressure(wf_ctx *c, const double *y_np1, const double *y_n, double 
 {
     const NvtxRange range("wf_pressure");
     if (!c || !y_np1 || !y_n || !pr) { set_error("wf_pressure: null argument"); return WF_ERR_ARG; }
+    if (const wf_status st0 = settle_p(c)) return st0;
     void *b1 = c->ybuf[1 - c->cur], *bn = c->Xa ? c->Xa : c->ybuf[c->cur];
     wf_status st = put_state(c, b1, y_np1);
     if (st) return st;
@@ -1905,6 +1966,7 @@ wf_status wf_pressure_device(wf_ctx *c, const double *y_np1, const double *y_n, 
 {
     const NvtxRange range("wf_pressure_device");
     if (!c || !y_np1 || !y_n || !pr) { set_error("wf_pressure_device: null argument"); return WF_ERR_ARG; }
+    if (const wf_status st0 = settle_p(c)) return st0;
     void *b1 = c->ybuf[1 - c->cur], *bn = c->Xa ? c->Xa : c->ybuf[c->cur];
     wf_status st = put_state_dev(c, b1, y_np1);
     if (st) return st;
