@@ -55,9 +55,18 @@ __device__ __forceinline__ float tanh_approx(float x)
     asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
-__device__ __forceinline__ float gelu_fast(float x)
+// Two activations at once on the paired FP32 pipe (FMUL2 / FFMA2, each lane
+// rounded like the scalar form): GELU(x) = h + h tanh(z), h = x/2,
+// z = x (k + k 0.044715 x^2) -- the tanh form above with its products regrouped.
+constexpr float kGeluK3 = kGeluK * 0.044715f;
+__device__ __forceinline__ float2 gelu2(float2 x)
 {
-    return 0.5f * x * (1.0f + tanh_approx(kGeluK * (x + 0.044715f * x * x * x)));
+    const float2 a = __fmul2_rn(x, x);
+    const float2 b = __ffma2_rn(a, make_float2(kGeluK3, kGeluK3), make_float2(kGeluK, kGeluK));
+    const float2 z = __fmul2_rn(b, x);
+    const float2 t = make_float2(tanh_approx(z.x), tanh_approx(z.y));
+    const float2 h = __fmul2_rn(x, make_float2(0.5f, 0.5f));
+    return __ffma2_rn(h, t, h);
 }
 __device__ __forceinline__ float softplus(float x) { return x > 20.0f ? x : log1pf(expf(x)); }
 __device__ __forceinline__ float sigmoid(float x) { return 1.0f / (1.0f + expf(-x)); }
@@ -76,9 +85,11 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 }
 
 // The 12 raw features at cell (i, j, k) of the state X (walls: zero).
+// hz = 1 / (z[k+1] - z[k-1]) and delta = (dx dy dz_k)^(1/3) of the cell's plane
+// come from a per-plane table (plane_scales).
 template <class R>
 __device__ void cell_features(const R *__restrict__ X, const Geom &g, double dx, double dy, int i, int j, int k,
-                              float (&f)[NIN])
+                              float hz, float delta, float (&f)[NIN])
 {
     const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz;
     const size_t N = (size_t)g.N;
@@ -92,9 +103,7 @@ __device__ void cell_features(const R *__restrict__ X, const Geom &g, double dx,
     const size_t c = ((size_t)i * Ny + j) * Nz + k;
     const size_t cxp = ((size_t)ip * Ny + j) * Nz + k, cxm = ((size_t)im * Ny + j) * Nz + k;
     const size_t cyp = ((size_t)i * Ny + jp) * Nz + k, cym = ((size_t)i * Ny + jm) * Nz + k;
-    const double *z = g.z;
     const float hx = (float)(0.5 / dx), hy = (float)(0.5 / dy);
-    const float hz = (float)(1.0 / (z[k + 1] - z[k - 1]));
     float d[4][3];   // d[field][x, y, z]
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -103,7 +112,6 @@ __device__ void cell_features(const R *__restrict__ X, const Geom &g, double dx,
         d[q][1] = ((float)F[cyp] - (float)F[cym]) * hy;
         d[q][2] = ((float)F[c + 1] - (float)F[c - 1]) * hz;
     }
-    const float delta = (float)cbrt(dx * dy * g.zc[ZDZ * Nz + k]);
     const float sv = delta, st = delta * 0.01f;   // Delta / (1 m/s), Delta / (100 K)
     f[0] = d[0][0] * sv;
     f[1] = d[1][1] * sv;
@@ -137,7 +145,9 @@ constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) <
 constexpr size_t kTcA1 = 0, kTcA2 = kTcA1 + 128 * 16 * 2, kTcB1 = kTcA2 + 128 * 64 * 2, kTcB2 = kTcB1 + 64 * 16 * 2;
 constexpr size_t kTcF = kTcB2 + 64 * 64 * 2;                       // fp32: b1, b2, W3, b3, scales
 constexpr size_t kTcBar = kTcF + sizeof(float) * (64 + 64 + 64 + 4 + 12);
-constexpr size_t kSmemTc = kTcBar + 16;
+constexpr int kTcPlanes = wf::kMaxZUnknowns + 1;                    // per-plane feature scales
+constexpr size_t kTcPlane = kTcBar + 16;                           // float hz[kTcPlanes], delta[kTcPlanes]
+constexpr size_t kSmemTc = kTcPlane + sizeof(float) * 2 * kTcPlanes;
 
 // byte offset of (row, k) in a K-major no-swizzle operand with K/8 core
 // matrices per 8-row group (core matrix = 8 rows x 8 bf16 = 128 bytes)
@@ -203,7 +213,7 @@ __device__ __forceinline__ void tc_ld64(uint32_t taddr, float (&v)[64])
 }
 
 template <class R, bool FEAT>
-__global__ void __launch_bounds__(kTcThreads, 1) k_closure_coef_tc(const R *__restrict__ X, Geom g, double dx,
+__global__ void __launch_bounds__(kTcThreads, 4) k_closure_coef_tc(const R *__restrict__ X, Geom g, double dx,
                                                                    double dy, const float *__restrict__ feat, size_t nfeat,
                                                                    const float *__restrict__ theta,
                                                                    R *__restrict__ coef, int *err, int wait_limit)
@@ -232,6 +242,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_closure_coef_tc(const R *__re
     }
     if (tid == 0) sb3[0] = theta[OB3];
     if (tid < NIN) sscale[tid] = theta[NPARAM + tid];
+    float *shz = reinterpret_cast<float *>(smem + kTcPlane), *sdel = shz + kTcPlanes;
+    if (!FEAT) {
+        // per-plane feature scales: 1 / (z[k+1] - z[k-1]) and (dx dy dz_k)^(1/3)
+        for (int k = tid; k < g.Nz && k < kTcPlanes; k += kTcThreads) {
+            shz[k] = (k > 0 && k < g.Nz - 1) ? (float)(1.0 / (g.z[k + 1] - g.z[k - 1])) : 0.0f;
+            sdel[k] = (float)cbrt(dx * dy * g.zc[ZDZ * g.Nz + k]);
+        }
+    }
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -260,7 +278,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_closure_coef_tc(const R *__re
             for (int q = 0; q < NIN; q++) f[q] = feat[cell * NIN + q];
         } else if (cell < N) {
             const int k = (int)(cell % g.Nz), j = (int)((cell / g.Nz) % g.Ny), i = (int)(cell / ((size_t)g.Nz * g.Ny));
-            cell_features(X, g, dx, dy, i, j, k, f);
+            cell_features(X, g, dx, dy, i, j, k, shz[k], sdel[k], f);
         } else {
 #pragma unroll
             for (int q = 0; q < NIN; q++) f[q] = 0.0f;
@@ -293,14 +311,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_closure_coef_tc(const R *__re
         float acc[64];
         tc_ld64(lane_base, acc);
         // layer-1 epilogue: GELU(h + b1) -> A operand of layer 2 (row tid)
+        const float2 *sb1p = reinterpret_cast<const float2 *>(sb1);
 #pragma unroll
         for (int c = 0; c < 8; c++) {
-            uint4 w;
-            w.x = pack_bf16(gelu_fast(acc[8 * c + 0] + sb1[8 * c + 0]), gelu_fast(acc[8 * c + 1] + sb1[8 * c + 1]));
-            w.y = pack_bf16(gelu_fast(acc[8 * c + 2] + sb1[8 * c + 2]), gelu_fast(acc[8 * c + 3] + sb1[8 * c + 3]));
-            w.z = pack_bf16(gelu_fast(acc[8 * c + 4] + sb1[8 * c + 4]), gelu_fast(acc[8 * c + 5] + sb1[8 * c + 5]));
-            w.w = pack_bf16(gelu_fast(acc[8 * c + 6] + sb1[8 * c + 6]), gelu_fast(acc[8 * c + 7] + sb1[8 * c + 7]));
-            *reinterpret_cast<uint4 *>(smem + kTcA2 + tc_off(tid, 8 * c, 8)) = w;
+            uint32_t w[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int e = 8 * c + 2 * q;
+                const float2 gv = gelu2(__fadd2_rn(make_float2(acc[e], acc[e + 1]), sb1p[e >> 1]));
+                w[q] = pack_bf16(gv.x, gv.y);
+            }
+            *reinterpret_cast<uint4 *>(smem + kTcA2 + tc_off(tid, 8 * c, 8)) = make_uint4(w[0], w[1], w[2], w[3]);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -318,9 +339,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_closure_coef_tc(const R *__re
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         tc_ld64(lane_base + 64, acc);
-        float o = sb3[0];
+        // layer 3: W3 . GELU(h2 + b2) + b3, two partial sums on the paired pipe
+        const float2 *sb2p = reinterpret_cast<const float2 *>(sb2), *sW3p = reinterpret_cast<const float2 *>(sW3);
+        float2 o2 = make_float2(0.0f, 0.0f);
 #pragma unroll
-        for (int q = 0; q < 64; q++) o += gelu_fast(acc[q] + sb2[q]) * sW3[q];
+        for (int q = 0; q < 32; q++)
+            o2 = __ffma2_rn(gelu2(__fadd2_rn(make_float2(acc[2 * q], acc[2 * q + 1]), sb2p[q])), sW3p[q], o2);
+        const float o = sb3[0] + (o2.x + o2.y);
         if (cell < N) coef[cell] = (R)softplus(o);
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();   // TMEM and operands free for the next tile
