@@ -263,6 +263,10 @@ struct wf_ctx {
     cudaStream_t up = nullptr;
     cudaEvent_t ev_y = nullptr, ev_p = nullptr;
     bool p_pending = false;
+    // FP32 uploads and downloads go through two staging buffers (G and p_prev):
+    // the host copy of one chunk runs on `up` while the other is converted on
+    // the context stream; ev_copy / ev_conv order the two per buffer
+    cudaEvent_t ev_copy[2] = {nullptr, nullptr}, ev_conv[2] = {nullptr, nullptr};
     // FP32: TMA tensor maps (CUtensorMap, 128 bytes) of the state buffers a stage
     // reads, for the boxes of 16-column (map[0]) and 8-column (map[1]) tiles
     struct TensorMaps {
@@ -767,26 +771,45 @@ template <class R> __global__ void k_from_prec(double *dst, const R *src, size_t
 }
 
 // host FP64 packed vector -> device buffer of the stencil precision
+// Chunk length (doubles) of the FP32 staging: each of the two staging buffers
+// (G and p_prev) holds one chunk.
+size_t staging_chunk(const wf_ctx *c)
+{
+    const size_t g = (size_t)(c->Nz) * (c->Nx - 1) * c->h1 * 2;
+    return g < (size_t)c->N ? g : (size_t)c->N;
+}
+
 wf_status put_state(wf_ctx *c, void *dst, const double *src)
 {
     if (c->prec == WF_FP64) {
         WF_TRY_CUDA(cudaMemcpyAsync(dst, src, c->S * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         return WF_OK;
     }
-    // stage through the (double-sized) spectral buffer
-    double *tmp = reinterpret_cast<double *>(c->G);
+    // chunks alternate between the two staging buffers: the host copy of chunk
+    // i + 1 (on `up`) runs while chunk i is converted (on the context stream)
+    double *stg[2] = {reinterpret_cast<double *>(c->G), c->p_prev};
+    const size_t chunk = staging_chunk(c);
+    // the staging buffers are free once the context stream's earlier work is done
+    WF_TRY_CUDA(cudaEventRecord(c->ev_conv[0], c->stream));
+    WF_TRY_CUDA(cudaEventRecord(c->ev_conv[1], c->stream));
     size_t done = 0;
-    const size_t chunk = c->bufs.empty() ? 0 : c->G ? (size_t)(c->Nz) * (c->Nx - 1) * c->h1 * 2 : 0;
-    while (done < c->S) {
+    for (int i = 0; done < c->S; i++) {
+        const int b = i & 1;
         const size_t nn = (c->S - done < chunk) ? c->S - done : chunk;
-        WF_TRY_CUDA(cudaMemcpyAsync(tmp, src + done, nn * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-        k_to_prec<float><<<592, 256, 0, c->stream>>>((float *)dst + done, tmp, nn);
+        WF_TRY_CUDA(cudaStreamWaitEvent(c->up, c->ev_conv[b], 0));
+        WF_TRY_CUDA(cudaMemcpyAsync(stg[b], src + done, nn * sizeof(double), cudaMemcpyHostToDevice, c->up));
+        WF_TRY_CUDA(cudaEventRecord(c->ev_copy[b], c->up));
+        WF_TRY_CUDA(cudaStreamWaitEvent(c->stream, c->ev_copy[b], 0));
+        k_to_prec<float><<<592, 256, 0, c->stream>>>((float *)dst + done, stg[b], nn);
         WF_TRY_CUDA(cudaGetLastError());
+        WF_TRY_CUDA(cudaEventRecord(c->ev_conv[b], c->stream));
         done += nn;
     }
     return WF_OK;
 }
 
+// Device state -> host FP64 (waits for the copies).  FP32: the conversion of
+// chunk i + 1 (context stream) runs while chunk i is copied to the host (`up`).
 wf_status get_state(wf_ctx *c, double *dst, const void *src)
 {
     if (c->prec == WF_FP64) {
@@ -794,17 +817,29 @@ wf_status get_state(wf_ctx *c, double *dst, const void *src)
         WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
         return WF_OK;
     }
-    double *tmp = reinterpret_cast<double *>(c->G);
-    const size_t chunk = (size_t)(c->Nz) * (c->Nx - 1) * c->h1 * 2;
+    double *stg[2] = {reinterpret_cast<double *>(c->G), c->p_prev};
+    const size_t chunk = staging_chunk(c);
+    // earlier copies out of the staging buffers (previous calls) are done
+    WF_TRY_CUDA(cudaEventRecord(c->ev_copy[0], c->up));
+    WF_TRY_CUDA(cudaEventRecord(c->ev_copy[1], c->up));
     size_t done = 0;
-    while (done < c->S) {
+    for (int i = 0; done < c->S; i++) {
+        const int b = i & 1;
         const size_t nn = (c->S - done < chunk) ? c->S - done : chunk;
-        k_from_prec<float><<<592, 256, 0, c->stream>>>(tmp, (const float *)src + done, nn);
+        WF_TRY_CUDA(cudaStreamWaitEvent(c->stream, c->ev_copy[b], 0));
+        k_from_prec<float><<<592, 256, 0, c->stream>>>(stg[b], (const float *)src + done, nn);
         WF_TRY_CUDA(cudaGetLastError());
-        WF_TRY_CUDA(cudaMemcpyAsync(dst + done, tmp, nn * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-        WF_TRY_CUDA(cudaStreamSynchronize(c->stream));
+        WF_TRY_CUDA(cudaEventRecord(c->ev_conv[b], c->stream));
+        WF_TRY_CUDA(cudaStreamWaitEvent(c->up, c->ev_conv[b], 0));
+        WF_TRY_CUDA(cudaMemcpyAsync(dst + done, stg[b], nn * sizeof(double), cudaMemcpyDeviceToHost, c->up));
+        WF_TRY_CUDA(cudaEventRecord(c->ev_copy[b], c->up));
         done += nn;
     }
+    // the context stream's later work (which may reuse the staging buffers)
+    // comes after the copies
+    WF_TRY_CUDA(cudaStreamWaitEvent(c->stream, c->ev_copy[0], 0));
+    WF_TRY_CUDA(cudaStreamWaitEvent(c->stream, c->ev_copy[1], 0));
+    WF_TRY_CUDA(cudaStreamSynchronize(c->up));
     return WF_OK;
 }
 
@@ -961,7 +996,11 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
     if (cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->up, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->ev_y, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ev_p, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&c->ev_p, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_copy[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_copy[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_conv[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_conv[1], cudaEventDisableTiming) != cudaSuccess) {
         set_error("wf_create: stream creation failed");
         return fail(WF_ERR_CUDA);
     }
@@ -1074,6 +1113,10 @@ wf_status wf_destroy(wf_ctx *c)
     if (c->up) cudaStreamSynchronize(c->up);
     if (c->ev_y) cudaEventDestroy(c->ev_y);
     if (c->ev_p) cudaEventDestroy(c->ev_p);
+    for (int b = 0; b < 2; b++) {
+        if (c->ev_copy[b]) cudaEventDestroy(c->ev_copy[b]);
+        if (c->ev_conv[b]) cudaEventDestroy(c->ev_conv[b]);
+    }
     if (c->up) cudaStreamDestroy(c->up);
     if (c->aux) cudaStreamDestroy(c->aux);
     if (c->own) cudaStreamDestroy(c->own);
