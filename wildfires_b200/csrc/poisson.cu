@@ -55,19 +55,33 @@ template <int L, int RB> __device__ __forceinline__ int padl(int i) { return fft
 // planes 0, 1, 2 at k = 0 and the centred weight c = 1/(dz_{k-1} + dz_k) above
 // (the reference's differences of pressure.cu:37-95 with the division folded
 // into a weight, the values of the zc table's ZF0..ZF2 and ZC rows).
+// The variable-density source also uses the second-derivative weights s0..s3
+// (k = 0: planes 0..3; above: planes k-1, k, k+1) and the spacing dz of plane k
+// (pressure.cu:150-262).
 struct DivZ {
     double f0, f1, f2, c;
+    double s0, s1, s2, s3, dz;
 };
 __device__ __forceinline__ DivZ div_weights(const double *z, int k)
 {
-    DivZ w{0.0, 0.0, 0.0, 0.0};
+    DivZ w{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (k == 0) {
-        const double A = z[1] - z[0], B = z[2] - z[1];
+        const double A = z[1] - z[0], B = z[2] - z[1], Cc = z[3] - z[2];
         w.f0 = -(2 * A + B) / (A * (A + B));
         w.f1 = (A + B) / (A * B);
         w.f2 = -A / (B * (A + B));
+        w.s0 = (6 * A + 4 * B + 2 * Cc) / (A * (A + B) * (A + B + Cc));
+        w.s1 = -(4 * A + 4 * B + 2 * Cc) / (A * B * (B + Cc));
+        w.s2 = (4 * A + 2 * B + 2 * Cc) / (B * Cc * (A + B));
+        w.s3 = -(4 * A + 2 * B) / (Cc * (B + Cc) * (A + B + Cc));
+        w.dz = A;
     } else {
-        w.c = 1.0 / ((z[k] - z[k - 1]) + (z[k + 1] - z[k]));
+        const double a1 = z[k] - z[k - 1], A = z[k + 1] - z[k];
+        w.c = 1.0 / (a1 + A);
+        w.s0 = 2 / (a1 * (a1 + A));
+        w.s1 = -2 / (a1 * A);
+        w.s2 = 2 / (A * (a1 + A));
+        w.dz = A;
     }
     return w;
 }
@@ -102,15 +116,47 @@ __device__ __forceinline__ double velocity_divergence(const PoissonArgs<R> &a, i
     return ux + vy + wz;
 }
 
-// Poisson source at (i, j, k), k < Nz-1 (pressure.cu:37-95 and 150-321).
+// Constants of the variable-density source, once per thread.
+struct VdK {
+    double TiRi, inv_TiRi, h2x, h2y, idx2, idy2, inv_tc, inv_dt, c12, c4, A, T_act, T_pc, HC_cp, hc, as_ss, cpT;
+    int suth;
+};
+__device__ __forceinline__ VdK vd_constants(const Phys &ph)
+{
+    VdK q;
+    q.TiRi = ph.T_inf * ph.rho_inf;
+    q.inv_TiRi = 1.0 / q.TiRi;
+    q.h2x = 1.0 / (2 * ph.dx);
+    q.h2y = 1.0 / (2 * ph.dy);
+    q.idx2 = 1.0 / (ph.dx * ph.dx);
+    q.idy2 = 1.0 / (ph.dy * ph.dy);
+    q.inv_tc = 1.0 / (q.TiRi * ph.c_p);
+    q.inv_dt = 1.0 / ph.dt;
+    q.c12 = 12 * kSigmaSB * ph.delta;
+    q.c4 = 4 * kSigmaSB * ph.delta;
+    q.A = ph.A;
+    q.T_act = ph.T_act;
+    q.T_pc = ph.T_pc;
+    q.HC_cp = ph.H_C / ph.c_p;
+    q.hc = ph.h_c;
+    q.as_ss = ph.alpha_s * ph.sigma_s;
+    q.cpT = ph.c_p * q.TiRi;
+    q.suth = ph.sutherland_conductivity;
+    return q;
+}
+
+// Variable-density Poisson source at (i, j, k), k < Nz-1, from the velocity
+// divergence div (pressure.cu:103-327): f = rho_n (div u* - D_T)/dt +
+// grad(rho_n).grad(p)/rho_n.  The reference's terms, with its divisions by grid
+// constants folded into weights (VdK, DivZ), each difference of two densities
+// T_inf rho_inf (1/T_a - 1/T_b) taken over one division, T^2 and T^3 as
+// products, and the two terms that vanish exactly skipped: the Arrhenius rate
+// below T_pc (the reference multiplies it by a zero step) and the convective
+// solid-gas exchange when alpha_s sigma_s = 0.
 template <class R>
-__device__ double poisson_source(const PoissonArgs<R> &a, int i, int j, int k)
+__device__ double vd_source(const PoissonArgs<R> &a, int i, int j, int k, double div, const DivZ &w, const VdK &q)
 {
     const Geom &g = a.g;
-    const Phys &ph = a.ph;
-    const double div = velocity_divergence(a, i, j, k, 1.0 / ph.dx, 1.0 / ph.dy, div_weights(g.z, k));
-    if (ph.variable_density == 0) return ph.rho_inf * div / ph.dt;
-    // variable density: f = rho_n (div u* - D_T)/dt + grad(rho).grad(p)/rho
     const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz, N = g.N;
     const int im1 = (i == 0) ? Nx - 2 : i - 1, ip1 = (i + 1 == Nx - 1) ? 0 : i + 1;
     const int jm1 = (j == 0) ? Ny - 2 : j - 1, jp1 = (j + 1 == Ny - 1) ? 0 : j + 1;
@@ -118,48 +164,33 @@ __device__ double poisson_source(const PoissonArgs<R> &a, int i, int j, int k)
     const size_t c = ((size_t)i * Ny + j) * Nz + k;
     const size_t cxm = ((size_t)im1 * Ny + j) * Nz + k, cxp = ((size_t)ip1 * Ny + j) * Nz + k;
     const size_t cym = ((size_t)i * Ny + jm1) * Nz + k, cyp = ((size_t)i * Ny + jp1) * Nz + k;
-    const double *z = g.z;
-    double dzk_f = 0, dzkp1_f = 0, dzkp2_f = 0, dzkm1_c = 0, dzk_c = 0;
-    if (k == 0) {
-        dzk_f = z[1] - z[0];
-        dzkp1_f = z[2] - z[1];
-        dzkp2_f = z[3] - z[2];
-    } else {
-        dzkm1_c = z[k] - z[k - 1];
-        dzk_c = z[k + 1] - z[k];
-    }
     const R *T1 = U + 3 * (size_t)N;
     const R *Tn = a.yn + 3 * (size_t)N;
     const double *p = a.p;
-    const double Ti = ph.T_inf, ri = ph.rho_inf;
-    const double T = T1[c];
-    const double rho = Ti * ri / (double)Tn[c];
+    const double T = T1[c], Tnc = Tn[c];
+    const double rho = q.TiRi / Tnc;
     const double T_im1 = T1[cxm], T_ip1 = T1[cxp], T_jm1 = T1[cym], T_jp1 = T1[cyp];
-    const double Tx = (T_ip1 - T_im1) / (2 * ph.dx), Ty = (T_jp1 - T_jm1) / (2 * ph.dy);
-    const double Txx = (T_ip1 - 2 * T + T_im1) / (ph.dx * ph.dx), Tyy = (T_jp1 - 2 * T + T_jm1) / (ph.dy * ph.dy);
-    const double rhox = (Ti * ri / (double)Tn[cxp] - Ti * ri / (double)Tn[cxm]) / (2 * ph.dx);
-    const double rhoy = (Ti * ri / (double)Tn[cyp] - Ti * ri / (double)Tn[cym]) / (2 * ph.dy);
-    const double px = (p[cxp] - p[cxm]) / (2 * ph.dx), py = (p[cyp] - p[cym]) / (2 * ph.dy);
-    double rhoz, pz, Tz, Tzz, dz_k;
+    const double Tx = (T_ip1 - T_im1) * q.h2x, Ty = (T_jp1 - T_jm1) * q.h2y;
+    const double Txx = (T_ip1 - 2 * T + T_im1) * q.idx2, Tyy = (T_jp1 - 2 * T + T_jm1) * q.idy2;
+    // T_inf rho_inf (1/Tb - 1/Ta) = T_inf rho_inf (Ta - Tb) / (Ta Tb)
+    auto drho = [&](double Ta, double Tb) { return q.TiRi * (Ta - Tb) / (Ta * Tb); };
+    const double Tn_xp = Tn[cxp], Tn_xm = Tn[cxm], Tn_yp = Tn[cyp], Tn_ym = Tn[cym];
+    const double rhox = drho(Tn_xm, Tn_xp) * q.h2x, rhoy = drho(Tn_ym, Tn_yp) * q.h2y;
+    const double px = (p[cxp] - p[cxm]) * q.h2x, py = (p[cyp] - p[cym]) * q.h2y;
+    double rhoz, pz, Tz, Tzz;
     if (k == 0) {
-        const double A = dzk_f, B = dzkp1_f, Cc = dzkp2_f;
-        dz_k = A;
-        const double r1 = Ti * ri / (double)Tn[c + 1], r2 = Ti * ri / (double)Tn[c + 2];
-        rhoz = -(2 * A + B) * rho / (A * (A + B)) + (A + B) * r1 / (A * B) - A * r2 / (B * (A + B));
-        pz = -(2 * A + B) * p[c] / (A * (A + B)) + (A + B) * p[c + 1] / (A * B) - A * p[c + 2] / (B * (A + B));
+        const double r1 = q.TiRi / (double)Tn[c + 1], r2 = q.TiRi / (double)Tn[c + 2];
+        rhoz = w.f0 * rho + w.f1 * r1 + w.f2 * r2;
+        pz = w.f0 * p[c] + w.f1 * p[c + 1] + w.f2 * p[c + 2];
         const double t1 = T1[c + 1], t2 = T1[c + 2], t3 = T1[c + 3];
-        Tz = -(2 * A + B) * T / (A * (A + B)) + (A + B) * t1 / (A * B) - A * t2 / (B * (A + B));
-        Tzz = (6 * A + 4 * B + 2 * Cc) * T / (A * (A + B) * (A + B + Cc)) -
-              (4 * A + 4 * B + 2 * Cc) * t1 / (A * B * (B + Cc)) + (4 * A + 2 * B + 2 * Cc) * t2 / (B * Cc * (A + B)) -
-              (4 * A + 2 * B) * t3 / (Cc * (B + Cc) * (A + B + Cc));
+        Tz = w.f0 * T + w.f1 * t1 + w.f2 * t2;
+        Tzz = w.s0 * T + w.s1 * t1 + w.s2 * t2 + w.s3 * t3;
     } else {
-        const double a1 = dzkm1_c, A = dzk_c;
-        dz_k = A;
-        rhoz = (Ti * ri / (double)Tn[c + 1] - Ti * ri / (double)Tn[c - 1]) / (A + a1);
-        pz = (p[c + 1] - p[c - 1]) / (A + a1);
+        rhoz = drho(Tn[c - 1], Tn[c + 1]) * w.c;
+        pz = (p[c + 1] - p[c - 1]) * w.c;
         const double tp = T1[c + 1], tm = T1[c - 1];
-        Tz = (tp - tm) / (A + a1);
-        Tzz = 2 * tm / (a1 * (a1 + A)) - 2 * T / (a1 * A) + 2 * tp / (A * (a1 + A));
+        Tz = (tp - tm) * w.c;
+        Tzz = w.s0 * tm + w.s1 * T + w.s2 * tp;
     }
     const double lap_T = Txx + Tyy + Tzz;
     const int col = i * Ny + j;
@@ -168,23 +199,25 @@ __device__ double poisson_source(const PoissonArgs<R> &a, int i, int j, int k)
     const double T_solid = T;
     if (k <= nzy) {
         if (k < nzy) Yc = (double)U[4 * (size_t)N + (size_t)col * g.NzY + k];
-        T_gas = (Yc > 0.0) ? ph.T_pc + (T - ph.T_pc) : T;
+        T_gas = (Yc > 0.0) ? q.T_pc + (T - q.T_pc) : T;
     }
-    const double H_step = (T > ph.T_pc) ? 1.0 : 0.0;
-    const double K_T = ph.A * exp(-ph.T_act / T) * H_step;
-    double kT = ph.kT, dk = 0.0;
-    if (ph.sutherland_conductivity == 1) {
-        kT = 0.0241 * pow(T / 273.15, 1.5) * (273.15 + 194) / (T + 194);
-        dk = 0.0241 * (1.5 * pow(T / 273.15, 0.5) * (273.15 + 194) / (T + 194) -
-                       pow(T / 273.15, 1.5) * (273.15 + 194) / ((T + 194) * (T + 194)));
+    const double K_T = (T > q.T_pc) ? q.A * exp(-q.T_act / T) : 0.0;
+    double kT = a.ph.kT, dk = 0.0;
+    if (q.suth == 1) {
+        const double x = T / 273.15, sx = sqrt(x), x15 = x * sx, d = 1.0 / (T + 194);
+        kT = 0.0241 * x15 * (273.15 + 194) * d;
+        dk = 0.0241 * (1.5 * sx * (273.15 + 194) * d - x15 * (273.15 + 194) * (d * d));
     }
-    // (T_gas - T_solid) without abs, as the reference (pressure.cu:313)
-    const double h_c = ph.h_c * dz_k * pow((T_gas - T_solid) / dz_k, 1.0 / 4.0);
-    const double q = ph.H_C * Yc * K_T / ph.c_p -
-                     h_c * ph.alpha_s * ph.sigma_s * (T_gas - T_solid) / (ph.c_p * Ti * ri / T_gas);
-    const double divT = (dk + 12 * kSigmaSB * ph.delta * pow(T, 2) * (Tx * Tx + Ty * Ty + Tz * Tz) +
-                         (kT + 4 * kSigmaSB * ph.delta * pow(T, 3)) * lap_T) / (Ti * ri * ph.c_p) + q / T;
-    return rho * (div - divT) / ph.dt + (rhox * px + rhoy * py + rhoz * pz) / rho;
+    double qs = q.HC_cp * Yc * K_T;
+    if (q.as_ss != 0.0) {
+        // (T_gas - T_solid) without abs, as the reference (pressure.cu:313)
+        const double h_c = q.hc * w.dz * pow((T_gas - T_solid) / w.dz, 1.0 / 4.0);
+        qs -= h_c * q.as_ss * (T_gas - T_solid) / (q.cpT / T_gas);
+    }
+    const double T2 = T * T;
+    const double divT = (dk + q.c12 * T2 * (Tx * Tx + Ty * Ty + Tz * Tz) + (kT + q.c4 * (T2 * T)) * lap_T) * q.inv_tc +
+                        qs / T;
+    return rho * (div - divT) * q.inv_dt + (rhox * px + rhoy * py + rhoz * pz) * (Tnc * q.inv_TiRi);
 }
 
 // Length-n DFT of the line (buf, jj): one power-of-two FFT when n = M, else
@@ -296,14 +329,14 @@ __global__ void __launch_bounds__(256, E::kMinBlocks) k_p_rhs_ffty(const Poisson
     const int nslices = nk + 1;                      // f slices + top-plane pressure
     double *Ad = reinterpret_cast<double *>(smem);
     const int total = n1 * 2 * LB;
+    __shared__ DivZ s_w[2 * LB];   // z weights of the block's slices
+    if (threadIdx.x < 2 * LB && 2 * pair0 + threadIdx.x < nk) s_w[threadIdx.x] = div_weights(g.z, 2 * pair0 + threadIdx.x);
+    __syncthreads();
     if (a.ph.variable_density == 0) {
         // the source is the scaled divergence: SU points per thread at a
         // time, so that their loads are in flight together
         constexpr int SU = 4;
         const double idx = 1.0 / a.ph.dx, idy = 1.0 / a.ph.dy, scale = a.ph.rho_inf / a.ph.dt;
-        __shared__ DivZ s_w[2 * LB];   // z weights of the block's slices
-        if (threadIdx.x < 2 * LB && 2 * pair0 + threadIdx.x < nk) s_w[threadIdx.x] = div_weights(g.z, 2 * pair0 + threadIdx.x);
-        __syncthreads();
         for (int t0 = threadIdx.x; t0 < total; t0 += 256 * SU) {
             double val[SU];
 #pragma unroll
@@ -323,13 +356,29 @@ __global__ void __launch_bounds__(256, E::kMinBlocks) k_p_rhs_ffty(const Poisson
             }
         }
     } else {
-        for (int t = threadIdx.x; t < total; t += 256) {
-            const int jj = t / (2 * LB), q = t - jj * (2 * LB);
-            const int kk = 2 * pair0 + q;
-            double val = 0.0;
-            if (kk < nk) val = poisson_source(a, i, jj, kk);
-            else if (kk == nk) val = a.p[((size_t)i * g.Ny + jj) * g.Nz + (g.Nz - 1)];
-            Ad[2 * ((q >> 1) * LS + E::pos(jj)) + (q & 1)] = val;
+        // variable density: two points per thread at a time (each reads some
+        // twenty values)
+        constexpr int SU = 2;
+        const double idx = 1.0 / a.ph.dx, idy = 1.0 / a.ph.dy;
+        const VdK vq = vd_constants(a.ph);
+        for (int t0 = threadIdx.x; t0 < total; t0 += 256 * SU) {
+            double val[SU];
+#pragma unroll
+            for (int r = 0; r < SU; r++) {
+                const int t = t0 + 256 * r;
+                const int jj = t / (2 * LB), q = t - jj * (2 * LB);
+                const int kk = 2 * pair0 + q;
+                val[r] = 0.0;
+                if (t < total && kk < nk)
+                    val[r] = vd_source(a, i, jj, kk, velocity_divergence(a, i, jj, kk, idx, idy, s_w[q]), s_w[q], vq);
+                else if (t < total && kk == nk) val[r] = a.p[((size_t)i * g.Ny + jj) * g.Nz + (g.Nz - 1)];
+            }
+#pragma unroll
+            for (int r = 0; r < SU; r++) {
+                const int t = t0 + 256 * r;
+                const int jj = t / (2 * LB), q = t - jj * (2 * LB);
+                if (t < total) Ad[2 * ((q >> 1) * LS + E::pos(jj)) + (q & 1)] = val[r];
+            }
         }
     }
     __syncthreads();
