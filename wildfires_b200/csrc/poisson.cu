@@ -152,59 +152,62 @@ __device__ __forceinline__ VdK vd_constants(const Phys &ph)
 // T_inf rho_inf (1/T_a - 1/T_b) taken over one division, T^2 and T^3 as
 // products, and the two terms that vanish exactly skipped: the Arrhenius rate
 // below T_pc (the reference multiplies it by a zero step) and the convective
-// solid-gas exchange when alpha_s sigma_s = 0.
-template <class R>
-__device__ double vd_source(const PoissonArgs<R> &a, int i, int j, int k, double div, const DivZ &w, const VdK &q)
+// solid-gas exchange when alpha_s sigma_s = 0.  vd_base is the first term and
+// vd_rho_grad the factor grad(rho_n)/rho_n of the second; neither depends on p,
+// so the fixed point of a step evaluates them once (k_vd_base) and each solve
+// adds only grad(p) (vd_p_grad).
+struct VdIdx {
+    size_t c, cxm, cxp, cym, cyp;
+    int col;
+};
+__device__ __forceinline__ VdIdx vd_index(const Geom &g, int i, int j, int k)
 {
-    const Geom &g = a.g;
-    const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz, N = g.N;
+    const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz;
     const int im1 = (i == 0) ? Nx - 2 : i - 1, ip1 = (i + 1 == Nx - 1) ? 0 : i + 1;
     const int jm1 = (j == 0) ? Ny - 2 : j - 1, jp1 = (j + 1 == Ny - 1) ? 0 : j + 1;
+    VdIdx x;
+    x.c = ((size_t)i * Ny + j) * Nz + k;
+    x.cxm = ((size_t)im1 * Ny + j) * Nz + k;
+    x.cxp = ((size_t)ip1 * Ny + j) * Nz + k;
+    x.cym = ((size_t)i * Ny + jm1) * Nz + k;
+    x.cyp = ((size_t)i * Ny + jp1) * Nz + k;
+    x.col = i * Ny + j;
+    return x;
+}
+template <class R>
+__device__ double vd_base(const PoissonArgs<R> &a, int k, const VdIdx &x, double div, const DivZ &w, const VdK &q)
+{
+    const Geom &g = a.g;
+    const size_t N = (size_t)g.N, c = x.c;
     const R *U = a.y1;
-    const size_t c = ((size_t)i * Ny + j) * Nz + k;
-    const size_t cxm = ((size_t)im1 * Ny + j) * Nz + k, cxp = ((size_t)ip1 * Ny + j) * Nz + k;
-    const size_t cym = ((size_t)i * Ny + jm1) * Nz + k, cyp = ((size_t)i * Ny + jp1) * Nz + k;
-    const R *T1 = U + 3 * (size_t)N;
-    const R *Tn = a.yn + 3 * (size_t)N;
-    const double *p = a.p;
-    const double T = T1[c], Tnc = Tn[c];
-    const double rho = q.TiRi / Tnc;
-    const double T_im1 = T1[cxm], T_ip1 = T1[cxp], T_jm1 = T1[cym], T_jp1 = T1[cyp];
+    const R *T1 = U + 3 * N;
+    const double T = T1[c];
+    const double rho = q.TiRi / (double)a.yn[3 * N + c];
+    const double T_im1 = T1[x.cxm], T_ip1 = T1[x.cxp], T_jm1 = T1[x.cym], T_jp1 = T1[x.cyp];
     const double Tx = (T_ip1 - T_im1) * q.h2x, Ty = (T_jp1 - T_jm1) * q.h2y;
     const double Txx = (T_ip1 - 2 * T + T_im1) * q.idx2, Tyy = (T_jp1 - 2 * T + T_jm1) * q.idy2;
-    // T_inf rho_inf (1/Tb - 1/Ta) = T_inf rho_inf (Ta - Tb) / (Ta Tb)
-    auto drho = [&](double Ta, double Tb) { return q.TiRi * (Ta - Tb) / (Ta * Tb); };
-    const double Tn_xp = Tn[cxp], Tn_xm = Tn[cxm], Tn_yp = Tn[cyp], Tn_ym = Tn[cym];
-    const double rhox = drho(Tn_xm, Tn_xp) * q.h2x, rhoy = drho(Tn_ym, Tn_yp) * q.h2y;
-    const double px = (p[cxp] - p[cxm]) * q.h2x, py = (p[cyp] - p[cym]) * q.h2y;
-    double rhoz, pz, Tz, Tzz;
+    double Tz, Tzz;
     if (k == 0) {
-        const double r1 = q.TiRi / (double)Tn[c + 1], r2 = q.TiRi / (double)Tn[c + 2];
-        rhoz = w.f0 * rho + w.f1 * r1 + w.f2 * r2;
-        pz = w.f0 * p[c] + w.f1 * p[c + 1] + w.f2 * p[c + 2];
         const double t1 = T1[c + 1], t2 = T1[c + 2], t3 = T1[c + 3];
         Tz = w.f0 * T + w.f1 * t1 + w.f2 * t2;
         Tzz = w.s0 * T + w.s1 * t1 + w.s2 * t2 + w.s3 * t3;
     } else {
-        rhoz = drho(Tn[c - 1], Tn[c + 1]) * w.c;
-        pz = (p[c + 1] - p[c - 1]) * w.c;
         const double tp = T1[c + 1], tm = T1[c - 1];
         Tz = (tp - tm) * w.c;
         Tzz = w.s0 * tm + w.s1 * T + w.s2 * tp;
     }
     const double lap_T = Txx + Tyy + Tzz;
-    const int col = i * Ny + j;
-    const int nzy = g.nzy[col];
+    const int nzy = g.nzy[x.col];
     double Yc = 0.0, T_gas = T;
     const double T_solid = T;
     if (k <= nzy) {
-        if (k < nzy) Yc = (double)U[4 * (size_t)N + (size_t)col * g.NzY + k];
+        if (k < nzy) Yc = (double)U[4 * N + (size_t)x.col * g.NzY + k];
         T_gas = (Yc > 0.0) ? q.T_pc + (T - q.T_pc) : T;
     }
     const double K_T = (T > q.T_pc) ? q.A * exp(-q.T_act / T) : 0.0;
     double kT = a.ph.kT, dk = 0.0;
     if (q.suth == 1) {
-        const double x = T / 273.15, sx = sqrt(x), x15 = x * sx, d = 1.0 / (T + 194);
+        const double xx = T / 273.15, sx = sqrt(xx), x15 = xx * sx, d = 1.0 / (T + 194);
         kT = 0.0241 * x15 * (273.15 + 194) * d;
         dk = 0.0241 * (1.5 * sx * (273.15 + 194) * d - x15 * (273.15 + 194) * (d * d));
     }
@@ -217,7 +220,60 @@ __device__ double vd_source(const PoissonArgs<R> &a, int i, int j, int k, double
     const double T2 = T * T;
     const double divT = (dk + q.c12 * T2 * (Tx * Tx + Ty * Ty + Tz * Tz) + (kT + q.c4 * (T2 * T)) * lap_T) * q.inv_tc +
                         qs / T;
-    return rho * (div - divT) * q.inv_dt + (rhox * px + rhoy * py + rhoz * pz) * (Tnc * q.inv_TiRi);
+    return rho * (div - divT) * q.inv_dt;
+}
+// grad(rho_n)/rho_n at the cell (p-independent)
+template <class R>
+__device__ __forceinline__ double3 vd_rho_grad(const PoissonArgs<R> &a, int k, const VdIdx &x, const DivZ &w, const VdK &q)
+{
+    const size_t N = (size_t)a.g.N, c = x.c;
+    const R *Tn = a.yn + 3 * N;
+    const double Tnc = Tn[c];
+    // T_inf rho_inf (1/Tb - 1/Ta) = T_inf rho_inf (Ta - Tb) / (Ta Tb)
+    auto drho = [&](double Ta, double Tb) { return q.TiRi * (Ta - Tb) / (Ta * Tb); };
+    const double Tn_xp = Tn[x.cxp], Tn_xm = Tn[x.cxm], Tn_yp = Tn[x.cyp], Tn_ym = Tn[x.cym];
+    const double rhox = drho(Tn_xm, Tn_xp) * q.h2x, rhoy = drho(Tn_ym, Tn_yp) * q.h2y;
+    double rhoz;
+    if (k == 0) {
+        const double rho = q.TiRi / Tnc;
+        const double r1 = q.TiRi / (double)Tn[c + 1], r2 = q.TiRi / (double)Tn[c + 2];
+        rhoz = w.f0 * rho + w.f1 * r1 + w.f2 * r2;
+    } else {
+        rhoz = drho(Tn[c - 1], Tn[c + 1]) * w.c;
+    }
+    const double ir = Tnc * q.inv_TiRi;
+    return make_double3(rhox * ir, rhoy * ir, rhoz * ir);
+}
+// grad(p) at the cell
+__device__ __forceinline__ double3 vd_p_grad(const double *p, int k, const VdIdx &x, const DivZ &w, const VdK &q)
+{
+    const size_t c = x.c;
+    const double px = (p[x.cxp] - p[x.cxm]) * q.h2x, py = (p[x.cyp] - p[x.cym]) * q.h2y;
+    const double pz = (k == 0) ? w.f0 * p[c] + w.f1 * p[c + 1] + w.f2 * p[c + 2] : (p[c + 1] - p[c - 1]) * w.c;
+    return make_double3(px, py, pz);
+}
+
+// p-independent part of the variable-density source of every cell k < Nz-1
+// (once per step, before the fixed point): one block per (i, j) column, one
+// thread per plane.
+template <class R>
+__global__ void __launch_bounds__(128) k_vd_base(const PoissonArgs<R> a)
+{
+    const Geom &g = a.g;
+    const int i = blockIdx.y, j = blockIdx.x;
+    const double idx = 1.0 / a.ph.dx, idy = 1.0 / a.ph.dy;
+    const VdK q = vd_constants(a.ph);
+    const size_t N = (size_t)g.N;
+    for (int k = threadIdx.x; k < g.Nz - 1; k += blockDim.x) {
+        const double *t = a.vdz + (size_t)k * kVdz;
+        const DivZ w{t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7], t[8]};
+        const VdIdx x = vd_index(g, i, j, k);
+        a.s0[x.c] = vd_base(a, k, x, velocity_divergence(a, i, j, k, idx, idy, w), w, q);
+        const double3 gr = vd_rho_grad(a, k, x, w, q);
+        a.g3[x.c] = (R)gr.x;
+        a.g3[N + x.c] = (R)gr.y;
+        a.g3[2 * N + x.c] = (R)gr.z;
+    }
 }
 
 // Length-n DFT of the line (buf, jj): one power-of-two FFT when n = M, else
@@ -369,8 +425,19 @@ __global__ void __launch_bounds__(256, E::kMinBlocks) k_p_rhs_ffty(const Poisson
                 const int jj = t / (2 * LB), q = t - jj * (2 * LB);
                 const int kk = 2 * pair0 + q;
                 val[r] = 0.0;
-                if (t < total && kk < nk)
-                    val[r] = vd_source(a, i, jj, kk, velocity_divergence(a, i, jj, kk, idx, idy, s_w[q]), s_w[q], vq);
+                if (t < total && kk < nk) {
+                    const VdIdx x = vd_index(g, i, jj, kk);
+                    const double3 pg = vd_p_grad(a.p, kk, x, s_w[q], vq);
+                    if (a.s0) {
+                        const size_t N = (size_t)g.N;
+                        val[r] = a.s0[x.c] + ((double)a.g3[x.c] * pg.x + (double)a.g3[N + x.c] * pg.y +
+                                              (double)a.g3[2 * N + x.c] * pg.z);
+                    } else {
+                        const double3 rg = vd_rho_grad(a, kk, x, s_w[q], vq);
+                        val[r] = vd_base(a, kk, x, velocity_divergence(a, i, jj, kk, idx, idy, s_w[q]), s_w[q], vq) +
+                                 (rg.x * pg.x + rg.y * pg.y + rg.z * pg.z);
+                    }
+                }
                 else if (t < total && kk == nk) val[r] = a.p[((size_t)i * g.Ny + jj) * g.Nz + (g.Nz - 1)];
             }
 #pragma unroll
@@ -841,6 +908,41 @@ cudaError_t launch_poisson_impl(const PoissonArgs<R> &a, const double *zt, cudaS
 }
 template cudaError_t launch_poisson_impl<double>(const PoissonArgs<double> &, const double *, cudaStream_t, cudaEvent_t *);
 template cudaError_t launch_poisson_impl<float>(const PoissonArgs<float> &, const double *, cudaStream_t, cudaEvent_t *);
+
+template <class R> cudaError_t launch_vd_base(const PoissonArgs<R> &a, cudaStream_t s)
+{
+    if (!a.s0 || !a.g3 || !a.vdz || a.g.Nx > 65535) return cudaErrorInvalidValue;
+    k_vd_base<R><<<dim3(a.g.Ny, a.g.Nx), 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+template cudaError_t launch_vd_base<double>(const PoissonArgs<double> &, cudaStream_t);
+template cudaError_t launch_vd_base<float>(const PoissonArgs<float> &, cudaStream_t);
+
+void vd_z_table(const double *z, int Nz, double *out)
+{
+    for (int k = 0; k < Nz; k++) {
+        double *w = out + (size_t)k * kVdz;
+        for (int e = 0; e < kVdz; e++) w[e] = 0.0;
+        if (k == 0 && Nz >= 4) {
+            const double A = z[1] - z[0], B = z[2] - z[1], Cc = z[3] - z[2];
+            w[0] = -(2 * A + B) / (A * (A + B));
+            w[1] = (A + B) / (A * B);
+            w[2] = -A / (B * (A + B));
+            w[4] = (6 * A + 4 * B + 2 * Cc) / (A * (A + B) * (A + B + Cc));
+            w[5] = -(4 * A + 4 * B + 2 * Cc) / (A * B * (B + Cc));
+            w[6] = (4 * A + 2 * B + 2 * Cc) / (B * Cc * (A + B));
+            w[7] = -(4 * A + 2 * B) / (Cc * (B + Cc) * (A + B + Cc));
+            w[8] = A;
+        } else if (k > 0 && k + 1 < Nz) {
+            const double a1 = z[k] - z[k - 1], A = z[k + 1] - z[k];
+            w[3] = 1.0 / (a1 + A);
+            w[4] = 2 / (a1 * (a1 + A));
+            w[5] = -2 / (a1 * A);
+            w[6] = 2 / (A * (a1 + A));
+            w[8] = A;
+        }
+    }
+}
 
 // ---- variable-density fixed point, driven on the device ------------------
 // The loop (pressure.cu:551-606) runs as a CUDA graph WHILE node: its body is

@@ -222,6 +222,8 @@ struct wf_ctx {
     void *Xa = nullptr, *Xb = nullptr, *acc = nullptr, *utau = nullptr, *bc = nullptr;
     void *Tsrc = nullptr;
     double *p = nullptr, *p_prev = nullptr, *d_diag = nullptr;
+    double *vd_s0 = nullptr, *d_vdz = nullptr;   // variable density: per-step source part, z weights
+    void *vd_g3 = nullptr;                        // variable density: grad(rho_n)/rho_n, [3][N] in the stencil precision
     double2 *G = nullptr;
     double *d_z = nullptr, *d_zc = nullptr, *d_topo = nullptr, *d_kx2 = nullptr, *d_ky2 = nullptr, *d_zt = nullptr;
     double *d_x = nullptr, *d_y = nullptr;
@@ -299,15 +301,15 @@ wf_status settle_p(wf_ctx *c)
 
 // Kernel launches of one step: per stage the optional closure inference,
 // k_utau, k_stage_fused and, when some column needs it, k_stage_bc; five
-// pressure kernels per solve (variable density: plus the record reset and,
-// per iteration, k_maxdiff_copy and k_piter_next; counted for max_iter
-// iterations, an upper bound when the tolerance ends the loop early); the
-// projection.
+// pressure kernels per solve (variable density: plus the record reset, the
+// source's p-independent part and, per iteration, k_maxdiff_copy and
+// k_piter_next; counted for max_iter iterations, an upper bound when the
+// tolerance ends the loop early); the projection.
 int launches_per_step(const wf_ctx *c)
 {
     const int per_stage = 2 + (c->nbcfix > 0 ? 1 : 0) + (c->closure ? 1 : 0);
     const int maxit = c->P.pressure_solver_iter > 0 ? c->P.pressure_solver_iter : 0;
-    const int pressure = (c->P.variable_density != 0) ? 1 + 7 * maxit : 5;
+    const int pressure = (c->P.variable_density != 0) ? 1 + (maxit > 0 ? 1 : 0) + 7 * maxit : 5;
     return c->nstages * per_stage + pressure + 1;
 }
 
@@ -575,6 +577,9 @@ template <class R> PoissonArgs<R> poisson_args(wf_ctx *c, const void *y1, const 
     a.fx = c->fx;
     a.fy = c->fy;
     a.h1 = c->h1;
+    a.s0 = nullptr;
+    a.g3 = nullptr;
+    a.vdz = c->d_vdz;
     return a;
 }
 
@@ -621,6 +626,13 @@ template <class R> wf_status capture_pressure_loop(wf_ctx *c, const PoissonArgs<
     WF_TRY_CUDA(cudaMemcpyAsync(c->p_prev, c->p, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, s));
     WF_TRY_CUDA(launch_piter_begin(c->rec, s));
     if (maxit <= 0) return WF_OK;   // the reference's loop body does not run
+    // the source's p-independent part, once for every solve of the fixed point
+    PoissonArgs<R> ab = a;
+    if (c->vd_s0 && c->vd_g3 && c->d_vdz) {
+        ab.s0 = c->vd_s0;
+        ab.g3 = (R *)c->vd_g3;
+        WF_TRY_CUDA(launch_vd_base<R>(ab, s));
+    }
     cudaStreamCaptureStatus cs;
     cudaGraph_t g = nullptr;
     const cudaGraphNode_t *deps = nullptr;
@@ -638,7 +650,7 @@ template <class R> wf_status capture_pressure_loop(wf_ctx *c, const PoissonArgs<
     WF_TRY_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
     cudaGraph_t body = np.conditional.phGraph_out[0];
     WF_TRY_CUDA(cudaStreamBeginCaptureToGraph(c->aux, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = launch_poisson_impl<R>(a, c->d_zt, c->aux);
+    cudaError_t e = launch_poisson_impl<R>(ab, c->d_zt, c->aux);
     if (!e) e = launch_maxdiff_copy(c->p, c->p_prev, c->N, c->rec, c->aux);
     if (!e) e = launch_piter_next(c->rec, tol, tol >= 0 ? 1 : 0, maxit, cond, c->aux);
     cudaGraph_t captured = nullptr;
@@ -987,6 +999,13 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
     if ((st = dev_alloc(c, &c->bc, (size_t)Nx * Ny * kBcSlots * c->esz))) return fail(st);
     if ((st = dev_alloc(c, (void **)&c->p, sizeof(double) * c->N))) return fail(st);
     if ((st = dev_alloc(c, (void **)&c->p_prev, sizeof(double) * c->N))) return fail(st);
+    if (P->variable_density != 0) {
+        if ((st = dev_alloc(c, (void **)&c->vd_s0, sizeof(double) * c->N))) return fail(st);
+        if ((st = dev_alloc(c, &c->vd_g3, 3 * (size_t)c->N * c->esz))) return fail(st);
+        std::vector<double> vz((size_t)Nz * kVdz);
+        vd_z_table(c->hz.data(), Nz, vz.data());
+        if ((st = upload(c, &c->d_vdz, vz.data(), vz.size()))) return fail(st);
+    }
     if ((st = dev_alloc(c, (void **)&c->G, sizeof(double2) * (size_t)Nz * (Nx - 1) * c->h1))) return fail(st);
     if ((st = dev_alloc(c, (void **)&c->rec, sizeof(PIterRec)))) return fail(st);
     if (cudaMemset(c->rec, 0, sizeof(PIterRec)) != cudaSuccess) {

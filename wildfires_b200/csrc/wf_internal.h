@@ -216,7 +216,18 @@ struct PoissonArgs {
     const double *ky2;      // [Ny-1] ky^2
     FftDesc fx, fy;         // x: length Nx-1, y: length Ny-1
     int h1;                 // (Ny-1)/2 + 1
+    // variable density: the parts of the source that do not depend on p, per
+    // cell (written once per step by launch_vd_base, then read by every solve of
+    // the fixed point), or nullptr (each solve evaluates the whole source); and
+    // the z weights of the source per plane ([Nz][kVdz]: f0, f1, f2, c, s0..s3, dz)
+    double *s0;
+    R *g3;                  // with s0: grad(rho_n)/rho_n per cell, [3][N] (x, y, z components)
+    const double *vdz;
 };
+constexpr int kVdz = 9;
+template <class R> cudaError_t launch_vd_base(const PoissonArgs<R> &a, cudaStream_t s);
+// z weights of the variable-density source for every plane (host, [Nz][kVdz])
+void vd_z_table(const double *z, int Nz, double *out);
 // zt: tridiagonal constants per k (layout documented at k_p_tridiag).
 // ev (optional): one event recorded after each of the 5 kernels, for profiling.
 template <class R>
