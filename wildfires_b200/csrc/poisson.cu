@@ -18,6 +18,8 @@
 // G is (Nz-1+1) x (Nx-1) x h1 complex doubles, s fastest, h1 = (Ny-1)/2+1.
 #include <math.h>
 
+#include <type_traits>
+
 #include "fft.cuh"
 #include "fft_pr.cuh"
 #include "wf_internal.h"
@@ -412,41 +414,48 @@ __global__ void __launch_bounds__(256, E::kMinBlocks) k_p_rhs_ffty(const Poisson
             }
         }
     } else {
-        // variable density: two points per thread at a time (each reads some
-        // twenty values)
-        constexpr int SU = 2;
+        // variable density.  Within the fixed point (a.s0 set) each point adds
+        // grad(p) . (grad(rho)/rho) to the per-step part: four points per thread
+        // at a time; otherwise the whole source, two at a time
         const double idx = 1.0 / a.ph.dx, idy = 1.0 / a.ph.dy;
         const VdK vq = vd_constants(a.ph);
-        for (int t0 = threadIdx.x; t0 < total; t0 += 256 * SU) {
-            double val[SU];
+        auto vd_points = [&](auto su, auto fixed) {
+            constexpr int SU = decltype(su)::value;
+            constexpr bool FIXED = decltype(fixed)::value;   // a.s0 and a.g3 are set
+            for (int t0 = threadIdx.x; t0 < total; t0 += 256 * SU) {
+                double val[SU];
 #pragma unroll
-            for (int r = 0; r < SU; r++) {
-                const int t = t0 + 256 * r;
-                const int jj = t / (2 * LB), q = t - jj * (2 * LB);
-                const int kk = 2 * pair0 + q;
-                val[r] = 0.0;
-                if (t < total && kk < nk) {
-                    const VdIdx x = vd_index(g, i, jj, kk);
-                    const double3 pg = vd_p_grad(a.p, kk, x, s_w[q], vq);
-                    if (a.s0) {
-                        const size_t N = (size_t)g.N;
-                        val[r] = a.s0[x.c] + ((double)a.g3[x.c] * pg.x + (double)a.g3[N + x.c] * pg.y +
-                                              (double)a.g3[2 * N + x.c] * pg.z);
-                    } else {
-                        const double3 rg = vd_rho_grad(a, kk, x, s_w[q], vq);
-                        val[r] = vd_base(a, kk, x, velocity_divergence(a, i, jj, kk, idx, idy, s_w[q]), s_w[q], vq) +
-                                 (rg.x * pg.x + rg.y * pg.y + rg.z * pg.z);
+                for (int r = 0; r < SU; r++) {
+                    const int t = t0 + 256 * r;
+                    const int jj = t / (2 * LB), q = t - jj * (2 * LB);
+                    const int kk = 2 * pair0 + q;
+                    val[r] = 0.0;
+                    if (t < total && kk < nk) {
+                        const VdIdx x = vd_index(g, i, jj, kk);
+                        const double3 pg = vd_p_grad(a.p, kk, x, s_w[q], vq);
+                        if constexpr (FIXED) {
+                            const size_t N = (size_t)g.N;
+                            val[r] = a.s0[x.c] + ((double)a.g3[x.c] * pg.x + (double)a.g3[N + x.c] * pg.y +
+                                                  (double)a.g3[2 * N + x.c] * pg.z);
+                        } else {
+                            const double3 rg = vd_rho_grad(a, kk, x, s_w[q], vq);
+                            val[r] = vd_base(a, kk, x, velocity_divergence(a, i, jj, kk, idx, idy, s_w[q]), s_w[q], vq) +
+                                     (rg.x * pg.x + rg.y * pg.y + rg.z * pg.z);
+                        }
+                    } else if (t < total && kk == nk) {
+                        val[r] = a.p[((size_t)i * g.Ny + jj) * g.Nz + (g.Nz - 1)];
                     }
                 }
-                else if (t < total && kk == nk) val[r] = a.p[((size_t)i * g.Ny + jj) * g.Nz + (g.Nz - 1)];
-            }
 #pragma unroll
-            for (int r = 0; r < SU; r++) {
-                const int t = t0 + 256 * r;
-                const int jj = t / (2 * LB), q = t - jj * (2 * LB);
-                if (t < total) Ad[2 * ((q >> 1) * LS + E::pos(jj)) + (q & 1)] = val[r];
+                for (int r = 0; r < SU; r++) {
+                    const int t = t0 + 256 * r;
+                    const int jj = t / (2 * LB), q = t - jj * (2 * LB);
+                    if (t < total) Ad[2 * ((q >> 1) * LS + E::pos(jj)) + (q & 1)] = val[r];
+                }
             }
-        }
+        };
+        if (a.s0) vd_points(std::integral_constant<int, 4>{}, std::true_type{});
+        else vd_points(std::integral_constant<int, 2>{}, std::false_type{});
     }
     __syncthreads();
     {
