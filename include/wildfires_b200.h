@@ -326,9 +326,12 @@ int wf_launches_per_step(const wf_ctx *ctx);
 /* Advance nsteps steps with the kernels launched one by one (no graph) and a
  * CUDA event recorded after each kernel on the context's stream.  For every
  * kernel kind q < WF_NPHASES, ms[q] receives the summed device time and
- * launches[q] the number of launches.  Returns WF_OK or an error status. */
+ * launches[q] the number of launches.  Variable density: pressure_solver_iter
+ * solves per step without the tolerance test, the per-step part of the source
+ * counted in the first solve's source kernel.  Returns WF_OK or an error
+ * status. */
 wf_status wf_profile_phases(wf_ctx *ctx, int nsteps, double *ms, int *launches);
-/* Name of kernel kind q ("stage_rhs", "p_fftx_fwd", ...), or NULL. */
+/* Name of kernel kind q ("stage_fused", "p_fftx_fwd", ...), or NULL. */
 const char *wf_phase_name(int q);
 
 /* ---- pressure solve without device allocation --------------------------- */

@@ -883,8 +883,15 @@ template <class R> wf_status profile_step(wf_ctx *c, cudaEvent_t *ev, int &ne)
         WF_TRY_CUDA(launch_stage<R>(stage_args<R>(c, ins[st], yn, (void *)outs[st], st + 1), s, ev + ne));
         ne += 3;
     }
-    const PoissonArgs<R> a = poisson_args<R>(c, y1, yn);
+    PoissonArgs<R> a = poisson_args<R>(c, y1, yn);
     const int nsolve = (c->P.variable_density == 0) ? 1 : c->P.pressure_solver_iter;
+    if (nsolve > 0 && c->P.variable_density != 0 && c->vd_s0 && c->vd_g3 && c->d_vdz) {
+        // as the fixed point runs: the per-step part of the source first (its
+        // time lands in the first solve's source kernel), then every solve
+        a.s0 = c->vd_s0;
+        a.g3 = (R *)c->vd_g3;
+        WF_TRY_CUDA(launch_vd_base<R>(a, s));
+    }
     for (int q = 0; q < nsolve; q++) {
         WF_TRY_CUDA(launch_poisson_impl<R>(a, c->d_zt, s, ev + ne));
         ne += 5;
