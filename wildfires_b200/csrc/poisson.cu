@@ -5,16 +5,19 @@
 // (:14-101), compute_f_density (:103-327), gammas_and_coefficients (:356-390),
 // update_coefficients (:473-504), thomas_algorithm (:418-443), post_fft
 // (:392-416).  The reference calls cuFFT Z2Z on real data; here every transform
-// is a hand-written FP64 FFT held in shared memory, real-to-complex in y (two
-// real z-slices packed into one complex line), complex in x on the half
+// is a hand-written FP64 FFT held in shared memory (power-of-two Stockham or
+// Bluestein, fft.cuh; prime factors and Rader, fft_pr.cuh), real-to-complex in
+// y (two real z-slices packed into one complex line), complex in x on the half
 // spectrum.  Five passes, each one kernel:
-//   P1 k_p_rhs_ffty   Poisson source f (and the top-plane pressure as one extra
-//                     slice) + forward FFT along y        -> G[kk][i][s]
-//   P2 k_p_fftx<fwd>  forward FFT along x                 -> G[kk][r][s]
-//   P3 k_p_tridiag    Thomas along z per (r,s)            -> G[kk][r][s]
-//   P4 k_p_fftx<inv>  inverse FFT along x
-//   P5 k_p_iffty_out  inverse FFT along y, normalisation, p and its periodic
-//                     duplicate planes.
+//   P1 k_p_rhs_ffty        Poisson source f (and the top-plane pressure as one
+//                          extra slice) + forward FFT along y   -> G[kk][i][s]
+//   P2 k_p_fftx[_pr]<fwd>  forward FFT along x                  -> G[kk][r][s]
+//   P3 k_p_tridiag         Thomas along z per (r,s)             -> G[kk][r][s]
+//   P4 k_p_fftx[_pr]<inv>  inverse FFT along x
+//   P5 k_p_iffty_out       inverse FFT along y, normalisation, p and its
+//                          periodic duplicate planes.
+// Variable density adds k_vd_base once per step (the source's p-independent
+// parts) ahead of the fixed point's solves.
 // G is (Nz-1+1) x (Nx-1) x h1 complex doubles, s fastest, h1 = (Ny-1)/2+1.
 #include <math.h>
 
