@@ -643,21 +643,29 @@ __global__ void __launch_bounds__(NT, sizeof(R) != 4 ? 1 : NT > 256 ? 2 : (TI * 
                     };
                     const int qxp = TL::cq(ii + 1, jj), qxm = TL::cq(ii - 1, jj);
                     const int qyp = TL::cq(ii, jj + 1), qym = TL::cq(ii, jj - 1);
-                    R fc = R(1), fxp_ = R(1), fxm_ = R(1), fyp_ = R(1), fym_ = R(1), fkm = R(1), fkp = R(1);
+                    R mu_c = t.G(0, ii, jj, kk);
+                    R mu_xp = t.G(0, ii + 1, jj, kk), mu_xm = t.G(0, ii - 1, jj, kk);
+                    R mu_yp = t.G(0, ii, jj + 1, kk), mu_ym = t.G(0, ii, jj - 1, kk);
+                    R mu_kp = t.G(0, ii, jj, kk + 1), mu_km = t.G(0, ii, jj, kk - 1);
+                    // Van Driest factors; where the bound shows them all to be
+                    // exactly 1 the products would not change mu
                     if (!(s_vd_bound > VanDriestCut<R>::v * R(1.001) * nu)) {
                         const R ut0 = t.cut_[cc];
-                        fc = van_driest(-zibm(cc, zk) * ut0 * inv_avd_nu);
-                        fxp_ = van_driest(-zibm(qxp, zk) * t.cut_[qxp] * inv_avd_nu);
-                        fxm_ = van_driest(-zibm(qxm, zk) * t.cut_[qxm] * inv_avd_nu);
-                        fyp_ = van_driest(-zibm(qyp, zk) * t.cut_[qyp] * inv_avd_nu);
-                        fym_ = van_driest(-zibm(qym, zk) * t.cut_[qym] * inv_avd_nu);
-                        fkm = van_driest(-zibm(cc, t.K(kk - 1, RZ)) * ut0 * inv_avd_nu);
-                        fkp = van_driest(-zibm(cc, t.K(kk + 1, RZ)) * ut0 * inv_avd_nu);
+                        const R fc = van_driest(-zibm(cc, zk) * ut0 * inv_avd_nu);
+                        const R fxp_ = van_driest(-zibm(qxp, zk) * t.cut_[qxp] * inv_avd_nu);
+                        const R fxm_ = van_driest(-zibm(qxm, zk) * t.cut_[qxm] * inv_avd_nu);
+                        const R fyp_ = van_driest(-zibm(qyp, zk) * t.cut_[qyp] * inv_avd_nu);
+                        const R fym_ = van_driest(-zibm(qym, zk) * t.cut_[qym] * inv_avd_nu);
+                        const R fkm = van_driest(-zibm(cc, t.K(kk - 1, RZ)) * ut0 * inv_avd_nu);
+                        const R fkp = van_driest(-zibm(cc, t.K(kk + 1, RZ)) * ut0 * inv_avd_nu);
+                        mu_c *= fc * fc;
+                        mu_xp *= fxp_ * fxp_;
+                        mu_xm *= fxm_ * fxm_;
+                        mu_yp *= fyp_ * fyp_;
+                        mu_ym *= fym_ * fym_;
+                        mu_kp *= fkp * fkp;
+                        mu_km *= fkm * fkm;
                     }
-                    const R mu_c = t.G(0, ii, jj, kk) * (fc * fc);
-                    const R mu_xp = t.G(0, ii + 1, jj, kk) * (fxp_ * fxp_), mu_xm = t.G(0, ii - 1, jj, kk) * (fxm_ * fxm_);
-                    const R mu_yp = t.G(0, ii, jj + 1, kk) * (fyp_ * fyp_), mu_ym = t.G(0, ii, jj - 1, kk) * (fym_ * fym_);
-                    const R mu_kp = t.G(0, ii, jj, kk + 1) * (fkp * fkp), mu_km = t.G(0, ii, jj, kk - 1) * (fkm * fkm);
                     const R S11 = t.G(1, ii, jj, kk), S12 = t.G(2, ii, jj, kk), S13 = t.G(3, ii, jj, kk);
                     const R S22 = t.G(4, ii, jj, kk), S23 = t.G(5, ii, jj, kk), S33 = t.G(6, ii, jj, kk);
                     const R wc = t.K(kk, RD1);
