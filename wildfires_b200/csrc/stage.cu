@@ -63,7 +63,6 @@ __global__ void __launch_bounds__(128) k_utau(const StageArgs<R> a)
 template <class R, int TI, int TJ, int KZ> struct Tile {
     static constexpr int SI = TI + 4, SJ = TJ + 4, SK = KZ + 4, SR = SI * SJ * SK;
     static constexpr int GI = TI + 2, GJ = TJ + 2, GK = KZ + 2, GJP = SJ, GR = GI * GK * GJP;
-    static constexpr int ZS = SJ;   // z stride of the state tile
     static constexpr bool PAIRED = sizeof(R) == 4;
     static constexpr int NCOL = GI * GJ, CELLS = TI * TJ * KZ;
     static constexpr size_t up16(size_t b) { return (b + 15) / 16 * 16; }
