@@ -251,6 +251,7 @@ __global__ void __launch_bounds__(NT, sizeof(R) != 4 ? 1 : NT > 256 ? 2 : (TI * 
     R *sgs = reinterpret_cast<R *>(smem_raw + TL::BUF);
     R *s_vd = reinterpret_cast<R *>(smem_raw + TL::O_MISC);
     int *s_fail = reinterpret_cast<int *>(smem_raw + TL::O_MISC + 8);
+    int *s_vd_zero = reinterpret_cast<int *>(smem_raw + TL::O_MISC + 12);
     const uint32_t bar = (uint32_t)__cvta_generic_to_shared(smem_raw + TL::O_MISC + 16);
     const Geom &g = a.g;
     const PhysR<R> &p = a.pr;
@@ -325,21 +326,34 @@ __global__ void __launch_bounds__(NT, sizeof(R) != 4 ? 1 : NT > 256 ? 2 : (TI * 
         // divergence source nu T_RHS / T reduces to mu/(T_inf rho_inf) T_RHS
         const bool lean = sizeof(R) == 4 && smu != 1 && sk != 1 && !(p.alpha_s * p.sigma_s != R(0));
 
-        // Lower bound over the tile of z_ibm u_tau / A_vd: when it exceeds
-        // the cut-off times nu, every Van Driest factor of the tile is exactly 1.
+        // Lower bound over the tile of z_ibm u_tau / A_vd, taken over the
+        // columns with wall friction: when it exceeds the cut-off times nu,
+        // every Van Driest factor of those columns is exactly 1, and every
+        // factor of a column without friction (u_tau = 0, as over the hills)
+        // is 1 - exp(-0) = 0 at any height.
         R &s_vd_bound = *s_vd;
         if (threadIdx.x < 32) {
             const R zlow = (k0 > 0) ? t.K(-1, RZ) : R(0);
             R hmax = R(-1e30), umin = R(1e30);
+            bool zero = false;
             for (int c = threadIdx.x; c < TL::NCOL; c += 32) {
-                hmax = rmax(hmax, (R)t.ctopo[c]);
-                umin = rmin(umin, t.cut_[c]);
+                const R ut = t.cut_[c];
+                if (ut == R(0)) {
+                    zero = true;
+                } else {
+                    hmax = rmax(hmax, (R)t.ctopo[c]);
+                    umin = rmin(umin, ut);
+                }
             }
             for (int o = 16; o > 0; o >>= 1) {
                 hmax = rmax(hmax, __shfl_xor_sync(0xffffffffu, hmax, o));
                 umin = rmin(umin, __shfl_xor_sync(0xffffffffu, umin, o));
             }
-            if (threadIdx.x == 0) s_vd_bound = rmax(zlow - hmax, R(0)) * rmax(umin, R(0)) * p.inv_avd;
+            zero = __any_sync(0xffffffffu, zero);
+            if (threadIdx.x == 0) {
+                s_vd_bound = rmax(zlow - hmax, R(0)) * rmax(umin, R(0)) * p.inv_avd;
+                *s_vd_zero = zero;
+            }
         }
 
         // ---- 2. SGS inputs on the tile and its halo 1 (pde.cu:632-765).  Needed
@@ -458,7 +472,7 @@ __global__ void __launch_bounds__(NT, sizeof(R) != 4 ? 1 : NT > 256 ? 2 : (TI * 
                                     : R(0);
             R g7;
             if (lean) {
-                const R K_T = (Tc > p.T_pc) ? p.A * rexp(-fdiv(p.T_act, Tc)) : R(0);
+                const R K_T = arrhenius(p, Tc);
                 const R Yv = (gk < nzy) ? Yq : R(0);
                 const R T2 = Tc * Tc;
                 g7 = p.mu_Trho * ((p.c12 * T2 * (Tx * Tx + Ty * Ty + Tz * Tz) + (p.kT + p.c4 * (T2 * Tc)) * (Txx + Tyy + Tzz)) *
@@ -648,15 +662,53 @@ __global__ void __launch_bounds__(NT, sizeof(R) != 4 ? 1 : NT > 256 ? 2 : (TI * 
                     R mu_kp = t.G(0, ii, jj, kk + 1), mu_km = t.G(0, ii, jj, kk - 1);
                     // Van Driest factors; where the bound shows them all to be
                     // exactly 1 the products would not change mu
-                    if (!(s_vd_bound > VanDriestCut<R>::v * R(1.001) * nu)) {
+                    if (s_vd_bound > VanDriestCut<R>::v * R(1.001) * nu) {
+                        if (*s_vd_zero) {
+                            // columns without friction: the factor of -z_ibm * 0 * inv_avd_nu,
+                            // 1 - exp(-0) = 0 (NaN when 1/nu is not finite, as there)
+                            const R f0 = R(0) * inv_avd_nu, f00 = f0 * f0;
+                            if (t.cut_[cc] == R(0)) {
+                                mu_c *= f00;
+                                mu_kp *= f00;
+                                mu_km *= f00;
+                            }
+                            if (t.cut_[qxp] == R(0)) mu_xp *= f00;
+                            if (t.cut_[qxm] == R(0)) mu_xm *= f00;
+                            if (t.cut_[qyp] == R(0)) mu_yp *= f00;
+                            if (t.cut_[qym] == R(0)) mu_ym *= f00;
+                        }
+                    } else {
                         const R ut0 = t.cut_[cc];
-                        const R fc = van_driest(-zibm(cc, zk) * ut0 * inv_avd_nu);
-                        const R fxp_ = van_driest(-zibm(qxp, zk) * t.cut_[qxp] * inv_avd_nu);
-                        const R fxm_ = van_driest(-zibm(qxm, zk) * t.cut_[qxm] * inv_avd_nu);
-                        const R fyp_ = van_driest(-zibm(qyp, zk) * t.cut_[qyp] * inv_avd_nu);
-                        const R fym_ = van_driest(-zibm(qym, zk) * t.cut_[qym] * inv_avd_nu);
-                        const R fkm = van_driest(-zibm(cc, t.K(kk - 1, RZ)) * ut0 * inv_avd_nu);
-                        const R fkp = van_driest(-zibm(cc, t.K(kk + 1, RZ)) * ut0 * inv_avd_nu);
+                        R fc = -zibm(cc, zk) * ut0 * inv_avd_nu;
+                        R fxp_ = -zibm(qxp, zk) * t.cut_[qxp] * inv_avd_nu;
+                        R fxm_ = -zibm(qxm, zk) * t.cut_[qxm] * inv_avd_nu;
+                        R fyp_ = -zibm(qyp, zk) * t.cut_[qyp] * inv_avd_nu;
+                        R fym_ = -zibm(qym, zk) * t.cut_[qym] * inv_avd_nu;
+                        R fkm = -zibm(cc, t.K(kk - 1, RZ)) * ut0 * inv_avd_nu;
+                        R fkp = -zibm(cc, t.K(kk + 1, RZ)) * ut0 * inv_avd_nu;
+                        // A factor is exactly 1 below the cut-off and exactly 0
+                        // where -z+/A is 0 (no height above the terrain, or a
+                        // column without wall friction, as over the hills): only
+                        // a cell with another argument evaluates the exponentials.
+                        if (van_driest_needs_exp(fc) || van_driest_needs_exp(fxp_) || van_driest_needs_exp(fxm_) ||
+                            van_driest_needs_exp(fyp_) || van_driest_needs_exp(fym_) || van_driest_needs_exp(fkm) ||
+                            van_driest_needs_exp(fkp)) {
+                            fc = van_driest(fc);
+                            fxp_ = van_driest(fxp_);
+                            fxm_ = van_driest(fxm_);
+                            fyp_ = van_driest(fyp_);
+                            fym_ = van_driest(fym_);
+                            fkm = van_driest(fkm);
+                            fkp = van_driest(fkp);
+                        } else {
+                            fc = van_driest_exact(fc);
+                            fxp_ = van_driest_exact(fxp_);
+                            fxm_ = van_driest_exact(fxm_);
+                            fyp_ = van_driest_exact(fyp_);
+                            fym_ = van_driest_exact(fym_);
+                            fkm = van_driest_exact(fkm);
+                            fkp = van_driest_exact(fkp);
+                        }
                         mu_c *= fc * fc;
                         mu_xp *= fxp_ * fxp_;
                         mu_xm *= fxm_ * fxm_;
@@ -709,7 +761,7 @@ __global__ void __launch_bounds__(NT, sizeof(R) != 4 ? 1 : NT > 256 ? 2 : (TI * 
             } else if (gk < nzy) {
                 // fuel cell whose velocity and temperature the boundary rules set (top plane)
                 const R T = t.S(3, ii, jj, kk);
-                const R K_T = (T > p.T_pc) ? p.A * rexp(-fdiv(p.T_act, T)) * R(1) : R(0);
+                const R K_T = arrhenius(p, T);
                 kY = -p.Y_f * K_T * Yx;
             }
             if (ylive) {

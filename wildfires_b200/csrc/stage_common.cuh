@@ -1,5 +1,5 @@
-// stage_common.cuh -- device helpers shared by the stage kernels (stage.cu,
-// stage_pair.cu): periodic indices, the precision-dependent fast operations,
+// stage_common.cuh -- device helpers of the stage kernels (stage.cu):
+// periodic indices, the precision-dependent fast operations,
 // the temperature source terms, the RK update and the column boundary rules
 // (reference src/cu/pde.cu:14-99, 640-720; solver.cu:14-93).
 #pragma once
@@ -60,6 +60,23 @@ __device__ __forceinline__ float van_driest(float x) { return x < -17.5f ? 1.0f 
 template <class R> struct VanDriestCut;
 template <> struct VanDriestCut<double> { static constexpr double v = 37.5; };
 template <> struct VanDriestCut<float> { static constexpr float v = 17.5f; };
+// Whether van_driest(x) needs its exponential: not below the cut-off and not
+// x = +-0, where 1 - exp(x) is exactly 0 (NaN needs it, and stays NaN).
+template <class R> __device__ __forceinline__ bool van_driest_needs_exp(R x)
+{
+    return !(x < -VanDriestCut<R>::v) && !(x == R(0));
+}
+// van_driest(x) for an x that does not need the exponential: 1 or 0.
+template <class R> __device__ __forceinline__ R van_driest_exact(R x) { return x < -VanDriestCut<R>::v ? R(1) : R(0); }
+
+// Arrhenius rate A exp(-T_act/T) H(T - T_pc) (pde.cu:665): exactly 0 below
+// the phase change; a warp with no lane above it skips the exponential.
+template <class R> __device__ __forceinline__ R arrhenius(const PhysR<R> &p, R T)
+{
+    R K_T = R(0);
+    if (__any_sync(__activemask(), T > p.T_pc)) K_T = (T > p.T_pc) ? p.A * rexp(-fdiv(p.T_act, T)) : R(0);
+    return K_T;
+}
 
 // Temperature source terms (pde.cu:664-711).
 template <class R> struct Thermo {
@@ -76,8 +93,7 @@ __device__ __forceinline__ Thermo<R> thermo(const PhysR<R> &p, int suth_mu, int 
 {
     Thermo<R> o;
     R mu = p.mu, kT = p.kT, dk = R(0);
-    // Arrhenius rate A exp(-T_act/T) H(T - T_pc); exactly 0 below the phase change
-    o.K_T = (T > p.T_pc) ? p.A * rexp(-fdiv(p.T_act, T)) * R(1) : R(0);
+    o.K_T = arrhenius(p, T);
     R Y = R(0), T_gas = p.T_inf, T_solid = p.T_inf;
     if (k <= nzy) {
         if (k < nzy) Y = Yc;
