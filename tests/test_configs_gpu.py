@@ -9,7 +9,13 @@ sensitivity to a 1e-15 relative change of the initial temperature (the gate
 tests/test_reference_gpu.py applies to C1).  The line fire on the hill
 amplifies rounding differences by about 1.5x per step (measured on the B200:
 relative L2 4e-9 and L-inf 2.4e-6 in T against the reference after 40
-steps), so the predictable horizon here is 10 steps.
+steps), so the predictable horizon here is 10 steps.  By step 500 the
+divergence has saturated: the reference and runs from perturbed initial
+temperatures all differ from this path by about 0.37% relative L2 in T, so
+the reference is one more draw from the spread the perturbed runs sample.
+The max of S such draws is exceeded by a further one with probability
+1/(S+1); the gate is therefore the max over three perturbations plus 10%
+(a real defect shows as an order of magnitude or more).
 
 C3 -- 512 x 512 x 128, eight seeded hills: the FP32 stencil path (the
 benchmark's chosen form) against the plain FP64 path, every field within 1e-5
@@ -75,16 +81,17 @@ def test_c2_hill_fp64_after_500_steps_within_model_sensitivity():
     P = res["P"]
     y = _run(P, res["y0"], res["p0"], 500)
     N = P.rec.Nx * P.rec.Ny * P.rec.Nz
-    own = {f: 0.0 for f in "uvwT"}
-    for seed in (0, 1):
+    draws = []
+    for seed in (0, 1, 2):
         yp0 = res["y0"].copy()
         yp0[3 * N:4 * N] *= 1 + 1e-15 * np.random.default_rng(seed).standard_normal(N)
         e = _errors(P, _run(P, yp0, res["p0"], 500), y)
-        own = {f: max(own[f], e[f][1]) for f in "uvwT"}
+        draws.append({f: e[f][1] for f in "uvwT"})
+    own = {f: max(d[f] for d in draws) for f in "uvwT"}
     vs_ref = _errors(P, y, res["y"])
-    print("C2 500 steps: vs reference", {f: vs_ref[f][1] for f in "uvwT"}, "own sensitivity", own)
+    print("C2 500 steps: vs reference", {f: vs_ref[f][1] for f in "uvwT"}, "perturbed runs", draws)
     for f in "uvwT":
-        assert vs_ref[f][1] <= max(own[f], 1e-10), (f, vs_ref[f], own[f])
+        assert vs_ref[f][1] <= max(1.1 * own[f], 1e-10), (f, vs_ref[f], own[f])
 
 
 def _c3(Nt):
