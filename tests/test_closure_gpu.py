@@ -97,7 +97,10 @@ def test_tensor_core_inference_matches_oracle():
         F = closure.features(u, v, w, T, r.dx, r.dy, P.z())
         ref = _oracle_predict(th, F.reshape(-1, 12))
         rel = np.abs(c - ref) / np.maximum(np.abs(ref), 1e-3)
-        assert np.median(rel) <= 5e-3 and rel.max() <= 5e-2, (prec, np.median(rel), rel.max())
+        print("state inference vs oracle", prec, np.median(rel), np.percentile(rel, 99.9), rel.max())
+        # BF16 operands (8-bit significands) through two 64-wide layers; measured on
+        # the B200: median 3.3e-4, 99.9th percentile 1.4e-2, max 1.8e-2
+        assert np.median(rel) <= 2.5e-3 and rel.max() <= 3e-2, (prec, np.median(rel), rel.max())
 
 
 def test_smagorinsky_weights_reproduce_the_smagorinsky_path():
@@ -129,7 +132,9 @@ def test_feature_rows_inference_matches_oracle():
     c = closure.predict(th, X)
     ref = _oracle_predict(th, X)
     rel = np.abs(c - ref) / np.maximum(np.abs(ref), 1e-3)
-    assert np.median(rel) <= 5e-3 and rel.max() <= 5e-2, (np.median(rel), rel.max())
+    print("feature-row inference vs oracle", np.median(rel), np.percentile(rel, 99.9), rel.max())
+    # measured on the B200: median 1.3e-3, 99.9th percentile 9.4e-3, max 1.4e-2
+    assert np.median(rel) <= 2.5e-3 and rel.max() <= 3e-2, (np.median(rel), rel.max())
 
 
 def test_timed_out_wait_reports_and_recovers():
