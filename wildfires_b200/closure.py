@@ -177,10 +177,10 @@ def _unpack(P, y):
     return [y[q * N:(q + 1) * N].reshape(sh) for q in range(4)]
 
 
-def fine_snapshots(seed, Nc, steps, every, precision="fp32"):
-    """Yield (step, u, v, w, T) of the fine run every `every` steps."""
+def fine_snapshots(seed, Nc, steps, every, precision="fp32", **kw):
+    """Yield (step, u, v, w, T) of the fine run every `every` steps (kw: study_case)."""
     from . import Solver, configs
-    P, y0, p0 = configs.materialize(study_case(Nc, fine=True, seed=seed, Nt=steps))
+    P, y0, p0 = configs.materialize(study_case(Nc, fine=True, seed=seed, Nt=steps, **kw))
     with Solver(P, precision) as s:
         s.upload(y0, p0)
         for n in range(every, steps + 1, every):
@@ -189,16 +189,16 @@ def fine_snapshots(seed, Nc, steps, every, precision="fp32"):
             yield n, P, y
 
 
-def dataset(seeds, Nc=(33, 33, 9), steps=120, every=12):
+def dataset(seeds, Nc=(33, 33, 9), steps=120, every=12, **kw):
     """Features (unnormalised) and targets at interior coarse nodes (samples
-    with a non-finite value are dropped)."""
+    with a non-finite value are dropped; kw: study_case)."""
     from . import configs
-    Pc, _, _ = configs.materialize(study_case(Nc, seed=0, Nt=1))
+    Pc, _, _ = configs.materialize(study_case(Nc, seed=0, Nt=1, **kw))
     r = Pc.rec
     zc = Pc.z()
     X, Yt = [], []
     for sd in seeds:
-        for n, Pf, y in fine_snapshots(sd, Nc, steps, every):
+        for n, Pf, y in fine_snapshots(sd, Nc, steps, every, **kw):
             uf, vf, wf, Tf = _unpack(Pf, y)
             F = features(box_filter(uf), box_filter(vf), box_filter(wf), box_filter(Tf), r.dx, r.dy, zc)
             c = targets(uf, vf, wf, r.dx, r.dy, zc)
@@ -254,19 +254,20 @@ def burned_fraction(P, y, y0):
     return float(1.0 - y[4 * N:].sum() / y0[4 * N:].sum())
 
 
-def evaluate(th, seed=100, Nc=(33, 33, 9), steps=120, precision="fp32"):
-    """Coarse runs with Smagorinsky and with the network against the filtered fine run."""
+def evaluate(th, seed=100, Nc=(33, 33, 9), steps=120, precision="fp32", **kw):
+    """Coarse runs with Smagorinsky and with the network against the filtered
+    fine run (kw: study_case)."""
     import ctypes as C
     from . import Solver, configs
     from ._abi import check, lib
-    Pf, yf0, pf0 = configs.materialize(study_case(Nc, fine=True, seed=seed, Nt=steps))
+    Pf, yf0, pf0 = configs.materialize(study_case(Nc, fine=True, seed=seed, Nt=steps, **kw))
     t0 = time.perf_counter()
     with Solver(Pf, precision) as s:
         s.upload(yf0, pf0)
         s.step(steps)
         yf, _ = s.download()
     t_fine = time.perf_counter() - t0
-    Pc, yc0, pc0 = configs.materialize(study_case(Nc, seed=seed, Nt=steps))
+    Pc, yc0, pc0 = configs.materialize(study_case(Nc, seed=seed, Nt=steps, **kw))
     truth = np.concatenate([box_filter(q).reshape(-1) for q in _unpack(Pf, yf)])
     rc = Pc.rec
     Nc_ = rc.Nx * rc.Ny * rc.Nz
@@ -291,7 +292,7 @@ def evaluate(th, seed=100, Nc=(33, 33, 9), steps=120, precision="fp32"):
     return out
 
 
-def cost_study(th, Nc=(65, 65, 17), steps=40, precision="fp32"):
+def cost_study(th, Nc=(65, 65, 17), steps=40, precision="fp32", **kw):
     """Cost of the 4x refinement at a size where the GPU, not launch latency,
     sets the pace: seconds per step of the fine run and of the coarse run
     with Smagorinsky and with the network, the same time step for both (the
@@ -304,7 +305,7 @@ def cost_study(th, Nc=(65, 65, 17), steps=40, precision="fp32"):
     out = {"coarse_grid": list(Nc), "fine_grid": [FACTOR * (n - 1) + 1 for n in Nc], "steps": steps}
     runs = (("fine", True, None), ("smagorinsky", False, None), ("mlp", False, th))
     for name, fine, params in runs:
-        P, y0, p0 = configs.materialize(study_case(Nc, fine=fine, seed=100, Nt=steps))
+        P, y0, p0 = configs.materialize(study_case(Nc, fine=fine, seed=100, Nt=steps, **kw))
         with Solver(P, precision) as s:
             if params is not None:
                 p = np.ascontiguousarray(params, dtype=np.float32)
@@ -322,20 +323,45 @@ def cost_study(th, Nc=(65, 65, 17), steps=40, precision="fp32"):
 
 
 def main(argv=None):
-    """python -m wildfires_b200.closure [out.npz]: build the dataset from fine
-    runs (seeds 0-2), train, evaluate on seed 100, save the parameters."""
+    """python -m wildfires_b200.closure [out.npy] [--coarse NX,NY,NZ] [--steps N]
+    [--gust G]: build the dataset from fine runs (seeds 0-2, a snapshot every
+    tenth of the horizon), train, score a priori and a posteriori on seed 100,
+    time the refinement at the same size, save the parameters."""
+    import argparse
     import json
-    argv = sys.argv[1:] if argv is None else argv
-    path = argv[0] if argv else "closure_params.npy"
-    X, y = dataset([0, 1, 2])
-    th, hist = train(X, y)
-    np.save(path, th)
-    res = evaluate(th)
-    res["cost"] = cost_study(th)
-    res["train"] = {"samples": int(len(y)), "loss_first": float(hist[0]), "loss_last": float(hist[-1]),
+    ap = argparse.ArgumentParser(prog="python -m wildfires_b200.closure")
+    ap.add_argument("out", nargs="?", default="closure_params.npy")
+    ap.add_argument("--coarse", default="33,33,9", help="coarse grid nodes; the fine grid has 4x the intervals")
+    ap.add_argument("--steps", type=int, default=120)
+    ap.add_argument("--gust", type=float, default=1.0, help="fine-scale velocity fluctuations, m/s")
+    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--batch", type=int, default=8192)
+    args = ap.parse_args(sys.argv[1:] if argv is None else argv)
+    Nc = tuple(int(v) for v in args.coarse.split(","))
+    every = max(args.steps // 10, 1)
+    kw = {"gust": args.gust}
+    X, y = dataset([0, 1, 2], Nc, args.steps, every, **kw)
+    th, hist = train(X, y, steps=args.train_steps, batch=args.batch)
+    np.save(args.out, th)
+    # a priori on the held-out seed: the solver's tensor-core inference against c*
+    Xh, yh = dataset([100], Nc, args.steps, every, **kw)
+    c = predict(th, Xh)
+    cs2 = float(configs_C_s()) ** 2
+    res = evaluate(th, 100, Nc, args.steps, **kw)
+    res["apriori"] = {"mse_network": float(np.mean((c - yh) ** 2)), "mse_smagorinsky": float(np.mean((cs2 - yh) ** 2)),
+                      "mse_best_constant": float(np.var(yh)), "samples": int(len(yh))}
+    res["cost"] = cost_study(th, Nc, **kw)
+    res["train"] = {"samples": int(len(y)), "loss_first": float(hist[0]), "loss_last": float(np.mean(hist[-50:])),
                     "target_mean": float(y.mean())}
+    res["case"] = {"coarse": list(Nc), "steps": args.steps, "gust": args.gust}
     print(json.dumps(res))
     return res
+
+
+def configs_C_s():
+    """The Smagorinsky constant of the study cases."""
+    from . import configs
+    return configs.base_params(9, 9, 9, 1, 1.0, 1.0, 1.0, 1.0)["C_s"]
 
 
 if __name__ == "__main__":
