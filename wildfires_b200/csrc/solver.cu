@@ -1262,9 +1262,13 @@ template <class R> wf_status tune_tiles_impl(wf_ctx *c)
     void *in = c->ybuf[c->cur], *scratch = c->Xa ? c->Xa : c->ybuf[1 - c->cur];
     const int saved = c->method;
     c->method = 3;
-    cudaEvent_t e0, e1;
-    WF_TRY_CUDA(cudaEventCreate(&e0));
-    WF_TRY_CUDA(cudaEventCreate(&e1));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        c->method = saved;
+        set_error("stage tile tuning: %s", cudaGetErrorString(cudaGetLastError()));
+        return WF_ERR_CUDA;
+    }
     float best = 1e30f;
     int pick = 0;
     cudaError_t err = cudaSuccess;
@@ -1514,8 +1518,15 @@ wf_status wf_profile_phases(wf_ctx *c, int nsteps, double *ms, int *launches)
     if (const wf_status st0 = settle_p(c)) return st0;
     for (int q = 0; q < WF_NPHASES; q++) { ms[q] = 0.0; launches[q] = 0; }
     const int maxev = 2 + 3 * 4 + 5 * (c->P.pressure_solver_iter > 1 ? c->P.pressure_solver_iter : 1);
-    std::vector<cudaEvent_t> ev(maxev);
-    for (auto &e : ev) WF_TRY_CUDA(cudaEventCreate(&e));
+    std::vector<cudaEvent_t> ev(maxev, nullptr);
+    for (auto &e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            e = nullptr;
+            for (auto &d : ev)
+                if (d) cudaEventDestroy(d);
+            set_error("wf_profile_phases: %s", cudaGetErrorString(cudaGetLastError()));
+            return WF_ERR_CUDA;
+        }
     wf_status st = WF_OK;
     for (int it = 0; it < nsteps && st == WF_OK; it++) {
         int ne = 0;
