@@ -154,3 +154,51 @@ def test_rader_plan_slots_are_a_permutation(plan):
     outs = sorted(((k1 * e1) + pmap[P + s]) % (N1 * P) for k1 in range(N1) for s in range(P - 1))
     outs += [k1 * e1 % (N1 * P) for k1 in range(N1)]
     assert sorted(outs) == list(range(N1 * P))
+
+
+def slot_tables(N1, P, F1, F2, F3):
+    """The slot table of the slotted run (plan_pr in wildfires_b200/csrc/solver.cu):
+    input x[j] at n1 SS + u for j = N1 map[u] + P n1 (mod n); output X[k] at
+    m1 UB + u (u = k1 M L + w) or, for the DC term of k1, at F1 UB + k1."""
+    n = N1 * P
+    pmap, _, e1, M, L = tables(N1, P, F1, F2, F3)
+    SS = P + ((M * L - P) % 8 + 8) % 8
+    UB = N1 * M * L
+    ins, outs = [-1] * n, [-1] * n
+    for u in range(P):
+        for n1 in range(N1):
+            ins[(N1 * pmap[u] + P * n1) % n] = n1 * SS + u
+    for k1 in range(N1):
+        kb = k1 * e1 % n
+        for w in range(M * L):
+            for m1 in range(F1):
+                outs[(kb + pmap[P + w + M * L * m1]) % n] = m1 * UB + k1 * M * L + w
+        outs[kb] = F1 * UB + k1
+    return ins, outs, SS, UB
+
+
+@pytest.mark.parametrize("plan", PLANS, ids=lambda p: "n%d" % (p[0] * p[1]))
+def test_slot_tables_are_the_passes_permutations(plan):
+    """Every input lands on the slot pass A reads for it (distinct slots inside
+    the N1 sub-lines), and every output slot is the one pass B3 posts that
+    output to (each of the n slots exactly once)."""
+    N1, P, F1 = plan[0], plan[1], plan[2]
+    n = N1 * P
+    ins, outs, SS, UB = slot_tables(*plan)
+    assert min(ins) >= 0 and len(set(ins)) == n and max(ins) < N1 * SS
+    assert sorted(outs) == list(range(n))
+    pmap, _, e1, M, L = tables(*plan)
+    # pass A's gather: slot n1 SS + u holds x[N1 map[u] + P n1]
+    for j in range(n):
+        n1, u = divmod(ins[j], SS)
+        assert (N1 * pmap[u] + P * n1) % n == j
+    # pass B3's scatter: slot m1 UB + u is the output the unit (k1, w) =
+    # divmod(u, M L) posts for m1, slot F1 UB + k1 the DC term of k1
+    for k in range(n):
+        s = outs[k]
+        if s < F1 * UB:
+            m1, u = divmod(s, UB)
+            k1, w = divmod(u, M * L)
+            assert (k1 * e1 + pmap[P + w + M * L * m1]) % n == k
+        else:
+            assert (s - F1 * UB) * e1 % n == k

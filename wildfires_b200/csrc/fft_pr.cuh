@@ -184,8 +184,13 @@ struct PrPlan {
     // Forward DFT (INV: exp(+2 pi i jk/n), unnormalised) of the line at buf,
     // by the 32 lanes of one warp.  pre(idx) supplies x[idx] (idx < n) and is
     // called before the first write to buf; post(idx, X) receives X[idx] after
-    // the last read of buf, so pre may read and post may write buf.
-    template <bool INV, class Pre, class Post>
+    // the last read of buf, so pre may read and post may write buf.  SLOT: pre
+    // and post take the slots of the plan's slot table instead (input x[j] at
+    // n1 SS + u, output X[k] at m1 UB + u or F1 UB + k1), which a warp's lanes
+    // visit contiguously: a caller that stores its line in that order in shared
+    // memory (the permutations moved into its copies) reads and writes it
+    // without bank conflicts.
+    template <bool INV, bool SLOT = false, class Pre, class Post>
     __device__ __forceinline__ static void run(const PrTables &t, double2 *buf, int lane, Pre pre, Post post)
     {
         // pass A
@@ -195,14 +200,21 @@ struct PrPlan {
             for (int r = 0; r < RA; r++) {
                 const int u = lane + 32 * r;
                 if (u < P) {
-                    const int base = N1 * __ldg(t.map + u);
+                    if constexpr (SLOT) {
 #pragma unroll
-                    for (int n1 = 0; n1 < N1; n1++) {
-                        int idx = base + P * n1;
-                        if (idx >= n) idx -= n;
-                        v[r][n1] = pre(idx);
-                        if (INV) v[r][n1].y = -v[r][n1].y;
+                        for (int n1 = 0; n1 < N1; n1++) v[r][n1] = pre(n1 * SS + u);
+                    } else {
+                        const int base = N1 * __ldg(t.map + u);
+#pragma unroll
+                        for (int n1 = 0; n1 < N1; n1++) {
+                            int idx = base + P * n1;
+                            if (idx >= n) idx -= n;
+                            v[r][n1] = pre(idx);
+                        }
                     }
+#pragma unroll
+                    for (int n1 = 0; n1 < N1; n1++)
+                        if (INV) v[r][n1].y = -v[r][n1].y;
                 }
             }
             __syncwarp();
@@ -325,15 +337,20 @@ struct PrPlan {
                     const int *km = t.map + P + w;
 #pragma unroll
                     for (int m1 = 0; m1 < F1; m1++) {
-                        int idx = kb + __ldg(km + M * L * m1);
-                        if (idx >= n) idx -= n;
+                        int idx;
+                        if constexpr (SLOT) {
+                            idx = m1 * UB + u;
+                        } else {
+                            idx = kb + __ldg(km + M * L * m1);
+                            if (idx >= n) idx -= n;
+                        }
                         // conj of the IDFT trick, and of the inverse transform
                         const double2 x = v[r][m1];
                         post(idx, INV ? x : make_double2(x.x, -x.y));
                     }
                     if (w == 0) {
                         const double2 x = x0[r];
-                        post(kb, INV ? make_double2(x.x, -x.y) : x);
+                        post(SLOT ? F1 * UB + k1 : kb, INV ? make_double2(x.x, -x.y) : x);
                     }
                 }
             }

@@ -366,6 +366,12 @@ struct EngPR {
     {
         Plan::template run<INV>(fft::PrTables{d.prb, d.prmap, d.pr_e1}, buf, jj, pre, post);
     }
+    // the same on a line stored in the plan's slot order (d.prslot)
+    template <bool INV, class Pre, class Post>
+    __device__ __forceinline__ static void run_slotted(const FftDesc &d, double2 *buf, int jj, Pre pre, Post post)
+    {
+        Plan::template run<INV, true>(fft::PrTables{d.prb, d.prmap, d.pr_e1}, buf, jj, pre, post);
+    }
 };
 
 // which engine a kernel instantiation got, and the power-of-two engine's log2 length
@@ -547,7 +553,10 @@ __global__ void __launch_bounds__(256, kFftMinBlocks)
 // lines (consecutive s, one warp each) into shared memory, each warp
 // transforms its line with no block barrier, and the block writes the lines
 // back.  Both copies move 128 contiguous bytes per 8 threads (LB = 8 lines of
-// 16-byte values); LS = 1 (mod 8) keeps the shared-memory side conflict-free.
+// 16-byte values); LS = 1 (mod 8) keeps the shared-memory side conflict-free
+// whatever the position within a line, so the copies also apply the engine's
+// input and output permutations (fx.prslot) and the transform itself reads
+// and writes its line contiguously (the slotted run).
 template <class E, bool INV>
 __global__ void __launch_bounds__(256, 2) k_p_fftx_pr(double2 *__restrict__ G, const FftDesc fx, int n0, int h1)
 {
@@ -557,9 +566,10 @@ __global__ void __launch_bounds__(256, 2) k_p_fftx_pr(double2 *__restrict__ G, c
     const int s0 = blockIdx.x * LB;
     const int nl = min(LB, h1 - s0);
     double2 *g = G + (size_t)blockIdx.y * n0 * h1 + s0;
+    const int *__restrict__ slot = fx.prslot;
     for (int e = threadIdx.x; e < LB * n0; e += 256) {
         const int l = e % LB, idx = e / LB;
-        if (l < nl) cp_async16(smem + l * LS + idx, g + (size_t)idx * h1 + l, true);
+        if (l < nl) cp_async16(smem + l * LS + __ldg(slot + idx), g + (size_t)idx * h1 + l, true);
     }
     cp_async_commit();
     cp_async_wait<0>();
@@ -567,13 +577,13 @@ __global__ void __launch_bounds__(256, 2) k_p_fftx_pr(double2 *__restrict__ G, c
     const int q = E::line(threadIdx.x);
     if (q < nl) {
         double2 *buf = smem + q * LS;
-        E::template run<INV>(
-            fx, buf, E::lane(threadIdx.x), [&](int idx) { return buf[idx]; }, [&](int idx, double2 v) { buf[idx] = v; });
+        E::template run_slotted<INV>(
+            fx, buf, E::lane(threadIdx.x), [&](int sl) { return buf[sl]; }, [&](int sl, double2 v) { buf[sl] = v; });
     }
     __syncthreads();
     for (int e = threadIdx.x; e < LB * n0; e += 256) {
         const int l = e % LB, idx = e / LB;
-        if (l < nl) g[(size_t)idx * h1 + l] = smem[l * LS + idx];
+        if (l < nl) g[(size_t)idx * h1 + l] = smem[l * LS + __ldg(slot + n0 + idx)];
     }
 }
 
@@ -824,6 +834,7 @@ struct LaunchFx {
                                            const int &h1, cudaStream_t &s)
     {
         if constexpr (kIsPR<E>) {
+            if (!fx.prslot) return cudaErrorInvalidValue;   // every compiled plan has its slot table
             k_p_fftx_pr<E, INV><<<dim3((h1 + E::LB - 1) / E::LB, nslices), 256, E::smem_bytes, s>>>(G, fx, n0, h1);
         } else {
             constexpr int L = kLog2<E>;
@@ -885,6 +896,12 @@ bool pr_plan_of(PlanList<Pl...>, int n, int f[5])
 }  // namespace
 
 bool poisson_pr_plan(int n, int f[5]) { return pr_plan_of(PrPlans{}, n, f); }
+
+template <class... Pl> bool pr_layout_of(PlanList<Pl...>, int n, int *ss, int *ub)
+{
+    return ((n == Pl::n ? (*ss = Pl::SS, *ub = Pl::UB, true) : false) || ...);
+}
+bool poisson_pr_layout(int n, int *ss, int *ub) { return pr_layout_of(PrPlans{}, n, ss, ub); }
 
 template <class R> cudaError_t poisson_set_attributes()
 {

@@ -45,7 +45,7 @@ const long double kPiL = 3.141592653589793238462643383279502884L;
 struct HostFft {
     FftDesc d;
     std::vector<double2> tw, chirp, filt, prb;
-    std::vector<int> prmap;
+    std::vector<int> prmap, prslot;
 };
 
 long long pow_mod(long long b, long long e, long long m)
@@ -125,6 +125,28 @@ void plan_pr(HostFft &h, const int f[5])
                 }
                 h.prb[(j1 * M + jm) * L + jl] = make_double2((double)(sr / Q), (double)(si / Q));
             }
+    // Slots of the engine's slotted run (a kernel that stages whole lines in
+    // shared memory applies both permutations in its copies): input x[j] at
+    // n1 SS + u for j = N1 map[u] + P n1 (mod n), the pass-A gather; output
+    // X[k] at m1 UB + u (k = k1 e1 + map[P + w + M L m1], u = k1 M L + w) or,
+    // for the DC terms k = k1 e1, at F1 UB + k1, the pass-B3 scatter.
+    int SS = 0, UB = 0;
+    if (poisson_pr_layout(n, &SS, &UB)) {
+        h.prslot.assign(2 * (size_t)n, -1);
+        for (int u = 0; u < P; u++)
+            for (int n1 = 0; n1 < N1; n1++) h.prslot[((long long)N1 * h.prmap[u] + (long long)P * n1) % n] = n1 * SS + u;
+        const int ML = M * L;
+        for (int k1 = 0; k1 < N1; k1++) {
+            const int kb = (int)(((long long)k1 * h.d.pr_e1) % n);
+            for (int w = 0; w < ML; w++)
+                for (int m1 = 0; m1 < F1; m1++)
+                    h.prslot[n + (kb + h.prmap[P + w + ML * m1]) % n] = m1 * UB + k1 * ML + w;
+            h.prslot[n + kb] = F1 * UB + k1;
+        }
+        bool full = true;
+        for (int v : h.prslot) full = full && v >= 0;
+        if (!full) h.prslot.clear();   // not a permutation: no slot table, and the x kernel refuses the plan
+    }
     h.d.pr = 1;
 }
 
@@ -350,10 +372,13 @@ wf_status upload_fft(wf_ctx *c, const HostFft &h, FftDesc &d)
     if (h.d.pr) {
         double2 *rb = nullptr;
         int *map = nullptr;
+        int *slot = nullptr;
         wf_status s = upload(c, &rb, h.prb.data(), h.prb.size());
         if (!s) s = upload(c, &map, h.prmap.data(), h.prmap.size());
+        if (!s && !h.prslot.empty()) s = upload(c, &slot, h.prslot.data(), h.prslot.size());
         d.prb = rb;
         d.prmap = map;
+        d.prslot = slot;
         return s;
     }
     double2 *tw = nullptr, *ch = nullptr, *fl = nullptr;

@@ -199,10 +199,13 @@ struct FftDesc {
     const double2 *prb;     // Rader: DFT of the root-power filter / (P-1), (j1, j2) order
     const int *prmap;       // Rader: input slot map [P] and output index map [P-1]
     int pr_e1;              // Rader: CRT weight of the N1 residue
+    const int *prslot;      // Rader: [n] shared-memory slot of input j, [n] slot of output k (slotted run)
 };
 // Prime-factor + Rader plan compiled for length n: f = {N1, P, F1, F2, F3} with
 // n = N1 P, P prime, P - 1 = F1 F2 F3.  False for every other length.
 bool poisson_pr_plan(int n, int f[5]);
+// Line layout of that plan: sub-line stride SS and the B1 / B3 unit count UB.
+bool poisson_pr_layout(int n, int *ss, int *ub);
 
 template <class R>
 struct PoissonArgs {
