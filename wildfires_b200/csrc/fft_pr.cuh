@@ -193,28 +193,41 @@ struct PrPlan {
     template <bool INV, bool SLOT = false, class Pre, class Post>
     __device__ __forceinline__ static void run(const PrTables &t, double2 *buf, int lane, Pre pre, Post post)
     {
-        // pass A
-        {
+        // pass A.  Slotted, a lane reads and writes the same slots (j SS + u for
+        // its u), so it transforms one round at a time; in the plain run its
+        // writes may land on inputs other lanes have yet to read, so all reads
+        // come first.
+        if constexpr (SLOT) {
+#pragma unroll
+            for (int r = 0; r < RA; r++) {
+                const int u = lane + 32 * r;
+                if (u < P) {
+                    double2 v[N1];
+#pragma unroll
+                    for (int n1 = 0; n1 < N1; n1++) {
+                        v[n1] = pre(n1 * SS + u);
+                        if (INV) v[n1].y = -v[n1].y;
+                    }
+                    dft_odd<N1>(v);
+#pragma unroll
+                    for (int k1 = 0; k1 < N1; k1++) buf[k1 * SS + u] = v[k1];
+                }
+            }
+            __syncwarp();
+        } else {
             double2 v[RA][N1];
 #pragma unroll
             for (int r = 0; r < RA; r++) {
                 const int u = lane + 32 * r;
                 if (u < P) {
-                    if constexpr (SLOT) {
+                    const int base = N1 * __ldg(t.map + u);
 #pragma unroll
-                        for (int n1 = 0; n1 < N1; n1++) v[r][n1] = pre(n1 * SS + u);
-                    } else {
-                        const int base = N1 * __ldg(t.map + u);
-#pragma unroll
-                        for (int n1 = 0; n1 < N1; n1++) {
-                            int idx = base + P * n1;
-                            if (idx >= n) idx -= n;
-                            v[r][n1] = pre(idx);
-                        }
-                    }
-#pragma unroll
-                    for (int n1 = 0; n1 < N1; n1++)
+                    for (int n1 = 0; n1 < N1; n1++) {
+                        int idx = base + P * n1;
+                        if (idx >= n) idx -= n;
+                        v[r][n1] = pre(idx);
                         if (INV) v[r][n1].y = -v[r][n1].y;
+                    }
                 }
             }
             __syncwarp();

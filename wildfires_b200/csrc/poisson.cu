@@ -354,7 +354,7 @@ struct EngPR {
     // y kernels: three blocks per SM (80 registers, a few hundred bytes spilled)
     // measured faster than two at 128 registers (source 0.465 -> 0.396 ms,
     // inverse 0.268 -> 0.246 ms at 512x512x128); the x kernel keeps two (at
-    // three, 184 bytes spilled: 0.196 / 0.190 -> 0.211 / 0.206 ms)
+    // three, 88-184 bytes spilled, it measured 2-8% slower in every form)
     static constexpr int kMinBlocks = 3;
     static constexpr int LB = Plan::LB, LS = Plan::LS;
     static constexpr size_t smem_bytes = Plan::smem_bytes;
