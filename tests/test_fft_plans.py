@@ -6,8 +6,10 @@ and N1 Rader transforms of the prime P, whose cyclic convolutions of length
 P - 1 = F1 F2 F3 are Good-Thomas transforms over the factors.  This test
 restates the same index maps and the same passes in numpy, slot by slot in the
 engine's shared-memory layout, and holds the result to numpy's FFT for every
-compiled plan, forward and inverse; so the plan arithmetic is pinned without a
-GPU (the GPU tests hold the engine itself to the oracle).
+compiled plan, forward and inverse, in the plain run and in the slotted run the
+x transform uses (its copies place the line in the slot table's order); so the
+plan arithmetic is pinned without a GPU (the GPU tests hold the engine itself
+to the oracle).
 """
 import os
 import re
@@ -77,13 +79,20 @@ def tables(N1, P, F1, F2, F3):
     return pmap, rb, e1, M, L
 
 
-def engine(x, N1, P, F1, F2, F3, inverse=False):
-    """The engine's passes on a line buffer laid out as in shared memory."""
+def engine(x, N1, P, F1, F2, F3, inverse=False, slotted=False):
+    """The engine's passes on a line buffer laid out as in shared memory.
+    slotted: the line arrives in the slot table's order (input x[j] at its
+    slot) and leaves in it (X[k] at its slot), as the x kernel stages it;
+    pass A then reads slot n1 SS + u and B3 writes slot m1 UB + u."""
     n = N1 * P
     pmap, rb, e1, M, L = tables(N1, P, F1, F2, F3)
     SS = P + ((M * L - P) % 8 + 8) % 8
+    UB = N1 * M * L
     buf = np.zeros(max(n, N1 * SS) + 8, complex)
     xin = np.conj(x) if inverse else x.copy()
+    if slotted:
+        ins, outs, _, _ = slot_tables(N1, P, F1, F2, F3)
+        buf[ins] = xin
     D = np.fft.fft
 
     def ID(v):
@@ -93,7 +102,10 @@ def engine(x, N1, P, F1, F2, F3, inverse=False):
         return k1 * SS + 1 + (a * M + bm) * L + cl
 
     for u in range(P):                                         # pass A: DFT_N1
-        v = D(np.array([xin[(N1 * pmap[u] + P * n1) % n] for n1 in range(N1)]))
+        if slotted:                                            # one round at a time, own slots
+            v = D(np.array([buf[n1 * SS + u] for n1 in range(N1)]))
+        else:
+            v = D(np.array([xin[(N1 * pmap[u] + P * n1) % n] for n1 in range(N1)]))
         for k1 in range(N1):
             buf[k1 * SS + u] = v[k1]
     for k1 in range(N1):
@@ -121,6 +133,7 @@ def engine(x, N1, P, F1, F2, F3, inverse=False):
                 idx = [pos(k1, j1, jm, ml) for jm in range(M)]
                 buf[idx] = ID(buf[idx])
     out = np.zeros(n, complex)
+    slots = np.zeros(n, complex)
     for k1 in range(N1):                                       # B3: IDFT_F1, outputs
         kb = k1 * e1 % n
         for mm in range(M):
@@ -129,17 +142,20 @@ def engine(x, N1, P, F1, F2, F3, inverse=False):
                 for m1 in range(F1):
                     k = (kb + pmap[P + (m1 * M + mm) * L + ml]) % n
                     out[k] = np.conj(y[m1]) if inverse else y[m1]
+                    slots[m1 * UB + k1 * M * L + mm * L + ml] = out[k]
         out[kb] = np.conj(buf[k1 * SS]) if inverse else buf[k1 * SS]
-    return out
+        slots[F1 * UB + k1] = out[kb]
+    return slots[outs] if slotted else out
 
 
+@pytest.mark.parametrize("slotted", [False, True], ids=["plain", "slotted"])
 @pytest.mark.parametrize("plan", PLANS, ids=lambda p: "n%d" % (p[0] * p[1]))
-def test_rader_plan_matches_numpy_fft(plan):
+def test_rader_plan_matches_numpy_fft(plan, slotted):
     n = plan[0] * plan[1]
     rng = np.random.default_rng(n)
     x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
-    fwd = engine(x, *plan)
-    inv = engine(x, *plan, inverse=True)
+    fwd = engine(x, *plan, slotted=slotted)
+    inv = engine(x, *plan, inverse=True, slotted=slotted)
     assert np.max(np.abs(fwd - np.fft.fft(x))) <= 1e-13 * np.max(np.abs(fwd))
     assert np.max(np.abs(inv - n * np.fft.ifft(x))) <= 1e-13 * np.max(np.abs(inv))
 
