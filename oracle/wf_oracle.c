@@ -1,7 +1,7 @@
 /*
  * wf_oracle.c -- CPU restatement (FP64) of the reference time step.
  *
- * TEST INFRASTRUCTURE ONLY: the checker for the GPU path.  See wf_oracle.h for
+ * TEST INFRASTRUCTURE ONLY: the oracle of the GPU path's tests.  See wf_oracle.h for
  * the contract and the list of deliberate differences.  Every function cites
  * the reference file:line whose arithmetic it restates; expression shapes are
  * kept close to the reference so rounding stays comparable.

@@ -2,7 +2,7 @@
  * wf_oracle.h -- CPU restatement (FP64) of the reference's coupled
  * atmosphere-wildfire time step.
  *
- * TEST INFRASTRUCTURE ONLY.  This is the checker the GPU kernels are compared
+ * TEST INFRASTRUCTURE ONLY.  This is the oracle the GPU kernels are compared
  * against.  It is called from tests/, from __graft_entry__.smoke() and from
  * bench.py's CPU-baseline leg, never from the product library.
  *

@@ -327,7 +327,7 @@ def write_case(case, directory, P=None, input_subdir="in/"):
     """Write parameters.txt and the initial fields (for the reference driver).
 
     The parameter file points input_path at ``input_subdir`` (relative to the
-    directory the driver runs in).  Returns the parameter-file path."""
+    directory the reference driver program runs in).  Returns the parameter-file path."""
     from . import read_parameters
     os.makedirs(directory, exist_ok=True)
     params = dict(case.params)

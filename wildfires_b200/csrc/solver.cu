@@ -982,7 +982,7 @@ wf_status wf_create(const Parameters *P, int precision, wf_ctx **out)
         set_error("wf_create: no CUDA device");
         return WF_ERR_NO_DEVICE;
     }
-    if (cc_major != 10) { set_error("wf_create: device %d is sm_%d0, this build targets sm_100a", dev, cc_major); return WF_ERR_NO_DEVICE; }
+    if (cc_major != 10) { set_error("wf_create: device %d is sm_%d0, the library is compiled for sm_100a", dev, cc_major); return WF_ERR_NO_DEVICE; }
 
     wf_ctx *c = new wf_ctx();
     c->P = *P;
